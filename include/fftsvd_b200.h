@@ -1,0 +1,223 @@
+/*
+ * fftsvd_b200 — B200 (sm_100a) implementation of the FFTSVD boundary-element
+ * matvec and GMRES solve for the linearised Poisson-Boltzmann equation.
+ *
+ * Two C-ABI surfaces live here:
+ *
+ * 1. Drop-in replacements for the reference entry points of FFTSVDpbeAPI.h
+ *    (same names, signatures and ownership).  A program that builds its
+ *    operator with the reference host code (generateSurfaceOperator and
+ *    generateSurfaceOperatorPreconditioner) relinks against this library and
+ *    the solve, the right-hand side and the potential collection run on the
+ *    GPU.  The reference structures are read, never modified.
+ *
+ * 2. fftsvd_b200_* entry points over plain arrays: a surface built by this
+ *    library's own host setup from a triangle mesh and point charges, matvec,
+ *    solve (FP64 or FP32 operator with FP64 refinement), right-hand side,
+ *    reaction potentials and energy.  All return an int status
+ *    (FFTSVD_OK = 0) and never exit the process; fftsvd_b200_last_error()
+ *    describes the last failure of the calling thread.
+ *
+ * Kernel and unit conventions follow the reference: Green's function 1/r
+ * (Laplace) and exp(-kappa r)/r (Yukawa), no 1/(4 pi); unknowns are
+ * x = [phi(0..N-1); dphi/dn(0..N-1)]; energies in kcal/mol.
+ */
+#ifndef FFTSVD_B200_H
+#define FFTSVD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFTSVD_MAX_DEPTH 16
+
+/* status codes */
+#define FFTSVD_OK 0
+#define FFTSVD_ERR_ARGUMENT 1      /* invalid argument or size */
+#define FFTSVD_ERR_CUDA 2          /* CUDA runtime or launch failure */
+#define FFTSVD_ERR_NO_DEVICE 3     /* no CUDA device visible */
+#define FFTSVD_ERR_SINGULAR 4      /* singular preconditioner block or GMRES breakdown */
+#define FFTSVD_ERR_NOT_CONVERGED 5 /* iteration cap reached above tolerance */
+#define FFTSVD_ERR_NONFINITE 6     /* NaN or Inf in input or iterate */
+#define FFTSVD_ERR_TIMEOUT 7       /* a bounded device wait expired */
+#define FFTSVD_ERR_UNSUPPORTED 8   /* operator topology this build does not handle */
+
+/* solve precision modes */
+#define FFTSVD_PREC_FP64 0         /* FP64 operator, FP64 Krylov vectors */
+#define FFTSVD_PREC_MIXED 1        /* FP32 operator inside GMRES, FP64 residual refinement */
+#define FFTSVD_PREC_FP32 2         /* FP32 operator, FP64 Krylov vectors, no refinement (reference as shipped) */
+
+/*
+ * Compressed FFTSVD operator of one region tree, flattened.  Mirrors the
+ * content of the reference Tree/Cube objects (Tree.h:3-38, Cube.h:3-54) in
+ * struct-of-arrays form.  All matrices are row-major.  Index arrays are
+ * zero-based; *_ptr arrays have count+1 entries.
+ */
+typedef struct {
+   int32_t num_panels;            /* source panels of the tree (columns) */
+   int32_t num_points;            /* collocation points (rows) */
+   int32_t depth;                 /* partitioning levels */
+   int32_t grid[FFTSVD_MAX_DEPTH];/* equivalent-density grid edge n per level (Tree.c:158-170) */
+
+   /* near field: every leaf with drows > 0 and dcolumns > 0 (Cube.c:715-793) */
+   int32_t num_leaves;
+   const int32_t* leaf_row_ptr;   /* [num_leaves+1] into leaf_rows */
+   const int32_t* leaf_rows;      /* point indices of the leaf (D rows) */
+   const int32_t* leaf_col_ptr;   /* [num_leaves+1] into leaf_cols */
+   const int32_t* leaf_cols;      /* own panels, then each local cube's panels (D columns) */
+   const int64_t* leaf_d_ptr;     /* [num_leaves+1] element offsets of each drows x dcolumns block */
+   const double* d_single;        /* single-layer near-field blocks */
+   const double* d_double;        /* double-layer near-field blocks */
+
+   /* far field: every cube with a non-empty interaction list */
+   int32_t num_cubes;
+   const int32_t* cube_level;     /* [num_cubes] */
+   const int32_t* cube_index;     /* [3*num_cubes] integer cube coordinates on its level */
+   const int32_t* cube_panel_ptr; /* [num_cubes+1] into cube_panels */
+   const int32_t* cube_panels;
+   const int32_t* cube_point_ptr; /* [num_cubes+1] into cube_points */
+   const int32_t* cube_points;
+   const int32_t* cube_row_rank;  /* VTsrc rows; 0 when the cube has no panels */
+   const int32_t* cube_col_rank;  /* Udest columns; 0 when the cube has no points */
+   const int64_t* cube_vt_ptr;    /* [num_cubes+1]; VT is row_rank x numpanels */
+   const double* vt;
+   const int64_t* cube_pv_ptr;    /* [num_cubes+1]; PV is n^3 x row_rank */
+   const double* pv_single;
+   const double* pv_double;
+   const int64_t* cube_uti_ptr;   /* [num_cubes+1]; UTI is col_rank x n^3 */
+   const double* uti;
+   const int64_t* cube_u_ptr;     /* [num_cubes+1]; U is numpoints x col_rank */
+   const double* u;
+   const int32_t* inter_ptr;      /* [num_cubes+1] into inter_cubes */
+   const int32_t* inter_cubes;    /* interacting cubes, as indices into the cube arrays */
+
+   /* translation operators (Tree.c:387-445): per level, 7*7*7 offset slots of
+      (2n-1)*(2n-1)*((2n-1)/2+1) complex values (re, im interleaved); slot
+      ((dx+3)*7+(dy+3))*7+(dz+3) for dx = dest.index - source.index; slots of
+      local offsets are unused */
+   const int64_t* t_level_ptr;    /* [depth+1] complex-element offsets */
+   const double* t_ops;
+} fftsvd_tree_flat;
+
+/*
+ * How one region tree reads and writes the global unknown vector
+ * (SurfaceOperator.c:51-158).  For tree panel k:
+ *   xs[k] = dphi_scale[k] * x[dphi_index[k]]   (single-layer density)
+ *   xd[k] = phi_scale[k]  * x[phi_index[k]]    (double-layer density)
+ *   y[out_index[k]] = (S xs + D xd)[k] + jump[k] * xd[k]
+ */
+typedef struct {
+   const int32_t* phi_index;
+   const double* phi_scale;
+   const int32_t* dphi_index;
+   const double* dphi_scale;
+   const int32_t* out_index;
+   const double* jump;
+} fftsvd_region_map;
+
+/* Preconditioner entries in compressed-column form (Preconditioner.c:201-225). */
+typedef struct {
+   int32_t n;
+   const int32_t* col_ptr;        /* [n+1] */
+   const int32_t* row_index;
+   const double* value;
+} fftsvd_precond_csc;
+
+/* Problem description for the library's own host setup. */
+typedef struct {
+   int32_t num_panels;
+   const double* vertices;        /* [9*num_panels] v1,v2,v3 per flat triangle, normal = (v3-v1)x(v2-v1) outward */
+   int32_t num_charges;
+   const double* charge_pos;      /* [3*num_charges] */
+   const double* charge;          /* [num_charges] in e */
+   double eps_in, eps_out;        /* dielectric constants inside / outside */
+   double kappa;                  /* inverse Debye length outside (1/A); 0 selects Laplace outside */
+   double svd_tol;                /* FFTSVD sampling tolerance (reference default 1e-5) */
+   int32_t max_panels_per_leaf;   /* octree leaf criterion (reference 32) */
+   int32_t grid_points;           /* equivalent-density grid edge (reference 4) */
+   int32_t num_threads;           /* host threads for setup; 0 = all */
+} fftsvd_problem;
+
+typedef struct fftsvd_surface fftsvd_surface;
+
+typedef struct {
+   int32_t iterations;            /* total inner GMRES iterations */
+   int32_t refinements;           /* outer FP64 refinement steps (mixed mode) */
+   int32_t status;
+   double residual;               /* final preconditioned relative residual */
+   double setup_ms, solve_ms;
+} fftsvd_solve_info;
+
+/* ---- library entry points (no counterpart in the reference unless stated) ---- */
+
+const char* fftsvd_b200_last_error(void);
+int fftsvd_b200_version(void);
+
+/* Build a two-region PBE surface (interior Laplace eps_in; exterior Laplace or
+   Yukawa eps_out) with this library's host setup and upload it to the current
+   CUDA device.  Replaces generateSurfaceOperator + Tree_fill +
+   generateSurfaceOperatorPreconditioner (FFTSVDpbeAPI.c:1053-1739,1853-1861). */
+int fftsvd_b200_surface_create(const fftsvd_problem* problem, fftsvd_surface** out);
+
+/* Upload an operator given in flat form (one tree per region). */
+int fftsvd_b200_surface_create_flat(int32_t num_unknowns, int32_t num_trees, const fftsvd_tree_flat* trees,
+                                    const fftsvd_region_map* maps, const fftsvd_precond_csc* precond,
+                                    int32_t num_charges, const double* charge_pos, const double* charge,
+                                    double eps_in, fftsvd_surface** out);
+
+void fftsvd_b200_surface_free(fftsvd_surface* s);
+int32_t fftsvd_b200_surface_num_unknowns(const fftsvd_surface* s);
+
+/* y = A x.  SurfaceOperator_topmultiply (SurfaceOperator.c:90-97).  Host pointers. */
+int fftsvd_b200_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y);
+/* Same with device pointers, asynchronous on the library stream. */
+int fftsvd_b200_matvec_device(fftsvd_surface* s, int32_t precision, const double* x, double* y);
+
+/* z = P^-1 r.  Preconditioner_solve (Preconditioner.c:272-294).  Host pointers. */
+int fftsvd_b200_precond_solve(fftsvd_surface* s, const double* r, double* z);
+
+/* One tree's b = S xs + D xd.  Tree_multiplyboth (Tree.c:597-683).  Host pointers. */
+int fftsvd_b200_tree_multiplyboth(fftsvd_surface* s, int32_t tree, int32_t precision, const double* xs,
+                                  const double* xd, double* b);
+
+/* GMRES solve of A x = rhs (GMRES.c:446-539).  Host pointers. */
+int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
+                      int32_t max_iterations, fftsvd_solve_info* info);
+/* Same with device pointers (rhs, sol resident in HBM). */
+int fftsvd_b200_solve_device(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
+                             int32_t max_iterations, fftsvd_solve_info* info);
+
+/* rhs[i] = sum_j q_j / |x_j - c_i| on the interior rows (SurfaceOperator.c:291-321). */
+int fftsvd_b200_rhs(fftsvd_surface* s, double* rhs);
+/* Reaction potential at every charge from a surface solution
+   (SurfaceOperator.c:364-396, direct analytic panel integrals). */
+int fftsvd_b200_reaction_potentials(fftsvd_surface* s, const double* sol, double* phi);
+/* 0.5 * sum q phi * 332.112 / eps_in (FFTSVDsalt.c:167-170). */
+int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
+
+/* Timing of the last device operations, for benchmarks: milliseconds of the
+   last matvec stages [near, far_forward, far_translate] and the algorithmic
+   byte count of one matvec at the given precision. */
+int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes);
+
+/* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ---- */
+
+struct _SurfaceOperator;
+struct _Preconditioner;
+struct PDBentry_s;
+
+/* FFTSVDpbeAPI.h:153 — solution is allocated with calloc (2*numtotalpanels
+   doubles) and owned by the caller, as in FFTSVDpbeAPI.c:1884-1888. */
+void solveSurfaceOperator(double** solution, struct _SurfaceOperator* pbesurfaceoperator,
+                          struct _Preconditioner* preconditioner, double* rhs, unsigned int numtotalpanels);
+/* FFTSVDpbeAPI.h:150 — rhs is allocated with calloc (2*numtotalpanels doubles). */
+void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceoperator, unsigned int numtotalpanels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

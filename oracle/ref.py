@@ -1,0 +1,201 @@
+"""ORACLE — test infrastructure only (never imported by the product path).
+
+ctypes access to the reference FFTSVD C code compiled by oracle/Makefile into
+oracle/_ref/ (libfftsvd_ref.so: as shipped, FP32 operator storage;
+libfftsvd_ref64.so: FP64 operator storage).  See oracle/ref_driver.c for the
+reference functions behind each call.
+
+The reference prints progress and every GMRES residual to stdout
+(GMRES.c:505-507); calls are wrapped so that this output goes to stderr and a
+caller's stdout stays clean.
+"""
+from __future__ import annotations
+
+import contextlib
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+sys.path.insert(0, os.path.dirname(HERE))
+from fftsvd_b200._abi import TreeFlat, tree_flat_to_numpy  # noqa: E402
+
+_f64p = C.POINTER(C.c_double)
+_libs = {}
+
+
+def library_path(fp64: bool) -> str:
+    return os.path.join(REF_DIR, "libfftsvd_ref64.so" if fp64 else "libfftsvd_ref.so")
+
+
+def available(fp64: bool = False) -> bool:
+    return os.path.exists(library_path(fp64))
+
+
+def _lib(fp64: bool):
+    key = bool(fp64)
+    if key not in _libs:
+        lib = C.CDLL(library_path(fp64))
+        lib.oref_create.restype = C.c_void_p
+        lib.oref_create.argtypes = [C.c_uint, _f64p, C.c_uint, _f64p, _f64p, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_uint, C.c_uint]
+        lib.oref_create_api.restype = C.c_void_p
+        lib.oref_create_api.argtypes = [C.c_uint, _f64p, C.c_uint, _f64p, _f64p, C.c_double, C.c_double,
+                                        C.c_double, C.c_double]
+        lib.oref_free.argtypes = [C.c_void_p]
+        lib.oref_surface_operator.restype = C.c_void_p
+        lib.oref_surface_operator.argtypes = [C.c_void_p]
+        lib.oref_preconditioner.restype = C.c_void_p
+        lib.oref_preconditioner.argtypes = [C.c_void_p]
+        lib.oref_num_panels.restype = C.c_uint
+        lib.oref_num_panels.argtypes = [C.c_void_p]
+        lib.oref_depth.restype = C.c_uint
+        lib.oref_depth.argtypes = [C.c_void_p, C.c_int]
+        lib.oref_matvec.argtypes = [C.c_void_p, _f64p, _f64p]
+        lib.oref_tree_multiplyboth.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p]
+        lib.oref_precond_solve.argtypes = [C.c_void_p, _f64p, _f64p]
+        lib.oref_rhs.argtypes = [C.c_void_p, _f64p]
+        lib.oref_gmres.restype = C.c_int
+        lib.oref_gmres.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double]
+        lib.oref_reaction.argtypes = [C.c_void_p, _f64p, _f64p]
+        lib.oref_energy.restype = C.c_double
+        lib.oref_energy.argtypes = [C.c_void_p, _f64p]
+        lib.oref_panel_integrals.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_uint, _f64p,
+                                             C.POINTER(C.c_uint), _f64p, _f64p]
+        lib.oref_export_tree.restype = C.c_int
+        lib.oref_export_tree.argtypes = [C.c_void_p, C.c_int, C.POINTER(TreeFlat)]
+        lib.oref_export_free.argtypes = [C.POINTER(TreeFlat)]
+        _libs[key] = lib
+    return _libs[key]
+
+
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """Route fd 1 to fd 2 while the reference prints."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        C.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
+def _p(a):
+    return a.ctypes.data_as(_f64p)
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads used by the reference's parallel regions (Tree.c:630-656)."""
+    os.environ["OMP_NUM_THREADS"] = str(n)
+    try:
+        C.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+    except OSError:
+        pass
+
+
+class RefSystem:
+    """The reference two-region PBE operator (outer region: tree 0, inner: tree 1)."""
+
+    def __init__(self, tri, qpos, q, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels=32, grid=4,
+                 fp64=False, via_api=False, gmres_tol=1e-6):
+        self.fp64 = fp64
+        self.lib = _lib(fp64)
+        self.tri = np.ascontiguousarray(tri, dtype=np.float64)
+        self.qpos = np.ascontiguousarray(qpos, dtype=np.float64)
+        self.q = np.ascontiguousarray(q, dtype=np.float64)
+        self.n = len(self.tri)
+        self.nq = len(self.q)
+        with stdout_to_stderr():
+            if via_api:
+                ionic = (kappa * 3.047) ** 2
+                self.h = self.lib.oref_create_api(self.n, _p(self.tri), self.nq, _p(self.qpos), _p(self.q),
+                                                  eps_in, eps_out, ionic, gmres_tol)
+            else:
+                self.h = self.lib.oref_create(self.n, _p(self.tri), self.nq, _p(self.qpos), _p(self.q),
+                                              eps_in, eps_out, kappa, svd_tol, max_panels, grid)
+
+    def close(self):
+        if self.h:
+            self.lib.oref_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def surface_operator(self):
+        return self.lib.oref_surface_operator(self.h)
+
+    @property
+    def preconditioner(self):
+        return self.lib.oref_preconditioner(self.h)
+
+    def depth(self, which):
+        return int(self.lib.oref_depth(self.h, which))
+
+    def matvec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(2 * self.n)
+        self.lib.oref_matvec(self.h, _p(x), _p(y))
+        return y
+
+    def tree_multiplyboth(self, which, xs, xd):
+        xs = np.ascontiguousarray(xs, dtype=np.float64)
+        xd = np.ascontiguousarray(xd, dtype=np.float64)
+        b = np.zeros(self.n)
+        self.lib.oref_tree_multiplyboth(self.h, which, _p(xs), _p(xd), _p(b))
+        return b
+
+    def precond_solve(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(2 * self.n)
+        self.lib.oref_precond_solve(self.h, _p(b), _p(x))
+        return x
+
+    def rhs(self):
+        r = np.zeros(2 * self.n)
+        self.lib.oref_rhs(self.h, _p(r))
+        return r
+
+    def solve(self, rhs, tol=1e-6):
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        sol = np.zeros(2 * self.n)
+        with stdout_to_stderr():
+            it = self.lib.oref_gmres(self.h, _p(rhs), _p(sol), tol)
+        return sol, it
+
+    def reaction(self, sol):
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        phi = np.zeros(self.nq)
+        self.lib.oref_reaction(self.h, _p(sol), _p(phi))
+        return phi
+
+    def energy(self, phi):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        return float(self.lib.oref_energy(self.h, _p(phi)))
+
+    def panel_integrals(self, kernel, kappa, pts, panel_of_point):
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        idx = np.ascontiguousarray(panel_of_point, dtype=np.uint32)
+        s = np.zeros(len(pts))
+        d = np.zeros(len(pts))
+        self.lib.oref_panel_integrals(self.h, int(kernel), float(kappa), len(pts), _p(pts),
+                                      idx.ctypes.data_as(C.POINTER(C.c_uint)), _p(s), _p(d))
+        return s, d
+
+    def export_tree(self, which) -> dict:
+        t = TreeFlat()
+        self.lib.oref_export_tree(self.h, which, C.byref(t))
+        try:
+            return tree_flat_to_numpy(t)
+        finally:
+            self.lib.oref_export_free(C.byref(t))
