@@ -1,0 +1,234 @@
+// GMRES vector kernels (FP64).  The reference orthogonalises with modified
+// Gram-Schmidt, one dot and one axpy per basis vector (GMRES.c:485-488); here
+// each Arnoldi step uses classical Gram-Schmidt applied twice (two passes of
+// one multi-dot and one multi-axpy over the whole basis), which is as stable as
+// MGS and turns 2(i+1) dependent vector sweeps into four.  All reductions are
+// two-stage with a fixed order, so results are bitwise reproducible run to run.
+#include <cmath>
+
+#include "gmres.cuh"
+
+namespace fftsvd {
+
+__device__ inline double warp_sum_d(double v) {
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   return v;
+}
+
+__global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
+                               const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
+                               const double* __restrict__ r, double* __restrict__ z) {
+   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += gridDim.x * blockDim.x) {
+      const int p0 = blk_ptr[b], k = blk_ptr[b + 1] - p0;
+      double in[8], out[8];
+      for (int i = 0; i < k; i++) in[i] = r[blk_idx[p0 + i]];
+      const double* M = inv + inv_off[b];
+      for (int i = 0; i < k; i++) {
+         double s = 0.0;
+         for (int j = 0; j < k; j++) s += M[i * k + j] * in[j];
+         out[i] = s;
+      }
+      for (int i = 0; i < k; i++) z[blk_idx[p0 + i]] = out[i];
+   }
+}
+
+// Block-wide reduction of 8 values per thread into red[0..7] (fixed order).
+__device__ inline void block_reduce8(double (&acc)[8], double* red /* [nwarps*8] */, int tid) {
+   const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+   for (int q = 0; q < 8; q++) acc[q] = warp_sum_d(acc[q]);
+   if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 8; q++) red[warp * 8 + q] = acc[q];
+   __syncthreads();
+   if (tid < 8) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w * 8 + tid];
+      red[kVecThreads / 32 * 8 + tid] = s;
+   }
+   __syncthreads();
+}
+
+__device__ inline void dots_of(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv, int64_t k0, int64_t k1,
+                               double w0, double w1, double* __restrict__ partial, double* red) {
+   const int tid = threadIdx.x;
+   for (int j = 0; j < nvec; j += 8) {
+      double acc[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+         double s = 0.0;
+         if (j + q < nvec) {
+            const double* v = V + (int64_t)(j + q) * ldv;
+            if (k0 < n) s += v[k0] * w0;
+            if (k1 < n) s += v[k1] * w1;
+         }
+         acc[q] = s;
+      }
+      block_reduce8(acc, red, tid);
+      if (tid < 8 && j + tid < nvec) partial[(int64_t)(j + tid) * gridDim.x + blockIdx.x] = red[kVecThreads / 32 * 8 + tid];
+      __syncthreads();
+   }
+}
+
+__global__ void __launch_bounds__(kVecThreads) dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V,
+                                                                   int64_t ldv, const double* __restrict__ w,
+                                                                   double* __restrict__ partial) {
+   __shared__ double red[kVecThreads / 32 * 8 + 8];
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
+   const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
+   dots_of(n, nvec, V, ldv, k0, k1, w0, w1, partial, red);
+}
+
+__global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
+                                      int accumulate) {
+   __shared__ double red[32];
+   const int j = blockIdx.x;
+   if (j >= nvec) return;
+   double s = 0.0;
+   for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[(int64_t)j * nblk + b];
+   s = warp_sum_d(s);
+   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+      out[j] = accumulate ? out[j] + t : t;
+   }
+}
+
+__global__ void __launch_bounds__(kVecThreads) update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V,
+                                                                  int64_t ldv, const double* __restrict__ h,
+                                                                  double* __restrict__ w, double* __restrict__ partial) {
+   extern __shared__ double sh[];  // [nvec] h, then reduction scratch
+   double* hs = sh;
+   double* red = sh + ((nvec + 1) & ~1);
+   for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
+   __syncthreads();
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
+   double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
+   for (int j = 0; j < nvec; j++) {
+      const double* v = V + (int64_t)j * ldv;
+      if (k0 < n) w0 -= v[k0] * hs[j];
+      if (k1 < n) w1 -= v[k1] * hs[j];
+   }
+   if (k0 < n) w[k0] = w0;
+   if (k1 < n) w[k1] = w1;
+   dots_of(n, nvec, V, ldv, k0, k1, w0, w1, partial, red);
+}
+
+__global__ void __launch_bounds__(kVecThreads) update_norm_kernel(int64_t n, int nvec, const double* __restrict__ V,
+                                                                  int64_t ldv, const double* __restrict__ h,
+                                                                  const double* __restrict__ w,
+                                                                  double* __restrict__ out,
+                                                                  double* __restrict__ partial) {
+   extern __shared__ double sh[];
+   double* hs = sh;
+   double* red = sh + ((nvec + 1) & ~1);
+   for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
+   __syncthreads();
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
+   double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
+   for (int j = 0; j < nvec; j++) {
+      const double* v = V + (int64_t)j * ldv;
+      if (k0 < n) w0 -= v[k0] * hs[j];
+      if (k1 < n) w1 -= v[k1] * hs[j];
+   }
+   if (k0 < n) out[k0] = w0;
+   if (k1 < n) out[k1] = w1;
+   double acc[8] = {w0 * w0 + w1 * w1, 0, 0, 0, 0, 0, 0, 0};
+   block_reduce8(acc, red, threadIdx.x);
+   if (threadIdx.x == 0) partial[blockIdx.x] = red[kVecThreads / 32 * 8];
+}
+
+__global__ void __launch_bounds__(kVecThreads) norm_partial_kernel(int64_t n, const double* __restrict__ w,
+                                                                   double* __restrict__ partial) {
+   __shared__ double red[kVecThreads / 32 * 8 + 8];
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
+   const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
+   double acc[8] = {w0 * w0 + w1 * w1, 0, 0, 0, 0, 0, 0, 0};
+   block_reduce8(acc, red, threadIdx.x);
+   if (threadIdx.x == 0) partial[blockIdx.x] = red[kVecThreads / 32 * 8];
+}
+
+__device__ inline void rotate(double c, double s, double* a, double* b) {  // GMRES.c:17-22
+   const double a1 = *a, b1 = *b;
+   *a = a1 * c - b1 * s;
+   *b = c * b1 + s * a1;
+}
+
+__global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
+                              const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
+                              double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
+                              GivensState* __restrict__ st) {
+   __shared__ double red[256];
+   double s = 0.0;
+   for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += norm_partial[b];
+   red[threadIdx.x] = s;
+   __syncthreads();
+   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      __syncthreads();
+   }
+   if (threadIdx.x != 0) return;
+   const double beta = sqrt(red[0]);
+   double* col = H + (int64_t)i * ldh;
+   bool finite = isfinite(beta);
+   for (int j = 0; j <= i; j++) {
+      col[j] = h1[j] + h2[j];
+      finite = finite && isfinite(col[j]);
+   }
+   col[i + 1] = beta;
+   for (int k = 0; k < i; k++) rotate(cs[k], sn[k], &col[k], &col[k + 1]);
+   // GMRES.c:3-15
+   double c, sv;
+   if (col[i + 1] == 0.0) {
+      c = 1.0;
+      sv = 0.0;
+   } else {
+      const double r1 = fabs(col[i]), r2 = fabs(col[i + 1]);
+      const double len = sqrt(r1 * r1 + r2 * r2);
+      c = col[i] / len;
+      sv = -col[i + 1] / len;
+   }
+   cs[i] = c;
+   sn[i] = sv;
+   rotate(c, sv, &col[i], &col[i + 1]);
+   g[i + 1] = 0.0;
+   rotate(c, sv, &g[i], &g[i + 1]);
+   st->residual = fabs(g[i + 1]) / st->normr;
+   st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
+   st->flag = !finite ? 2 : (beta == 0.0 ? 1 : 0);
+}
+
+__global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
+                             double factor, double* __restrict__ dst) {
+   const double f = factor_ptr ? *factor_ptr : factor;
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      dst[k] = src[k] * f;
+}
+
+__global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                               const double* __restrict__ y, double* __restrict__ x) {
+   extern __shared__ double ys[];
+   for (int j = threadIdx.x; j < nvec; j += blockDim.x) ys[j] = y[j];
+   __syncthreads();
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+      double s = x[k];
+      for (int j = 0; j < nvec; j++) s += V[(int64_t)j * ldv + k] * ys[j];
+      x[k] = s;
+   }
+}
+
+__global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ dst) {
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      dst[k] = a[k] - b[k];
+}
+
+__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst) {
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      dst[k] += a[k];
+}
+
+}  // namespace fftsvd

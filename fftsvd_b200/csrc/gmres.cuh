@@ -1,0 +1,66 @@
+// Device kernels of the GMRES solve (GMRES.c:446-539) and the block-diagonal
+// preconditioner (Preconditioner.c:272-294).  FP64 throughout.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fftsvd {
+
+constexpr int kVecThreads = 256;
+constexpr int kRowsPerThread = 2;
+constexpr int kRowsPerBlock = kVecThreads * kRowsPerThread;
+
+// z[idx] = inv * r[idx] for every preconditioner block (blocks of size <= 8).
+__global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
+                               const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
+                               const double* __restrict__ r, double* __restrict__ z);
+
+// partial[j * nblk + b] = sum over rows of block b of V[j][k] * w[k], j < nvec
+__global__ void dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                                    const double* __restrict__ w, double* __restrict__ partial);
+// out[j] = (accumulate ? out[j] : 0) + sum_b partial[j * nblk + b]; one block per j
+__global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
+                                      int accumulate);
+// w -= V h; then partial dots of the updated w against V (second Gram-Schmidt pass)
+__global__ void update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                                   const double* __restrict__ h, double* __restrict__ w, double* __restrict__ partial);
+// out = w - V h (written to out, may alias w); partial[b] = sum of squares of out over block b
+__global__ void update_norm_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                                   const double* __restrict__ h, const double* __restrict__ w, double* __restrict__ out,
+                                   double* __restrict__ partial);
+// partial[b] = sum of squares of w over block b
+__global__ void norm_partial_kernel(int64_t n, const double* __restrict__ w, double* __restrict__ partial);
+
+struct GivensState {
+   double normr;      // preconditioned rhs norm
+   double residual;   // |g[i+1]| / normr after the last step
+   double inv_beta;   // 1 / H[i][i+1]
+   int32_t flag;      // 0 ok, 1 breakdown (beta == 0), 2 non-finite
+   int32_t pad;
+};
+
+// Completes Arnoldi step i: H column from the two Gram-Schmidt passes and the
+// norm partials, applies the previous rotations, forms the new one, updates g
+// (GMRES.c:485-503).  Single block.
+__global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
+                              const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
+                              double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
+                              GivensState* __restrict__ st);
+
+__global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
+                             double factor, double* __restrict__ dst);
+
+// x += V y  (y on device)
+__global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                               const double* __restrict__ y, double* __restrict__ x);
+
+// dst = a - b
+__global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst);
+// dst += a
+__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst);
+
+inline int vec_blocks(int64_t n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
+
+}  // namespace fftsvd

@@ -1,0 +1,244 @@
+// Charge <-> panel interaction kernels (FP64):
+//   right-hand side          SurfaceOperator_makeRHS                 SurfaceOperator.c:291-321
+//   reaction potentials      SurfaceOperator_calculateReactionPotentials, direct branch
+//                                                                     SurfaceOperator.c:364-396
+//   energy                   FFTSVDsalt.c:167-170
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "nbody.h"
+#include "surface.h"
+
+namespace fftsvd {
+
+void set_geometry(Surface& S, int num_panels, const double* vertices, const int32_t* phi_row, const int32_t* dphi_row) {
+   FFTSVD_REQUIRE(num_panels > 0 && vertices && phi_row && dphi_row, "bad panel geometry");
+   auto g = std::make_shared<PanelGeometry>();
+   g->num_panels = num_panels;
+   g->host.resize(num_panels);
+   for (int i = 0; i < num_panels; i++) {
+      const double* v = vertices + 9 * (size_t)i;
+      make_flat_panel(g->host[i], v, v + 3, v + 6);
+      FFTSVD_REQUIRE(g->host[i].area > 0.0, "degenerate panel " + std::to_string(i));
+   }
+   for (int i = 0; i < num_panels; i++)
+      FFTSVD_REQUIRE(phi_row[i] >= 0 && phi_row[i] < S.n && dphi_row[i] >= 0 && dphi_row[i] < S.n,
+                     "panel row out of range");
+   g->panels.upload(g->host);
+   g->phi_row.upload(phi_row, num_panels);
+   g->dphi_row.upload(dphi_row, num_panels);
+   S.geom = g;
+}
+
+void set_charges(Surface& S, int num_charges, const double* pos, const double* q) {
+   FFTSVD_REQUIRE(num_charges >= 0, "negative charge count");
+   S.num_charges = num_charges;
+   if (num_charges == 0) return;
+   FFTSVD_REQUIRE(pos && q, "null charge arrays");
+   for (int i = 0; i < num_charges; i++)
+      FFTSVD_REQUIRE(std::isfinite(q[i]) && std::isfinite(pos[3 * i]) && std::isfinite(pos[3 * i + 1]) &&
+                         std::isfinite(pos[3 * i + 2]),
+                     "non-finite charge input");
+   S.charge_pos.upload(pos, 3 * (size_t)num_charges);
+   S.charge_q.upload(q, num_charges);
+   S.charge_q_host.assign(q, q + num_charges);
+}
+
+constexpr int kRhsThreads = 256;
+constexpr int kRhsTile = 256;
+
+// One thread per panel; charges streamed through shared memory in order, so each
+// panel accumulates over charges in the reference's order (charge-major loop).
+__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, const FlatPanel* __restrict__ panels,
+                                                          const int32_t* __restrict__ phi_row, int nq,
+                                                          const double* __restrict__ qpos,
+                                                          const double* __restrict__ q, double* __restrict__ rhs) {
+   __shared__ double4 tile[kRhsTile];
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   double c[3] = {0, 0, 0};
+   if (i < np) { c[0] = panels[i].centroid[0]; c[1] = panels[i].centroid[1]; c[2] = panels[i].centroid[2]; }
+   double acc = 0.0;
+   for (int base = 0; base < nq; base += kRhsTile) {
+      const int cnt = min(kRhsTile, nq - base);
+      __syncthreads();
+      for (int j = threadIdx.x; j < cnt; j += blockDim.x)
+         tile[j] = make_double4(qpos[3 * (base + j)], qpos[3 * (base + j) + 1], qpos[3 * (base + j) + 2], q[base + j]);
+      __syncthreads();
+      if (i < np)
+         for (int j = 0; j < cnt; j++) {
+            const double4 t = tile[j];
+            if (t.w == 0.0) continue;
+            const double dx = t.x - c[0], dy = t.y - c[1], dz = t.z - c[2];
+            acc += t.w / sqrt(dx * dx + dy * dy + dz * dz);
+         }
+   }
+   if (i < np) rhs[phi_row[i]] = acc;
+}
+
+constexpr int kReactThreads = 128;
+constexpr int kReactPanelTile = 16;
+constexpr int kReactChunks = 64;
+
+// Block (charge chunk, panel chunk): each thread owns one charge and sums the
+// panel integrals of its panel chunk; panels staged through shared memory.
+__global__ void __launch_bounds__(kReactThreads) reaction_partial_kernel(
+    int np, const FlatPanel* __restrict__ panels, const int32_t* __restrict__ phi_row,
+    const int32_t* __restrict__ dphi_row, const double* __restrict__ sol, int nq, const double* __restrict__ qpos,
+    double* __restrict__ partial) {
+   __shared__ FlatPanel tile[kReactPanelTile];
+   __shared__ double2 dens[kReactPanelTile];
+   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+   const int per = (np + gridDim.y - 1) / gridDim.y;
+   const int p0 = blockIdx.y * per, p1 = min(np, p0 + per);
+   double pt[3] = {0, 0, 0};
+   if (j < nq) { pt[0] = qpos[3 * j]; pt[1] = qpos[3 * j + 1]; pt[2] = qpos[3 * j + 2]; }
+   double acc = 0.0;
+   for (int base = p0; base < p1; base += kReactPanelTile) {
+      const int cnt = min(kReactPanelTile, p1 - base);
+      __syncthreads();
+      {
+         const double* src = reinterpret_cast<const double*>(panels + base);
+         double* dst = reinterpret_cast<double*>(tile);
+         const int words = cnt * (int)(sizeof(FlatPanel) / sizeof(double));
+         for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+         for (int k = threadIdx.x; k < cnt; k += blockDim.x)
+            dens[k] = make_double2(sol[phi_row[base + k]], sol[dphi_row[base + k]]);
+      }
+      __syncthreads();
+      if (j < nq)
+         for (int k = 0; k < cnt; k++) {
+            double s, d;
+            laplace_panel(pt, tile[k], &s, &d);
+            const double2 dn = dens[k];
+            acc += dn.y * s - dn.x * d;
+            if (tile[k].centroid[0] == pt[0] && tile[k].centroid[1] == pt[1] && tile[k].centroid[2] == pt[2])
+               acc -= 4.0 * M_PI * dn.x;
+         }
+   }
+   if (j < nq) partial[(size_t)blockIdx.y * nq + j] = acc;
+}
+
+__global__ void reaction_reduce_kernel(int nq, int chunks, const double* __restrict__ partial, double* __restrict__ phi) {
+   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+   if (j >= nq) return;
+   double s = 0.0;
+   for (int c = 0; c < chunks; c++) s += partial[(size_t)c * nq + j];
+   phi[j] = s;
+}
+
+void rhs_device(Surface& S, double* rhs) {
+   FFTSVD_REQUIRE(S.geom, "surface has no panel geometry");
+   FFTSVD_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * S.n, S.stream));
+   const int np = S.geom->num_panels;
+   rhs_kernel<<<(np + kRhsThreads - 1) / kRhsThreads, kRhsThreads, 0, S.stream>>>(
+       np, S.geom->panels.get(), S.geom->phi_row.get(), S.num_charges, S.charge_pos.get(), S.charge_q.get(), rhs);
+   FFTSVD_CHECK_LAUNCH();
+}
+
+void reaction_device(Surface& S, const double* sol, double* phi) {
+   FFTSVD_REQUIRE(S.geom, "surface has no panel geometry");
+   const int nq = S.num_charges, np = S.geom->num_panels;
+   if (nq == 0) return;
+   const int chunks = std::max(1, std::min(kReactChunks, (np + kReactPanelTile - 1) / kReactPanelTile));
+   DevBuf<double> partial((size_t)chunks * nq);
+   dim3 grid((nq + kReactThreads - 1) / kReactThreads, chunks);
+   reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
+                                                                 S.geom->dphi_row.get(), sol, nq,
+                                                                 S.charge_pos.get(), partial.get());
+   FFTSVD_CHECK_LAUNCH();
+   reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, partial.get(), phi);
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+}
+
+double energy_device(Surface& S, const double* phi) {
+   std::vector<double> h(S.num_charges);
+   if (S.num_charges == 0) return 0.0;
+   FFTSVD_CUDA(cudaMemcpyAsync(h.data(), phi, sizeof(double) * S.num_charges, cudaMemcpyDeviceToHost, S.stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   double e = 0.0;
+   for (int c = 0; c < S.num_charges; c++) e += 0.5 * S.charge_q_host[c] * h[c];
+   return e * 332.112 / S.eps_in;
+}
+
+}  // namespace fftsvd
+
+using namespace fftsvd;
+
+extern "C" {
+
+int fftsvd_b200_set_geometry(fftsvd_surface* s, int32_t num_panels, const double* vertices, const int32_t* phi_row,
+                             const int32_t* dphi_row) {
+   if (!s) return FFTSVD_ERR_ARGUMENT;
+   try {
+      set_geometry(s->s, num_panels, vertices, phi_row, dphi_row);
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+int fftsvd_b200_rhs(fftsvd_surface* s, double* rhs) {
+   if (!s || !rhs) return FFTSVD_ERR_ARGUMENT;
+   try {
+      Surface& S = s->s;
+      rhs_device(S, S.t2.get());
+      FFTSVD_CUDA(cudaMemcpyAsync(rhs, S.t2.get(), sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+int fftsvd_b200_rhs_device(fftsvd_surface* s, double* rhs) {
+   if (!s || !rhs) return FFTSVD_ERR_ARGUMENT;
+   try {
+      rhs_device(s->s, rhs);
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+int fftsvd_b200_reaction_potentials(fftsvd_surface* s, const double* sol, double* phi) {
+   if (!s || !sol || !phi) return FFTSVD_ERR_ARGUMENT;
+   try {
+      Surface& S = s->s;
+      if (S.num_charges == 0) return FFTSVD_OK;
+      DevBuf<double> dsol, dphi(S.num_charges);
+      dsol.upload(sol, S.n);
+      reaction_device(S, dsol.get(), dphi.get());
+      FFTSVD_CUDA(cudaMemcpy(phi, dphi.get(), sizeof(double) * S.num_charges, cudaMemcpyDeviceToHost));
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+int fftsvd_b200_reaction_potentials_device(fftsvd_surface* s, const double* sol, double* phi) {
+   if (!s || !sol || !phi) return FFTSVD_ERR_ARGUMENT;
+   try {
+      reaction_device(s->s, sol, phi);
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy) {
+   if (!s || !phi || !energy) return FFTSVD_ERR_ARGUMENT;
+   double e = 0.0;
+   for (int c = 0; c < s->s.num_charges; c++) e += 0.5 * s->s.charge_q_host[c] * phi[c];
+   *energy = e * 332.112 / s->s.eps_in;
+   return FFTSVD_OK;
+}
+
+}  // extern "C"

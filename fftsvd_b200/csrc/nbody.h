@@ -1,0 +1,33 @@
+// Point-charge right-hand side and reaction-potential collection: dense
+// charge x panel interactions evaluated on the GPU in FP64.
+#pragma once
+
+#include <vector>
+
+#include "common.h"
+#include "integrals.h"
+
+namespace fftsvd {
+
+struct Surface;
+
+struct PanelGeometry {
+   int num_panels = 0;
+   DevBuf<FlatPanel> panels;          // panel geometry (device)
+   DevBuf<int32_t> phi_row, dphi_row; // unknown rows of phi and dphi/dn of each panel
+   std::vector<FlatPanel> host;
+};
+
+// Panel geometry of the charge-bearing (interior) region and the rows that
+// hold phi / dphi/dn of each of its panels (SurfaceOperator.c:291-321, 364-396).
+void set_geometry(Surface& S, int num_panels, const double* vertices, const int32_t* phi_row, const int32_t* dphi_row);
+void set_charges(Surface& S, int num_charges, const double* pos, const double* q);
+
+// rhs[phi_row[i]] = sum_j q_j / |x_j - c_i|, other rows zero.  Device pointer.
+void rhs_device(Surface& S, double* rhs);
+// phi_j = sum_i (dphi_i SLP(x_j, i) - phi_i DLP(x_j, i)) - 4 pi phi_i [x_j == c_i].  Device pointers.
+void reaction_device(Surface& S, const double* sol, double* phi);
+// 0.5 * sum q phi * 332.112 / eps_in
+double energy_device(Surface& S, const double* phi);
+
+}  // namespace fftsvd

@@ -1,0 +1,431 @@
+// Surface object, preconditioner, GMRES driver and the fftsvd_b200_* C-ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+
+#include "nbody.h"
+#include "surface.h"
+
+namespace fftsvd {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// ------------------------------------------------------------------ preconditioner
+
+// Split the assembled sparse matrix into connected components of its pattern
+// (one 2x2 block per panel for the PBE operator, SurfaceOperator.c:183-193)
+// and store the dense inverse of each.  Entries given twice are summed.
+void Preconditioner::build(const fftsvd_precond_csc& P, int n) {
+   FFTSVD_REQUIRE(P.n == n, "preconditioner size does not match the operator");
+   std::vector<int> parent(n);
+   std::iota(parent.begin(), parent.end(), 0);
+   auto find = [&](int a) {
+      while (parent[a] != a) a = parent[a] = parent[parent[a]];
+      return a;
+   };
+   for (int c = 0; c < n; c++)
+      for (int k = P.col_ptr[c]; k < P.col_ptr[c + 1]; k++) {
+         const int r = P.row_index[k];
+         FFTSVD_REQUIRE(r >= 0 && r < n, "preconditioner row out of range");
+         const int a = find(r), b = find(c);
+         if (a != b) parent[a] = b;
+      }
+   std::vector<int> root_block(n, -1), local(n), size;
+   std::vector<std::vector<int>> members;
+   for (int i = 0; i < n; i++) {
+      const int rt = find(i);
+      if (root_block[rt] < 0) {
+         root_block[rt] = (int)members.size();
+         members.emplace_back();
+      }
+      const int b = root_block[rt];
+      local[i] = (int)members[b].size();
+      members[b].push_back(i);
+   }
+   nblocks = (int)members.size();
+   std::vector<int32_t> ptr(nblocks + 1, 0), idx;
+   std::vector<int64_t> off(nblocks);
+   std::vector<double> inv;
+   std::vector<std::vector<double>> dense(nblocks);
+   for (int b = 0; b < nblocks; b++) {
+      const int k = (int)members[b].size();
+      if (k > 8) throw Error(FFTSVD_ERR_UNSUPPORTED, "preconditioner block larger than 8 unknowns");
+      dense[b].assign((size_t)k * k, 0.0);
+   }
+   for (int c = 0; c < n; c++)
+      for (int k = P.col_ptr[c]; k < P.col_ptr[c + 1]; k++) {
+         const int r = P.row_index[k];
+         const int b = root_block[find(c)];
+         const int kk = (int)members[b].size();
+         dense[b][(size_t)local[r] * kk + local[c]] += P.value[k];
+      }
+   for (int b = 0; b < nblocks; b++) {
+      const int k = (int)members[b].size();
+      ptr[b + 1] = ptr[b] + k;
+      for (int i : members[b]) idx.push_back(i);
+      off[b] = (int64_t)inv.size();
+      // Gauss-Jordan with partial pivoting
+      std::vector<double> a = dense[b], e((size_t)k * k, 0.0);
+      for (int i = 0; i < k; i++) e[(size_t)i * k + i] = 1.0;
+      for (int col = 0; col < k; col++) {
+         int piv = col;
+         for (int i = col + 1; i < k; i++)
+            if (std::fabs(a[(size_t)i * k + col]) > std::fabs(a[(size_t)piv * k + col])) piv = i;
+         if (a[(size_t)piv * k + col] == 0.0 || !std::isfinite(a[(size_t)piv * k + col]))
+            throw Error(FFTSVD_ERR_SINGULAR, "singular preconditioner block at unknown " + std::to_string(members[b][col]));
+         if (piv != col)
+            for (int j = 0; j < k; j++) {
+               std::swap(a[(size_t)piv * k + j], a[(size_t)col * k + j]);
+               std::swap(e[(size_t)piv * k + j], e[(size_t)col * k + j]);
+            }
+         const double d = a[(size_t)col * k + col];
+         for (int j = 0; j < k; j++) { a[(size_t)col * k + j] /= d; e[(size_t)col * k + j] /= d; }
+         for (int i = 0; i < k; i++) {
+            if (i == col) continue;
+            const double f = a[(size_t)i * k + col];
+            if (f == 0.0) continue;
+            for (int j = 0; j < k; j++) {
+               a[(size_t)i * k + j] -= f * a[(size_t)col * k + j];
+               e[(size_t)i * k + j] -= f * e[(size_t)col * k + j];
+            }
+         }
+      }
+      inv.insert(inv.end(), e.begin(), e.end());
+   }
+   blk_ptr.upload(ptr);
+   blk_idx.upload(idx);
+   inv_off.upload(off);
+   this->inv.upload(inv);
+}
+
+void Preconditioner::apply(const double* r, double* z, cudaStream_t s) const {
+   const int threads = 256;
+   const int blocks = std::max(1, std::min((nblocks + threads - 1) / threads, 148 * 8));
+   precond_kernel<<<blocks, threads, 0, s>>>(nblocks, blk_ptr.get(), blk_idx.get(), inv_off.get(), inv.get(), r, z);
+   FFTSVD_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------------ surface
+
+Surface::~Surface() {
+   if (st_host) cudaFreeHost(st_host);
+   if (stream) cudaStreamDestroy(stream);
+}
+
+void Surface::ensure_capacity(int nvec) {
+   if (nvec <= capacity) return;
+   const int64_t nb = vec_blocks(n);
+   V.alloc((size_t)nvec * n);
+   H.alloc((size_t)nvec * nvec);
+   cs.alloc(nvec);
+   sn.alloc(nvec);
+   g.alloc(nvec);
+   h1.alloc(nvec);
+   h2.alloc(nvec);
+   y.alloc(nvec);
+   partial.alloc((size_t)nvec * nb);
+   capacity = nvec;
+}
+
+void Surface::apply(int precision, const double* x, double* yv) {
+   if (precision == FFTSVD_PREC_FP64)
+      op64.apply(x, yv, stream);
+   else
+      op32.apply(x, yv, stream);
+}
+
+double Surface::pnorm(const double* v) {
+   const int nb = vec_blocks(n);
+   norm_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, v, normpart.get());
+   FFTSVD_CHECK_LAUNCH();
+   reduce_partial_kernel<<<1, 256, 0, stream>>>(1, nb, normpart.get(), scal.get(), 0);
+   FFTSVD_CHECK_LAUNCH();
+   double s = 0.0;
+   FFTSVD_CUDA(cudaMemcpyAsync(&s, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   return std::sqrt(s);
+}
+
+int Surface::gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status) {
+   const int nb = vec_blocks(n);
+   const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
+   ensure_capacity(maxit + 1);
+   *status = FFTSVD_OK;
+   FFTSVD_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+   // r = P^-1 rhs (GMRES.c:457-465)
+   precond.apply(rhs, r.get(), stream);
+   const double normr = pnorm(r.get());
+   if (!std::isfinite(normr)) {
+      *status = FFTSVD_ERR_NONFINITE;
+      *res = normr;
+      return 0;
+   }
+   if (normr < tol) {  // hand back zero solution
+      *res = 0.0;
+      return 0;
+   }
+   double* Vp = V.get();
+   const int64_t ldv = n;
+   scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, r.get(), nullptr, 1.0 / normr, Vp);
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_CUDA(cudaMemsetAsync(g.get(), 0, sizeof(double) * capacity, stream));
+   FFTSVD_CUDA(cudaMemcpyAsync(g.get(), &normr, sizeof(double), cudaMemcpyHostToDevice, stream));
+   st_host->normr = normr;
+   st_host->residual = 1.0;
+   st_host->flag = 0;
+   FFTSVD_CUDA(cudaMemcpyAsync(st.get(), st_host, sizeof(GivensState), cudaMemcpyHostToDevice, stream));
+
+   int i = 0;
+   double resid = 1.0;
+   for (i = 0; i < maxit; i++) {
+      const int nvec = i + 1;
+      const double* vi = Vp + (int64_t)i * ldv;
+      double* vnext = Vp + (int64_t)(i + 1) * ldv;
+      apply(precision, vi, w.get());
+      precond.apply(w.get(), w.get(), stream);
+      dots_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get());
+      FFTSVD_CHECK_LAUNCH();
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h1.get(), 0);
+      FFTSVD_CHECK_LAUNCH();
+      const size_t sh = sizeof(double) * (((nvec + 1) & ~1) + kVecThreads / 32 * 8 + 8);
+      update_dots_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), partial.get());
+      FFTSVD_CHECK_LAUNCH();
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h2.get(), 0);
+      FFTSVD_CHECK_LAUNCH();
+      update_norm_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get());
+      FFTSVD_CHECK_LAUNCH();
+      givens_kernel<<<1, 256, 0, stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb, cs.get(),
+                                           sn.get(), g.get(), st.get());
+      FFTSVD_CHECK_LAUNCH();
+      scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext);
+      FFTSVD_CHECK_LAUNCH();
+      FFTSVD_CUDA(cudaMemcpyAsync(st_host, st.get(), sizeof(GivensState), cudaMemcpyDeviceToHost, stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(stream));
+      resid = st_host->residual;
+      if (st_host->flag == 2) {
+         *status = FFTSVD_ERR_NONFINITE;
+         break;
+      }
+      if (resid < tol || st_host->flag == 1) break;
+   }
+   int last = i;
+   if (i == maxit) {
+      last = maxit - 1;
+      *status = FFTSVD_ERR_NOT_CONVERGED;
+   }
+   // back substitution on the host (GMRES.c:512-521): k <= 1000 unknowns
+   const int k = last + 1;
+   std::vector<double> Hh((size_t)k * capacity), gh(k), yh(k);
+   FFTSVD_CUDA(cudaMemcpyAsync(Hh.data(), H.get(), sizeof(double) * (size_t)k * capacity, cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaMemcpyAsync(gh.data(), g.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   for (int q = 0; q < k; q++) yh[q] = gh[q];
+   for (int q = k - 1; q >= 0; q--) {
+      yh[q] /= Hh[(size_t)q * capacity + q];
+      for (int j = q - 1; j >= 0; j--) yh[j] -= Hh[(size_t)q * capacity + j] * yh[q];
+   }
+   FFTSVD_CUDA(cudaMemcpyAsync(y.get(), yh.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream));
+   combine_kernel<<<ew_blocks, 256, sizeof(double) * k, stream>>>(n, k, Vp, ldv, y.get(), x);
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   *res = resid;
+   return k;
+}
+
+int Surface::solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info) {
+   FFTSVD_REQUIRE(tol > 0.0 && maxit > 0, "tolerance and iteration cap must be positive");
+   const auto clock_start = std::chrono::steady_clock::now();
+   int status = FFTSVD_OK, iters = 0, refinements = 0;
+   double res = 0.0;
+   if (precision == FFTSVD_PREC_FP64 || precision == FFTSVD_PREC_FP32) {
+      iters = gmres(precision, rhs, x, tol, maxit, &res, &status);
+   } else if (precision == FFTSVD_PREC_MIXED) {
+      // FP64 iterative refinement around FP32-operator GMRES: x += A32^-1 (b - A64 x)
+      const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
+      precond.apply(rhs, t0.get(), stream);
+      const double bn = pnorm(t0.get());
+      FFTSVD_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+      FFTSVD_CUDA(cudaMemcpyAsync(t1.get(), rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+      res = 1.0;
+      if (!std::isfinite(bn)) status = FFTSVD_ERR_NONFINITE;
+      else if (bn < tol) res = 0.0;
+      for (refinements = 0; status == FFTSVD_OK && res >= tol && refinements < 8; refinements++) {
+         double inner_res = 0.0;
+         int st2 = FFTSVD_OK;
+         // inner solve to tol relative to the current residual
+         iters += gmres(FFTSVD_PREC_FP32, t1.get(), xout.get(), std::max(tol, 1e-12), maxit, &inner_res, &st2);
+         if (st2 == FFTSVD_ERR_NONFINITE) { status = st2; break; }
+         add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x);
+         FFTSVD_CHECK_LAUNCH();
+         op64.apply(x, t2.get(), stream);
+         sub_kernel<<<ew_blocks, 256, 0, stream>>>(n, rhs, t2.get(), t1.get());
+         FFTSVD_CHECK_LAUNCH();
+         precond.apply(t1.get(), t0.get(), stream);
+         res = pnorm(t0.get()) / bn;
+         if (!std::isfinite(res)) status = FFTSVD_ERR_NONFINITE;
+      }
+      if (status == FFTSVD_OK && res >= tol) status = FFTSVD_ERR_NOT_CONVERGED;
+   } else {
+      throw Error(FFTSVD_ERR_ARGUMENT, "unknown precision mode");
+   }
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   const auto clock_end = std::chrono::steady_clock::now();
+   if (info) {
+      info->iterations = iters;
+      info->refinements = refinements;
+      info->status = status;
+      info->residual = res;
+      info->solve_ms = std::chrono::duration<double, std::milli>(clock_end - clock_start).count();
+   }
+   return status;
+}
+
+static void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
+                         const fftsvd_region_map* maps, const fftsvd_precond_csc* P) {
+   int ndev = 0;
+   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+      throw Error(FFTSVD_ERR_NO_DEVICE, "no CUDA device visible");
+   FFTSVD_REQUIRE(trees && maps && P, "null operator description");
+   S.n = num_unknowns;
+   FFTSVD_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+   OperatorLayout L = build_layout(num_unknowns, num_trees, trees, maps);
+   S.operator_elems = L.operator_elems;
+   S.t_elems = L.t_elems;
+   S.op64.upload(L);
+   S.op32.upload(L);
+   S.precond.build(*P, num_unknowns);
+   const int nb = vec_blocks(num_unknowns);
+   S.w.alloc(num_unknowns);
+   S.r.alloc(num_unknowns);
+   S.t0.alloc(num_unknowns);
+   S.t1.alloc(num_unknowns);
+   S.t2.alloc(num_unknowns);
+   S.xin.alloc(num_unknowns);
+   S.xout.alloc(num_unknowns);
+   S.sold.alloc(num_unknowns);
+   S.scal.alloc(8);
+   S.normpart.alloc(nb);
+   S.st.alloc(1);
+   FFTSVD_CUDA(cudaMallocHost(&S.st_host, sizeof(GivensState)));
+   FFTSVD_CUDA(cudaDeviceSynchronize());
+}
+
+}  // namespace fftsvd
+
+using namespace fftsvd;
+
+template <typename F>
+static int guarded(F&& f) {
+   try {
+      f();
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   } catch (const std::bad_alloc&) {
+      set_last_error("host allocation failed");
+      return FFTSVD_ERR_ARGUMENT;
+   } catch (const std::exception& e) {
+      set_last_error(e.what());
+      return FFTSVD_ERR_ARGUMENT;
+   }
+}
+
+extern "C" {
+
+const char* fftsvd_b200_last_error(void) { return g_last_error.c_str(); }
+int fftsvd_b200_version(void) { return 100; }
+
+int fftsvd_b200_surface_create_flat(int32_t num_unknowns, int32_t num_trees, const fftsvd_tree_flat* trees,
+                                    const fftsvd_region_map* maps, const fftsvd_precond_csc* precond,
+                                    int32_t num_charges, const double* charge_pos, const double* charge,
+                                    double eps_in, fftsvd_surface** out) {
+   if (!out) return FFTSVD_ERR_ARGUMENT;
+   *out = nullptr;
+   fftsvd_surface* s = new (std::nothrow) fftsvd_surface();
+   if (!s) return FFTSVD_ERR_ARGUMENT;
+   int rc = guarded([&] {
+      init_surface(s->s, num_unknowns, num_trees, trees, maps, precond);
+      s->s.eps_in = eps_in;
+      set_charges(s->s, num_charges, charge_pos, charge);
+   });
+   if (rc != FFTSVD_OK) {
+      delete s;
+      return rc;
+   }
+   *out = s;
+   return FFTSVD_OK;
+}
+
+void fftsvd_b200_surface_free(fftsvd_surface* s) { delete s; }
+
+int32_t fftsvd_b200_surface_num_unknowns(const fftsvd_surface* s) { return s ? s->s.n : 0; }
+
+int fftsvd_b200_matvec_device(fftsvd_surface* s, int32_t precision, const double* x, double* y) {
+   if (!s || !x || !y) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] { s->s.apply(precision == FFTSVD_PREC_FP64 ? FFTSVD_PREC_FP64 : FFTSVD_PREC_FP32, x, y); });
+}
+
+int fftsvd_b200_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y) {
+   if (!s || !x || !y) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      Surface& S = s->s;
+      FFTSVD_CUDA(cudaMemcpyAsync(S.xin.get(), x, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
+      S.apply(precision == FFTSVD_PREC_FP64 ? FFTSVD_PREC_FP64 : FFTSVD_PREC_FP32, S.xin.get(), S.w.get());
+      FFTSVD_CUDA(cudaMemcpyAsync(y, S.w.get(), sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   });
+}
+
+int fftsvd_b200_precond_solve(fftsvd_surface* s, const double* r, double* z) {
+   if (!s || !r || !z) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      Surface& S = s->s;
+      FFTSVD_CUDA(cudaMemcpyAsync(S.xin.get(), r, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
+      S.precond.apply(S.xin.get(), S.w.get(), S.stream);
+      FFTSVD_CUDA(cudaMemcpyAsync(z, S.w.get(), sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   });
+}
+
+int fftsvd_b200_solve_device(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
+                             int32_t max_iterations, fftsvd_solve_info* info) {
+   if (!s || !rhs || !sol) return FFTSVD_ERR_ARGUMENT;
+   int status = FFTSVD_OK;
+   int rc = guarded([&] { status = s->s.solve(precision, rhs, sol, tol, max_iterations, info); });
+   if (rc != FFTSVD_OK) return rc;
+   if (status != FFTSVD_OK)
+      set_last_error(status == FFTSVD_ERR_NOT_CONVERGED ? "GMRES reached the iteration cap above tolerance"
+                                                        : "non-finite value in the right-hand side or an iterate");
+   return status;
+}
+
+int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
+                      int32_t max_iterations, fftsvd_solve_info* info) {
+   if (!s || !rhs || !sol) return FFTSVD_ERR_ARGUMENT;
+   int status = FFTSVD_OK;
+   int rc = guarded([&] {
+      Surface& S = s->s;
+      FFTSVD_CUDA(cudaMemcpyAsync(S.xin.get(), rhs, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
+      status = S.solve(precision, S.xin.get(), S.sold.get(), tol, max_iterations, info);
+      FFTSVD_CUDA(cudaMemcpyAsync(sol, S.sold.get(), sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   });
+   if (rc != FFTSVD_OK) return rc;
+   return status;
+}
+
+int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes) {
+   if (!s || !bytes) return FFTSVD_ERR_ARGUMENT;
+   const double es = precision == FFTSVD_PREC_FP64 ? 8.0 : 4.0;
+   *bytes = (double)s->s.operator_elems * es + (double)s->s.t_elems * es + 2.0 * s->s.n * 8.0;
+   return FFTSVD_OK;
+}
+
+}  // extern "C"

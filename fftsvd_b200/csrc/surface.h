@@ -1,0 +1,65 @@
+// The surface object behind the C-ABI: both operator precisions, the
+// block-diagonal preconditioner, the GMRES workspace and (optionally) the
+// panel geometry and point charges used by the right-hand side and the
+// reaction-potential collection.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "gmres.cuh"
+#include "operator.h"
+
+namespace fftsvd {
+
+struct PanelGeometry;  // nbody.h
+
+struct Preconditioner {
+   int nblocks = 0;
+   DevBuf<int32_t> blk_ptr, blk_idx;
+   DevBuf<int64_t> inv_off;
+   DevBuf<double> inv;
+   void build(const fftsvd_precond_csc& P, int n);  // host factorisation into dense block inverses
+   void apply(const double* r, double* z, cudaStream_t s) const;
+};
+
+struct Surface {
+   int n = 0;  // unknowns
+   cudaStream_t stream = nullptr;
+   DeviceOperator<double> op64;
+   DeviceOperator<float> op32;
+   Preconditioner precond;
+   int64_t operator_elems = 0, t_elems = 0;
+   double eps_in = 1.0;
+   // inner region (interior, Laplace) tree panel -> unknown rows, for RHS and collection
+   std::vector<int32_t> inner_phi_row, inner_dphi_row;
+   std::shared_ptr<PanelGeometry> geom;
+   int num_charges = 0;
+   DevBuf<double> charge_pos, charge_q;
+   std::vector<double> charge_q_host;
+
+   // GMRES workspace
+   int capacity = 0;  // basis vectors
+   DevBuf<double> V, H, cs, sn, g, h1, h2, partial, normpart, y;
+   DevBuf<double> w, r, t0, t1, t2, xin, xout, sold, scal;
+   DevBuf<GivensState> st;
+   GivensState* st_host = nullptr;
+
+   ~Surface();
+   void ensure_capacity(int nvec);
+   void apply(int precision, const double* x, double* y);
+   double pnorm(const double* v);  // ||v|| on device, synchronous
+   // Left-preconditioned un-restarted GMRES (GMRES.c:446-539) with operator `precision`;
+   // x overwritten.  Returns iterations; residual via *res.
+   int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status);
+   int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
+};
+
+}  // namespace fftsvd
+
+struct fftsvd_surface {
+   fftsvd::Surface s;
+};

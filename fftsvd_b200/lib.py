@@ -1,0 +1,92 @@
+"""ctypes binding of libfftsvd_b200.so (the in-tree CUDA library).
+
+The library is required: importing this module on a machine without the
+built .so raises immediately, and every call that needs a GPU fails with
+FFTSVDError(FFTSVD_ERR_NO_DEVICE) instead of falling back to host code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import PrecondCSC, Problem, RegionMap, SolveInfo, TreeFlat
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfftsvd_b200.so")
+
+_f64p = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+
+# every symbol declared in include/fftsvd_b200.h
+EXPORTED = [
+    "fftsvd_b200_last_error", "fftsvd_b200_version", "fftsvd_b200_surface_create",
+    "fftsvd_b200_surface_create_flat", "fftsvd_b200_surface_free", "fftsvd_b200_surface_num_unknowns",
+    "fftsvd_b200_matvec", "fftsvd_b200_matvec_device", "fftsvd_b200_precond_solve", "fftsvd_b200_solve",
+    "fftsvd_b200_solve_device", "fftsvd_b200_set_geometry", "fftsvd_b200_rhs", "fftsvd_b200_rhs_device",
+    "fftsvd_b200_reaction_potentials", "fftsvd_b200_reaction_potentials_device", "fftsvd_b200_energy",
+    "fftsvd_b200_matvec_bytes", "solveSurfaceOperator", "generateRHS",
+]
+
+
+class FFTSVDError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m fftsvd_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    lib.fftsvd_b200_last_error.restype = C.c_char_p
+    lib.fftsvd_b200_version.restype = C.c_int
+    sp = C.c_void_p
+    lib.fftsvd_b200_surface_create.argtypes = [C.POINTER(Problem), C.POINTER(sp)]
+    lib.fftsvd_b200_surface_create_flat.argtypes = [C.c_int32, C.c_int32, C.POINTER(TreeFlat), C.POINTER(RegionMap),
+                                                    C.POINTER(PrecondCSC), C.c_int32, _f64p, _f64p, C.c_double,
+                                                    C.POINTER(sp)]
+    lib.fftsvd_b200_surface_free.argtypes = [sp]
+    lib.fftsvd_b200_surface_num_unknowns.argtypes = [sp]
+    lib.fftsvd_b200_surface_num_unknowns.restype = C.c_int32
+    for name in ("fftsvd_b200_matvec", "fftsvd_b200_matvec_device"):
+        getattr(lib, name).argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.fftsvd_b200_precond_solve.argtypes = [sp, _f64p, _f64p]
+    for name in ("fftsvd_b200_solve", "fftsvd_b200_solve_device"):
+        getattr(lib, name).argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
+                                       C.POINTER(SolveInfo)]
+    lib.fftsvd_b200_set_geometry.argtypes = [sp, C.c_int32, _f64p, _i32p, _i32p]
+    lib.fftsvd_b200_rhs.argtypes = [sp, _f64p]
+    lib.fftsvd_b200_rhs_device.argtypes = [sp, C.c_void_p]
+    lib.fftsvd_b200_reaction_potentials.argtypes = [sp, _f64p, _f64p]
+    lib.fftsvd_b200_reaction_potentials_device.argtypes = [sp, C.c_void_p, C.c_void_p]
+    lib.fftsvd_b200_energy.argtypes = [sp, _f64p, _f64p]
+    lib.fftsvd_b200_matvec_bytes.argtypes = [sp, C.c_int32, _f64p]
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != _abi.FFTSVD_OK:
+        msg = load().fftsvd_b200_last_error()
+        raise FFTSVDError(rc, msg.decode() if msg else "")
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def ptr(a: np.ndarray, ctype=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ctype))

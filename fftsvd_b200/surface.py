@@ -1,0 +1,267 @@
+"""Host-side mirror of the reference PBE operator interface (FFTSVDpbeAPI.h:125-157).
+
+``Surface`` owns one device-resident two-region PBE operator.  The
+module-level functions keep the reference names and argument meaning:
+
+    generateSurfaceOperator(panels, charges, ...) -> Surface     (FFTSVDpbeAPI.c:1053)
+    generateRHS(surface) -> rhs[2N]                              (FFTSVDpbeAPI.c:1871)
+    solveSurfaceOperator(surface, rhs, tol) -> solution[2N]      (FFTSVDpbeAPI.c:1884)
+    collectPotentials(surface, solution) -> potentials (kT/e)    (FFTSVDpbeAPI.c:1896)
+
+Where the reference calls exit() on failure (FFTSVDpbeAPI.c:38-50) these raise
+FFTSVDError with the library's status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import PrecondCSC, Problem, RegionMap, SolveInfo, numpy_to_tree_flat
+from .lib import check, f64, i32, load, ptr
+
+KT_CONVERSION = 561.0       # FFTSVDpbeAPI.h:13
+DEBYE_CONSTANT = 3.047      # FFTSVDpbeAPI.h:14
+COULOMB_KCAL = 332.112      # FFTSVDsalt.c:170
+
+PRECISIONS = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED, "fp32": _abi.PREC_FP32}
+
+
+def _prec(p) -> int:
+    return PRECISIONS[p] if isinstance(p, str) else int(p)
+
+
+@dataclass
+class SolveResult:
+    solution: np.ndarray
+    iterations: int
+    refinements: int
+    residual: float
+    status: int
+    solve_ms: float
+
+
+def two_region_maps(n: int, eps_in: float, eps_out: float):
+    """Region maps of the single-molecule PBE operator (SurfaceOperator.c:51-158).
+
+    Unknowns x = [phi(0..n-1); dphi(0..n-1)].  Tree 0 is the exterior region
+    (no own panels, its child's panels enter with phi -> -phi,
+    dphi -> eps_in/eps_out dphi, result to the dphi rows, plus the -4 pi phi
+    jump); tree 1 is the interior region (phi -> phi, dphi -> -dphi, result to
+    the phi rows).
+    """
+    k = np.arange(n, dtype=np.int32)
+    outer = dict(phi_index=k, phi_scale=np.full(n, -1.0), dphi_index=k + n,
+                 dphi_scale=np.full(n, eps_in / eps_out), out_index=k + n, jump=np.full(n, -4.0 * np.pi))
+    inner = dict(phi_index=k, phi_scale=np.ones(n), dphi_index=k + n, dphi_scale=np.full(n, -1.0),
+                 out_index=k, jump=np.zeros(n))
+    return [outer, inner]
+
+
+def two_region_precond(diag_single: np.ndarray, diag_double: np.ndarray, rel_eps: float):
+    """Per-panel 2x2 preconditioner blocks (SurfaceOperator.c:170-197) in CSC form.
+
+    Rows/columns (phi_i, dphi_i):  [[Dd, -Ds], [Dd, rel_eps * Ds]] with the
+    interior tree's self terms Ds = D_single(i,i), Dd = D_double(i,i).
+    """
+    n = len(diag_single)
+    col_ptr = np.arange(0, 4 * n + 1, 2, dtype=np.int32)
+    rows = np.empty(4 * n, dtype=np.int32)
+    vals = np.empty(4 * n)
+    i = np.arange(n)
+    # column phi_i: rows phi_i, dphi_i
+    rows[2 * i] = i
+    rows[2 * i + 1] = n + i
+    vals[2 * i] = diag_double
+    vals[2 * i + 1] = diag_double
+    # column dphi_i: rows phi_i, dphi_i
+    rows[2 * (n + i)] = i
+    rows[2 * (n + i) + 1] = n + i
+    vals[2 * (n + i)] = -diag_single
+    vals[2 * (n + i) + 1] = rel_eps * diag_single
+    return dict(n=2 * n, col_ptr=col_ptr, row_index=rows, value=vals)
+
+
+def leaf_diagonals(tree: dict):
+    """Self terms D(i,i) of every panel from a flat tree (Cube.c:2349-2390)."""
+    n = tree["num_points"]
+    ds = np.zeros(n)
+    dd = np.zeros(n)
+    rp, cp, dp = tree["leaf_row_ptr"], tree["leaf_col_ptr"], tree["leaf_d_ptr"]
+    for l in range(tree["num_leaves"]):
+        nr = rp[l + 1] - rp[l]
+        nc = cp[l + 1] - cp[l]
+        rows = tree["leaf_rows"][rp[l]:rp[l + 1]]
+        blk_s = tree["d_single"][dp[l]:dp[l + 1]].reshape(nr, nc)
+        blk_d = tree["d_double"][dp[l]:dp[l + 1]].reshape(nr, nc)
+        r = np.arange(nr)
+        ds[rows] = blk_s[r, r]
+        dd[rows] = blk_d[r, r]
+    return ds, dd
+
+
+class Surface:
+    """A device-resident PBE surface operator (both FP32 and FP64 copies)."""
+
+    def __init__(self, handle, n_unknowns: int, keep=None, num_charges: int = 0, eps_in: float = 1.0):
+        self._h = handle
+        self.n = n_unknowns
+        self._keep = keep
+        self.num_charges = num_charges
+        self.eps_in = eps_in
+
+    # ---- construction
+    @classmethod
+    def from_flat(cls, trees, maps, precond, charge_pos=None, charge=None, eps_in=1.0, vertices=None,
+                  geometry_rows=None):
+        lib = load()
+        n_unknowns = int(precond["n"])
+        keep = []
+        tf = (_abi.TreeFlat * len(trees))()
+        for i, t in enumerate(trees):
+            s, k = numpy_to_tree_flat(t)
+            tf[i] = s
+            keep.append(k)
+        rm = (RegionMap * len(maps))()
+        for i, m in enumerate(maps):
+            arrs = {"phi_index": i32(m["phi_index"]), "phi_scale": f64(m["phi_scale"]),
+                    "dphi_index": i32(m["dphi_index"]), "dphi_scale": f64(m["dphi_scale"]),
+                    "out_index": i32(m["out_index"]), "jump": f64(m["jump"])}
+            keep.append(arrs)
+            rm[i] = RegionMap(ptr(arrs["phi_index"], C.c_int32), ptr(arrs["phi_scale"]),
+                              ptr(arrs["dphi_index"], C.c_int32), ptr(arrs["dphi_scale"]),
+                              ptr(arrs["out_index"], C.c_int32), ptr(arrs["jump"]))
+        pc = {"col_ptr": i32(precond["col_ptr"]), "row_index": i32(precond["row_index"]),
+              "value": f64(precond["value"])}
+        keep.append(pc)
+        P = PrecondCSC(n_unknowns, ptr(pc["col_ptr"], C.c_int32), ptr(pc["row_index"], C.c_int32), ptr(pc["value"]))
+        nq = 0 if charge is None else len(charge)
+        qp = f64(charge_pos if nq else np.zeros((1, 3)))
+        qv = f64(charge if nq else np.zeros(1))
+        h = C.c_void_p()
+        check(lib.fftsvd_b200_surface_create_flat(n_unknowns, len(trees), tf, rm, C.byref(P), nq, ptr(qp), ptr(qv),
+                                                  float(eps_in), C.byref(h)))
+        s = cls(h, n_unknowns, None, nq, eps_in)
+        if vertices is not None:
+            vv = f64(vertices)
+            npan = len(vv)
+            if geometry_rows is None:
+                geometry_rows = (np.arange(npan), np.arange(npan) + npan)
+            pr, dr = i32(geometry_rows[0]), i32(geometry_rows[1])
+            check(lib.fftsvd_b200_set_geometry(h, npan, ptr(vv), ptr(pr, C.c_int32), ptr(dr, C.c_int32)))
+        return s
+
+    @classmethod
+    def from_problem(cls, vertices, charge_pos, charge, eps_in, eps_out, kappa, svd_tol=1e-5,
+                     max_panels_per_leaf=32, grid_points=4, num_threads=0):
+        """Own host setup (octree, panel integrals, sampled SVD bases, translation operators)."""
+        lib = load()
+        vv, qp, qv = f64(vertices), f64(charge_pos), f64(charge)
+        p = Problem(len(vv), ptr(vv), len(qv), ptr(qp), ptr(qv), float(eps_in), float(eps_out), float(kappa),
+                    float(svd_tol), int(max_panels_per_leaf), int(grid_points), int(num_threads))
+        h = C.c_void_p()
+        check(lib.fftsvd_b200_surface_create(C.byref(p), C.byref(h)))
+        return cls(h, 2 * len(vv), None, len(qv), eps_in)
+
+    def close(self):
+        if self._h:
+            load().fftsvd_b200_surface_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- operations (host arrays)
+    def matvec(self, x, precision="fp32"):
+        x = f64(x)
+        y = np.empty(self.n)
+        check(load().fftsvd_b200_matvec(self._h, _prec(precision), x.ctypes.data, y.ctypes.data))
+        return y
+
+    def precond_solve(self, r):
+        r = f64(r)
+        z = np.empty(self.n)
+        check(load().fftsvd_b200_precond_solve(self._h, ptr(r), ptr(z)))
+        return z
+
+    def solve(self, rhs, precision="mixed", tol=1e-6, max_iterations=1000, raise_on_error=True) -> SolveResult:
+        rhs = f64(rhs)
+        sol = np.empty(self.n)
+        info = SolveInfo()
+        rc = load().fftsvd_b200_solve(self._h, _prec(precision), rhs.ctypes.data, sol.ctypes.data, float(tol),
+                                      int(max_iterations), C.byref(info))
+        if raise_on_error:
+            check(rc)
+        return SolveResult(sol, info.iterations, info.refinements, info.residual, rc, info.solve_ms)
+
+    def rhs(self):
+        r = np.empty(self.n)
+        check(load().fftsvd_b200_rhs(self._h, ptr(r)))
+        return r
+
+    def reaction_potentials(self, solution):
+        s = f64(solution)
+        phi = np.empty(self.num_charges)
+        check(load().fftsvd_b200_reaction_potentials(self._h, ptr(s), ptr(phi)))
+        return phi
+
+    def energy(self, phi):
+        phi = f64(phi)
+        e = C.c_double()
+        check(load().fftsvd_b200_energy(self._h, ptr(phi), C.byref(e)))
+        return e.value
+
+    def matvec_bytes(self, precision="fp32") -> float:
+        b = C.c_double()
+        check(load().fftsvd_b200_matvec_bytes(self._h, _prec(precision), C.byref(b)))
+        return b.value
+
+    # ---- operations on device pointers (torch tensors or raw ints)
+    def matvec_device(self, x_ptr: int, y_ptr: int, precision="fp32"):
+        check(load().fftsvd_b200_matvec_device(self._h, _prec(precision), C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
+
+    def solve_device(self, rhs_ptr: int, sol_ptr: int, precision="mixed", tol=1e-6, max_iterations=1000):
+        info = SolveInfo()
+        rc = load().fftsvd_b200_solve_device(self._h, _prec(precision), C.c_void_p(rhs_ptr), C.c_void_p(sol_ptr),
+                                             float(tol), int(max_iterations), C.byref(info))
+        check(rc)
+        return info
+
+    def rhs_device(self, rhs_ptr: int):
+        check(load().fftsvd_b200_rhs_device(self._h, C.c_void_p(rhs_ptr)))
+
+    def reaction_potentials_device(self, sol_ptr: int, phi_ptr: int):
+        check(load().fftsvd_b200_reaction_potentials_device(self._h, C.c_void_p(sol_ptr), C.c_void_p(phi_ptr)))
+
+
+# ---- reference-named entry points
+
+def generateSurfaceOperator(vertices, charge_pos, charge, innerdielectric, outerdielectric, ionicstrength=0.0,
+                            svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4) -> Surface:
+    """Two-region PBE operator; kappa = sqrt(I)/3.047 as in FFTSVDpbeAPI.c:1060."""
+    kappa = np.sqrt(ionicstrength) / DEBYE_CONSTANT if ionicstrength > 0 else 0.0
+    return Surface.from_problem(vertices, charge_pos, charge, innerdielectric, outerdielectric, kappa, svd_tol,
+                                max_panels_per_leaf, grid_points)
+
+
+def generateRHS(surface: Surface) -> np.ndarray:
+    return surface.rhs()
+
+
+def solveSurfaceOperator(surface: Surface, rhs, errortolerance=1e-6, precision="mixed") -> np.ndarray:
+    return surface.solve(rhs, precision=precision, tol=errortolerance).solution
+
+
+def collectPotentials(surface: Surface, solution) -> np.ndarray:
+    """Reaction potentials at the charges in kT/e (KT_CONVERSION * phi / eps_in)."""
+    return KT_CONVERSION * surface.reaction_potentials(solution) / surface.eps_in
+
+
+def solvation_energy(surface: Surface, solution) -> float:
+    """0.5 * sum q phi_reac * 332.112 / eps_in in kcal/mol."""
+    return surface.energy(surface.reaction_potentials(solution))

@@ -179,10 +179,6 @@ int fftsvd_b200_matvec_device(fftsvd_surface* s, int32_t precision, const double
 /* z = P^-1 r.  Preconditioner_solve (Preconditioner.c:272-294).  Host pointers. */
 int fftsvd_b200_precond_solve(fftsvd_surface* s, const double* r, double* z);
 
-/* One tree's b = S xs + D xd.  Tree_multiplyboth (Tree.c:597-683).  Host pointers. */
-int fftsvd_b200_tree_multiplyboth(fftsvd_surface* s, int32_t tree, int32_t precision, const double* xs,
-                                  const double* xd, double* b);
-
 /* GMRES solve of A x = rhs (GMRES.c:446-539).  Host pointers. */
 int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
                       int32_t max_iterations, fftsvd_solve_info* info);
@@ -190,17 +186,25 @@ int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, d
 int fftsvd_b200_solve_device(fftsvd_surface* s, int32_t precision, const double* rhs, double* sol, double tol,
                              int32_t max_iterations, fftsvd_solve_info* info);
 
+/* Attach the panel geometry of the charge-bearing region to a surface built
+   with fftsvd_b200_surface_create_flat: vertices as in fftsvd_problem, and for
+   each panel the unknown rows of its phi and dphi/dn. */
+int fftsvd_b200_set_geometry(fftsvd_surface* s, int32_t num_panels, const double* vertices, const int32_t* phi_row,
+                             const int32_t* dphi_row);
+
 /* rhs[i] = sum_j q_j / |x_j - c_i| on the interior rows (SurfaceOperator.c:291-321). */
 int fftsvd_b200_rhs(fftsvd_surface* s, double* rhs);
+int fftsvd_b200_rhs_device(fftsvd_surface* s, double* rhs);
 /* Reaction potential at every charge from a surface solution
    (SurfaceOperator.c:364-396, direct analytic panel integrals). */
 int fftsvd_b200_reaction_potentials(fftsvd_surface* s, const double* sol, double* phi);
+int fftsvd_b200_reaction_potentials_device(fftsvd_surface* s, const double* sol, double* phi);
 /* 0.5 * sum q phi * 332.112 / eps_in (FFTSVDsalt.c:167-170). */
 int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
 
-/* Timing of the last device operations, for benchmarks: milliseconds of the
-   last matvec stages [near, far_forward, far_translate] and the algorithmic
-   byte count of one matvec at the given precision. */
+/* Algorithmic bytes of one matvec at the given precision: compressed operator
+   (D, VT, PV, UTI, U) at the stored element size, unique translation tables,
+   and the FP64 input and output vectors. */
 int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes);
 
 /* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ---- */
