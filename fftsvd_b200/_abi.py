@@ -70,6 +70,12 @@ class SolveInfo(C.Structure):
                 ("residual", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
 
 
+class SurfaceStats(C.Structure):
+    _fields_ = [("depth", C.c_int32 * 2), ("num_leaves", C.c_int32 * 2), ("num_cubes", C.c_int32 * 2),
+                ("setup_ms", C.c_double * 4), ("device_bytes", C.c_double), ("matvec_bytes_fp32", C.c_double),
+                ("matvec_bytes_fp64", C.c_double)]
+
+
 # field name -> (count expression, dtype) used to copy a TreeFlat into numpy arrays
 def tree_flat_to_numpy(t: TreeFlat) -> dict:
     """Copy every array of a TreeFlat into owned numpy arrays (dict keyed by field name)."""

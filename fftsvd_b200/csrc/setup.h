@@ -1,0 +1,105 @@
+// Host setup of the compressed FFTSVD operator (see setup.cpp).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/fftsvd_b200.h"
+#include "integrals.h"
+
+namespace fftsvd {
+namespace setup {
+
+struct Kernel {
+   bool yukawa = false;
+   double kappa = 0.0;
+   void panel(const double* point, const FlatPanel& p, double* slp, double* dlp) const;
+   double point(const double* dest, const double* src) const;
+};
+
+struct Cube {
+   int level = 0;
+   int idx[3] = {0, 0, 0};
+   double b0[3] = {0, 0, 0}, b1[3] = {0, 0, 0}, center[3] = {0, 0, 0};
+   int parent = -1;
+   bool leaf = false;
+   int child[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+   std::vector<int> panels, points, local, inter, dcols;
+   std::vector<double> Ds, Dd;        // near-field blocks, points x dcols
+   int rowrank = 0, colrank = 0;
+   std::vector<double> VT, U;         // rowrank x panels, points x colrank
+   std::vector<double> PVs, PVd, UTI; // n^3 x rowrank (x2), colrank x n^3
+};
+
+// Owned flat arrays of one tree; view() exposes them as fftsvd_tree_flat.
+struct FlatTree {
+   int num_panels = 0, num_points = 0, depth = 0, num_cubes = 0;
+   std::vector<int> grid;
+   std::vector<int32_t> leaf_row_ptr, leaf_rows, leaf_col_ptr, leaf_cols;
+   std::vector<int64_t> leaf_d_ptr;
+   std::vector<double> d_single, d_double;
+   std::vector<int32_t> cube_level, cube_index, cube_panel_ptr, cube_panels, cube_point_ptr, cube_points;
+   std::vector<int32_t> cube_row_rank, cube_col_rank, inter_ptr, inter_cubes;
+   std::vector<int64_t> cube_vt_ptr, cube_pv_ptr, cube_uti_ptr, cube_u_ptr, t_level_ptr;
+   std::vector<double> vt, pv_single, pv_double, uti, u, t_ops;
+   void view(fftsvd_tree_flat& t) const;
+};
+
+struct Tree {
+   const std::vector<FlatPanel>* panels = nullptr;
+   const std::vector<double>* points = nullptr;  // 3 per point
+   Kernel kernel;
+   double eps = 1e-5;
+   int grid_points = 4;
+   int depth = 0;
+   std::vector<int> grid;
+   double bounds0[3] = {0, 0, 0}, bounds1[3] = {0, 0, 0};
+   double rootbox = 0.0;
+   std::vector<Cube> cubes;                  // cubes[0] is the root
+   std::vector<std::vector<double>> pinv;    // per level, n^3 x 49
+   std::vector<std::vector<double>> tops;    // per level, 343 slots x padded grid complex (re, im)
+
+   void build_cubes(int depth);
+   void choose_depth(int max_panels);
+   void make_lists();
+   void fill_near();
+   void fill_pinv();
+   void fill_T();
+   void fill_bases();
+   void flatten(FlatTree& F) const;
+};
+
+struct Timings {
+   double partition_ms = 0, near_ms = 0, pinv_t_ms = 0, bases_ms = 0;
+};
+
+Timings build_tree(Tree& T, int max_panels);
+
+// The complete host-side product for one molecule: both region trees in flat
+// form, the region maps and the preconditioner entries.
+struct HostOperator {
+   int n = 0;
+   double eps_in = 1, eps_out = 1, kappa = 0;
+   std::vector<FlatPanel> panels;
+   std::vector<double> points;
+   FlatTree flat[2];
+   fftsvd_tree_flat views[2];
+   int depth[2] = {0, 0};
+   Timings tm[2];
+   std::vector<int32_t> idx_phi, idx_dphi, out_outer;
+   std::vector<double> m1, ratio, jump, one, zero;
+   fftsvd_region_map maps[2];
+   std::vector<int32_t> col_ptr, rows;
+   std::vector<double> vals;
+   fftsvd_precond_csc precond;
+};
+
+// Build the two-region operator on the host (no GPU involved).
+void host_setup(const fftsvd_problem& pr, HostOperator& H);
+
+int column_basis(const std::vector<double>& A, int rows, int cols, double eps, std::vector<double>& Q);
+int row_basis(const std::vector<double>& A, int rows, int cols, double eps, std::vector<double>& VT);
+void pseudoinverse(const std::vector<double>& X, int rows, int cols, std::vector<double>& XI);
+
+}  // namespace setup
+}  // namespace fftsvd

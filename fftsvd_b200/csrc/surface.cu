@@ -286,7 +286,7 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
    return status;
 }
 
-static void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
+void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
                          const fftsvd_region_map* maps, const fftsvd_precond_csc* P) {
    int ndev = 0;
    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

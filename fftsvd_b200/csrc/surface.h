@@ -41,6 +41,9 @@ struct Surface {
    DevBuf<double> charge_pos, charge_q;
    std::vector<double> charge_q_host;
 
+   // setup statistics (zero for surfaces built from a flat operator)
+   fftsvd_surface_stats stats{};
+
    // GMRES workspace
    int capacity = 0;  // basis vectors
    DevBuf<double> V, H, cs, sn, g, h1, h2, partial, normpart, y;
@@ -57,6 +60,9 @@ struct Surface {
    int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status);
    int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
 };
+
+void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
+                  const fftsvd_region_map* maps, const fftsvd_precond_csc* P);
 
 }  // namespace fftsvd
 

@@ -239,6 +239,34 @@ class Surface:
         check(load().fftsvd_b200_reaction_potentials_device(self._h, C.c_void_p(sol_ptr), C.c_void_p(phi_ptr)))
 
 
+def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4,
+                  num_threads=0):
+    """Run only the host setup (no GPU): returns ([exterior tree, interior tree], preconditioner) as numpy."""
+    lib = load()
+    vv = f64(vertices)
+    zero3, zero1 = np.zeros(3), np.zeros(1)
+    p = Problem(len(vv), ptr(vv), 0, ptr(zero3), ptr(zero1), float(eps_in), float(eps_out), float(kappa),
+                float(svd_tol), int(max_panels_per_leaf), int(grid_points), int(num_threads))
+    h = C.c_void_p()
+    check(lib.fftsvd_b200_host_setup(C.byref(p), C.byref(h)))
+    try:
+        trees = []
+        for t in range(2):
+            tf = _abi.TreeFlat()
+            check(lib.fftsvd_b200_host_operator_tree(h, t, C.byref(tf)))
+            trees.append(_abi.tree_flat_to_numpy(tf))
+        pc = PrecondCSC()
+        check(lib.fftsvd_b200_host_operator_precond(h, C.byref(pc)))
+        n = pc.n
+        col_ptr = np.ctypeslib.as_array(pc.col_ptr, shape=(n + 1,)).copy()
+        nnz = int(col_ptr[-1])
+        pre = dict(n=n, col_ptr=col_ptr, row_index=np.ctypeslib.as_array(pc.row_index, shape=(nnz,)).copy(),
+                   value=np.ctypeslib.as_array(pc.value, shape=(nnz,)).copy())
+    finally:
+        lib.fftsvd_b200_host_operator_free(h)
+    return trees, pre
+
+
 # ---- reference-named entry points
 
 def generateSurfaceOperator(vertices, charge_pos, charge, innerdielectric, outerdielectric, ionicstrength=0.0,

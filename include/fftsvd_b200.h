@@ -144,6 +144,16 @@ typedef struct {
 typedef struct fftsvd_surface fftsvd_surface;
 
 typedef struct {
+   int32_t depth[2];              /* partitioning levels of the exterior and interior trees */
+   int32_t num_leaves[2];
+   int32_t num_cubes[2];          /* cubes with a non-empty interaction list */
+   double setup_ms[4];            /* partition + lists, near field, pinv + translation operators, bases */
+   double device_bytes;           /* resident operator bytes, both precisions */
+   double matvec_bytes_fp32;      /* algorithmic bytes of one matvec, FP32 operator */
+   double matvec_bytes_fp64;      /* algorithmic bytes of one matvec, FP64 operator */
+} fftsvd_surface_stats;
+
+typedef struct {
    int32_t iterations;            /* total inner GMRES iterations */
    int32_t refinements;           /* outer FP64 refinement steps (mixed mode) */
    int32_t status;
@@ -162,6 +172,15 @@ int fftsvd_b200_version(void);
    generateSurfaceOperatorPreconditioner (FFTSVDpbeAPI.c:1053-1739,1853-1861). */
 int fftsvd_b200_surface_create(const fftsvd_problem* problem, fftsvd_surface** out);
 
+/* The same host setup without any device work: the two region trees in flat
+   form (tree 0 exterior, tree 1 interior) and the preconditioner entries.
+   The views stay valid until fftsvd_b200_host_operator_free. */
+typedef struct fftsvd_host_operator fftsvd_host_operator;
+int fftsvd_b200_host_setup(const fftsvd_problem* problem, fftsvd_host_operator** out);
+int fftsvd_b200_host_operator_tree(const fftsvd_host_operator* op, int32_t tree, fftsvd_tree_flat* view);
+int fftsvd_b200_host_operator_precond(const fftsvd_host_operator* op, fftsvd_precond_csc* out);
+void fftsvd_b200_host_operator_free(fftsvd_host_operator* op);
+
 /* Upload an operator given in flat form (one tree per region). */
 int fftsvd_b200_surface_create_flat(int32_t num_unknowns, int32_t num_trees, const fftsvd_tree_flat* trees,
                                     const fftsvd_region_map* maps, const fftsvd_precond_csc* precond,
@@ -170,6 +189,7 @@ int fftsvd_b200_surface_create_flat(int32_t num_unknowns, int32_t num_trees, con
 
 void fftsvd_b200_surface_free(fftsvd_surface* s);
 int32_t fftsvd_b200_surface_num_unknowns(const fftsvd_surface* s);
+int fftsvd_b200_surface_stats(const fftsvd_surface* s, fftsvd_surface_stats* out);
 
 /* y = A x.  SurfaceOperator_topmultiply (SurfaceOperator.c:90-97).  Host pointers. */
 int fftsvd_b200_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y);
