@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: PBE solve ms and matvec GB/s on B200 (mixed FP32/FP64 vs FP64).
+
+Workload (default): the synthetic protein-like blob — level-6 icosphere
+(81 920 flat panels) of radius 22 A displaced radially by seeded real spherical
+harmonics of degree <= 8 (15 % amplitude), 2 500 seeded charges uniform inside
+(>= 1.5 A from every panel centroid, U[-0.6, 0.6] e shifted to zero net),
+eps_in 4, eps_out 80, kappa 0.125 1/A, leaf <= 32 panels, grid 4, FFTSVD
+tolerance 1e-4, GMRES tolerance 1e-6.
+
+One step = one complete GMRES solve of A x = b with b resident in HBM
+(mixed: FP32 operator inside GMRES, FP64 residual refinement).  L2 is flushed
+(256 MiB write on the solve stream) before every timed step.  Prints one JSON
+line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config blob|born|large] [--no-cpu-baseline]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # the headline single-solve configuration
+    "blob": dict(name="blob L6 (81920 panels, R 22 A, 2500 charges, eps 4/80, kappa 0.125)", kind="blob",
+                 level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1),
+    "born": dict(name="Born ion L5 (20480 panels, R 10 A, +1 e, eps 1/80)", kind="born", level=5, radius=10.0,
+                 nq=1, eps_in=1.0, eps_out=80.0, kappa=0.0, seed=0),
+    "large": dict(name="large blob L7 (327680 panels, R 60 A, 30000 charges, eps 4/80, kappa 0.125)", kind="blob",
+                  level=7, radius=60.0, nq=30000, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=3),
+}
+SVD_TOL = 1e-4
+GMRES_TOL = 1e-6
+METRIC = "PBE solve ms & matvec GB/s, 40k-400k panels: mixed vs FP64 GPU at 1e-6 dG err"
+
+
+def make_workload(cfg):
+    from fftsvd_b200 import meshes
+    if cfg["kind"] == "born":
+        tri, qpos, q = meshes.born_ion(cfg["level"], cfg["radius"])
+    else:
+        tri = meshes.blob(cfg["level"], cfg["radius"], seed=cfg["seed"])
+        qpos, q = meshes.blob_charges(tri, cfg["radius"], cfg["nq"], seed=cfg["seed"] + 1, surface_seed=cfg["seed"])
+    return tri, qpos, q
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.rows = []
+        self.gpu = str(gpu_index)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for i, nm in enumerate(names):
+                    if r[5 + i].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier_max(value: float, ws: int) -> float:
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_solve(tri, qpos, q, cfg, threads):
+    """The reference CPU solve (compiled reference, OpenMP) of the same system: ms, iterations, dG."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available(False):
+        return None
+    ref.set_threads(threads)
+    t0 = time.time()
+    with ref.stdout_to_stderr():
+        rs = ref.RefSystem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    setup_s = time.time() - t0
+    rhs = rs.rhs()
+    t1 = time.perf_counter()
+    sol, it = rs.solve(rhs, GMRES_TOL)
+    solve_ms = (time.perf_counter() - t1) * 1e3
+    e = rs.energy(rs.reaction(sol))
+    rs.close()
+    return dict(solve_ms=solve_ms, iterations=it, dG=e, setup_s=setup_s)
+
+
+def run_reference(args, cfg, ws, rank):
+    if rank != 0:
+        return
+    tri, qpos, q = make_workload(cfg)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 2))  # each step is a full CPU solve of tens of seconds
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available(False):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfftsvd_ref.so is not built"}))
+        return
+    ref.set_threads(threads)
+    with ref.stdout_to_stderr():
+        rs = ref.RefSystem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    rhs = rs.rhs()
+    times = []
+    it = 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        sol, it = rs.solve(rhs, GMRES_TOL)
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = float(np.mean(times))
+    e = rs.energy(rs.reaction(sol))
+    sample = f"full GMRES solve to {GMRES_TOL} of the same system per step ({it} iterations), operator setup excluded"
+    line = {"metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+            "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": cfg["name"], "svd_tol": SVD_TOL, "gmres_tol": GMRES_TOL,
+                       "panels": len(tri), "charges": len(q)},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "iterations": it, "dG_kcal": e}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, ws, rank, local):
+    import torch
+    from fftsvd_b200 import _abi
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface
+
+    torch.cuda.set_device(local)
+    lib = load()
+    tri, qpos, q = make_workload(cfg)
+    t0 = time.time()
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    setup_s = time.time() - t0
+    st = _abi.SurfaceStats()
+    lib.fftsvd_b200_surface_stats(s._h, C.byref(st))
+    n = s.n
+    stream = torch.cuda.ExternalStream(lib.fftsvd_b200_surface_stream(s._h))
+    rhs = torch.empty(n, dtype=torch.float64, device="cuda")
+    s.rhs_device(rhs.data_ptr())
+    torch.cuda.synchronize()
+    sol = torch.empty_like(rhs)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+
+    def timed_solves(precision, k, warm):
+        for _ in range(warm):
+            s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
+        total = 0.0
+        info = None
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total, info
+
+    barrier(ws)
+    torch.cuda.synchronize()
+    launches0 = lib.fftsvd_b200_launch_count()
+    with ClockSampler(local) as clk:
+        t_mixed, info_mixed = timed_solves("mixed", args.steps, args.warmup)
+    launches = lib.fftsvd_b200_launch_count() - launches0 - 0
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_max = barrier_max(t_mixed, ws)
+    ms_per_step = t_max / args.steps
+    value = t_max / (args.steps * ws)
+    x_mixed = sol.cpu().numpy()
+
+    # plain FP64 GPU solve of the same system (the comparison the target is stated against)
+    k64 = max(1, args.steps // 2)
+    t64, info64 = timed_solves("fp64", k64, 1)
+    x64 = sol.cpu().numpy()
+    fp64_ms = t64 / k64
+    e_mixed = s.energy(s.reaction_potentials(x_mixed))
+    e64 = s.energy(s.reaction_potentials(x64))
+
+    # matvec: per-kernel CUDA-event times on the library stream, algorithmic bytes per kernel
+    xv = torch.randn(n, dtype=torch.float64, device="cuda")
+    yv = torch.empty_like(xv)
+    kernels = ["join", "far_forward", "far_backward", "near"]
+    prof = {}
+    for prec, pid in (("fp32", _abi.PREC_FP32), ("fp64", _abi.PREC_FP64)):
+        ms4 = (C.c_double * 4)()
+        b4 = (C.c_double * 4)()
+        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 3, ms4)
+        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 20, ms4)
+        lib.fftsvd_b200_matvec_kernel_bytes(s._h, pid, b4)
+        prof[prec] = {k: {"ms": ms4[i], "bytes": b4[i], "gbs": b4[i] / (ms4[i] * 1e6) if ms4[i] > 0 else None}
+                      for i, k in enumerate(kernels)}
+        prof[prec]["total_ms"] = sum(ms4[i] for i in range(4))
+    mv_bytes32 = st.matvec_bytes_fp32
+    mv_bytes64 = st.matvec_bytes_fp64
+
+    # e2e through the host-pointer C-ABI (pinned host buffers, copies inside the timed region)
+    rhs_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    sol_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    rhs_h.copy_(rhs.cpu())
+    infoC = _abi.SolveInfo()
+    e2e_total = 0.0
+    for i in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.fftsvd_b200_solve(s._h, _abi.PREC_MIXED, C.c_void_p(rhs_h.data_ptr()), C.c_void_p(sol_h.data_ptr()),
+                                   GMRES_TOL, 1000, C.byref(infoC))
+        e1.record(stream)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"solve failed: {rc}")
+        if i >= args.warmup:
+            e2e_total += e0.elapsed_time(e1)
+    e2e_ms = barrier_max(e2e_total, ws) / (args.steps * ws)
+
+    # roofline of the dominant kernel of the mixed solve's matvec (FP32 operator)
+    peak, peak_kind = hbm_peak()
+    dom = max(kernels, key=lambda k: prof["fp32"][k]["ms"])
+    ach = prof["fp32"][dom]["gbs"]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                tj = json.load(f)
+            ent = tj.get(cfg["kind"] + str(cfg["level"]), {}).get(dom)
+            if ent:
+                traffic = float(ent)
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_solve(tri, qpos, q, cfg, threads)
+        if r is not None:
+            cpu = {"value": r["solve_ms"], "unit": "ms", "cores": threads, "kind": "reference",
+                   "sample": f"the reference's full GMRES solve of the same system ({r['iterations']} iterations, "
+                             f"setup {r['setup_s']:.0f} s excluded), OpenMP build, dG {r['dG']:.6f} kcal/mol"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["name"], "panels": len(tri), "charges": len(q), "svd_tol": SVD_TOL,
+                       "gmres_tol": GMRES_TOL, "precision": "FP32 operator, FP64 Krylov + FP64 refinement",
+                       "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas x{ws}",
+                       "depth": list(st.depth), "leaves": list(st.num_leaves), "far_cubes": list(st.num_cubes)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": prof["fp32"][dom]["bytes"]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "fp64_solve_ms": fp64_ms, "speedup_mixed_vs_fp64": fp64_ms / (t_mixed / args.steps),
+            "iterations_mixed": info_mixed.iterations, "refinements_mixed": info_mixed.refinements,
+            "iterations_fp64": info64.iterations,
+            "dG_kcal_mixed": e_mixed, "dG_kcal_fp64": e64, "dG_rel_err_mixed_vs_fp64": abs(e_mixed - e64) / abs(e64),
+            "matvec_ms_fp32": prof["fp32"]["total_ms"], "matvec_ms_fp64": prof["fp64"]["total_ms"],
+            "matvec_gbs_fp32": mv_bytes32 / (prof["fp32"]["total_ms"] * 1e6),
+            "matvec_gbs_fp64": mv_bytes64 / (prof["fp64"]["total_ms"] * 1e6),
+            "matvec_kernels": prof, "setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=list(CONFIGS), default="blob")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, cfg, ws, rank)
+        else:
+            run_ours(args, cfg, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -31,7 +32,14 @@ void set_last_error(const std::string& msg);
          throw ::fftsvd::Error(FFTSVD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_)); \
    } while (0)
 
-#define FFTSVD_CHECK_LAUNCH() FFTSVD_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by this check, which also
+// counts the launch (fftsvd_b200_launch_count).
+extern std::atomic<long long> g_kernel_launches;
+#define FFTSVD_CHECK_LAUNCH()                                        \
+   do {                                                              \
+      ::fftsvd::g_kernel_launches.fetch_add(1, std::memory_order_relaxed); \
+      FFTSVD_CUDA(cudaGetLastError());                              \
+   } while (0)
 
 #define FFTSVD_REQUIRE(cond, msg)                                        \
    do {                                                                 \

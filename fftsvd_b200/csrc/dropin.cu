@@ -1,0 +1,313 @@
+// Drop-in replacements for the reference PBE API entry points
+// (FFTSVDpbeAPI.h:150,153) over a caller's reference-built SurfaceOperator:
+//
+//   solveSurfaceOperator  FFTSVDpbeAPI.c:1884-1888 -> GMRES_SurfaceOperator (GMRES.c:446-539)
+//   generateRHS           FFTSVDpbeAPI.c:1871-1876 -> SurfaceOperator_makeRHS (SurfaceOperator.c:291-321)
+//
+// The reference structures (layout in refabi.h) are read, never modified.  On
+// the first solve for a given (SurfaceOperator, Preconditioner) pair the
+// operator of every region tree is flattened and uploaded; later solves with
+// the same pair reuse the device copy, so the operator must not change between
+// calls.  Errors are reported on stderr and leave *solution / *rhs NULL instead
+// of exiting the process.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "refabi.h"
+#include "setup.h"
+#include "surface.h"
+
+// The reference keeps the GMRES tolerance in this process global
+// (FFTSVDpbeAPI.c:25); weak so that the library also links without it.
+extern "C" double errortolerance __attribute__((weak));
+
+namespace fftsvd {
+namespace {
+
+void collect_cubes(ref::Cube* c, std::vector<ref::Cube*>& all) {
+   if (!c) return;
+   all.push_back(c);
+   if (!c->leaf)
+      for (int x = 0; x < 2; x++)
+         for (int y = 0; y < 2; y++)
+            for (int z = 0; z < 2; z++) collect_cubes(c->children[x][y][z], all);
+}
+
+// Reference Tree/Cube objects -> flat arrays (the fields Tree_multiplyboth reads).
+void flatten_reference_tree(const ref::Tree* t, setup::FlatTree& F) {
+   FFTSVD_REQUIRE(t && t->root, "region without a tree");
+   FFTSVD_REQUIRE(t->partitioningdepth >= 1 && t->partitioningdepth <= FFTSVD_MAX_DEPTH, "tree depth out of range");
+   F = setup::FlatTree();
+   F.num_panels = (int)t->numpanels;
+   F.num_points = (int)t->numpoints;
+   F.depth = (int)t->partitioningdepth;
+   for (int d = 0; d < F.depth; d++) F.grid.push_back((int)t->gridpointsperlevel[d]);
+   std::vector<ref::Cube*> all;
+   collect_cubes(t->root, all);
+   std::map<const ref::Cube*, int> far_index;
+   for (ref::Cube* c : all) {
+      if (c->leaf && c->drows > 0 && c->dcolumns > 0) {
+         FFTSVD_REQUIRE(c->D_single && c->D_double, "leaf without near-field blocks");
+         F.leaf_row_ptr.push_back((int32_t)F.leaf_rows.size());
+         F.leaf_col_ptr.push_back((int32_t)F.leaf_cols.size());
+         F.leaf_d_ptr.push_back((int64_t)F.d_single.size());
+         for (unsigned i = 0; i < c->numpointindices; i++) F.leaf_rows.push_back((int32_t)c->pointindices[i]);
+         for (unsigned i = 0; i < c->numpanelindices; i++) F.leaf_cols.push_back((int32_t)c->panelindices[i]);
+         for (unsigned l = 0; l < c->numlocalcubes; l++)
+            for (unsigned j = 0; j < c->localcubes[l]->numpanelindices; j++)
+               F.leaf_cols.push_back((int32_t)c->localcubes[l]->panelindices[j]);
+         FFTSVD_REQUIRE(F.leaf_rows.size() - F.leaf_row_ptr.back() == c->drows, "leaf rows do not match drows");
+         FFTSVD_REQUIRE(F.leaf_cols.size() - F.leaf_col_ptr.back() == c->dcolumns, "leaf columns do not match dcolumns");
+         const size_t cnt = (size_t)c->drows * c->dcolumns;
+         F.d_single.insert(F.d_single.end(), c->D_single[0], c->D_single[0] + cnt);
+         F.d_double.insert(F.d_double.end(), c->D_double[0], c->D_double[0] + cnt);
+      }
+      if (c->numinteractingcubes > 0) far_index[c] = (int)far_index.size();
+   }
+   F.leaf_row_ptr.push_back((int32_t)F.leaf_rows.size());
+   F.leaf_col_ptr.push_back((int32_t)F.leaf_cols.size());
+   F.leaf_d_ptr.push_back((int64_t)F.d_single.size());
+   for (ref::Cube* c : all) {
+      if (c->numinteractingcubes == 0) continue;
+      const unsigned n = t->gridpointsperlevel[c->level], gp3 = n * n * n;
+      F.cube_level.push_back((int32_t)c->level);
+      for (int k = 0; k < 3; k++) F.cube_index.push_back((int32_t)c->indices[k]);
+      F.cube_panel_ptr.push_back((int32_t)F.cube_panels.size());
+      for (unsigned i = 0; i < c->numpanelindices; i++) F.cube_panels.push_back((int32_t)c->panelindices[i]);
+      F.cube_point_ptr.push_back((int32_t)F.cube_points.size());
+      for (unsigned i = 0; i < c->numpointindices; i++) F.cube_points.push_back((int32_t)c->pointindices[i]);
+      const bool src = c->numpanelindices > 0 && c->rowrank > 0 && c->VTsrc && c->PV_single && c->PV_double;
+      const bool dst = c->numpointindices > 0 && c->columnrank > 0 && c->Udest && c->UTI;
+      F.cube_row_rank.push_back(src ? (int32_t)c->rowrank : 0);
+      F.cube_col_rank.push_back(dst ? (int32_t)c->columnrank : 0);
+      F.cube_vt_ptr.push_back((int64_t)F.vt.size());
+      F.cube_pv_ptr.push_back((int64_t)F.pv_single.size());
+      F.cube_uti_ptr.push_back((int64_t)F.uti.size());
+      F.cube_u_ptr.push_back((int64_t)F.u.size());
+      if (src) {
+         F.vt.insert(F.vt.end(), c->VTsrc[0], c->VTsrc[0] + (size_t)c->rowrank * c->numpanelindices);
+         F.pv_single.insert(F.pv_single.end(), c->PV_single[0], c->PV_single[0] + (size_t)gp3 * c->rowrank);
+         F.pv_double.insert(F.pv_double.end(), c->PV_double[0], c->PV_double[0] + (size_t)gp3 * c->rowrank);
+      }
+      if (dst) {
+         F.uti.insert(F.uti.end(), c->UTI[0], c->UTI[0] + (size_t)c->columnrank * gp3);
+         F.u.insert(F.u.end(), c->Udest[0], c->Udest[0] + (size_t)c->numpointindices * c->columnrank);
+      }
+      F.inter_ptr.push_back((int32_t)F.inter_cubes.size());
+      for (unsigned i = 0; i < c->numinteractingcubes; i++) {
+         auto it = far_index.find(c->interactingcubes[i]);
+         FFTSVD_REQUIRE(it != far_index.end(), "interacting cube outside the tree");
+         F.inter_cubes.push_back(it->second);
+      }
+   }
+   F.num_cubes = (int)far_index.size();
+   F.cube_panel_ptr.push_back((int32_t)F.cube_panels.size());
+   F.cube_point_ptr.push_back((int32_t)F.cube_points.size());
+   F.cube_vt_ptr.push_back((int64_t)F.vt.size());
+   F.cube_pv_ptr.push_back((int64_t)F.pv_single.size());
+   F.cube_uti_ptr.push_back((int64_t)F.uti.size());
+   F.cube_u_ptr.push_back((int64_t)F.u.size());
+   F.inter_ptr.push_back((int32_t)F.inter_cubes.size());
+   int64_t off = 0;
+   for (int d = 0; d < F.depth; d++) {
+      const int np = 2 * F.grid[d] - 1, pg = np * np * F.grid[d];
+      F.t_level_ptr.push_back(off);
+      for (int s = 0; s < 343; s++) {
+         const float* tv = t->Tprecomputed ? t->Tprecomputed[d][s / 49][(s / 7) % 7][s % 7] : nullptr;
+         for (int f = 0; f < pg; f++) {
+            F.t_ops.push_back(tv ? tv[2 * f] : 0.0);
+            F.t_ops.push_back(tv ? tv[2 * f + 1] : 0.0);
+         }
+      }
+      off += 343LL * pg;
+   }
+   F.t_level_ptr.push_back(off);
+}
+
+struct RegionArrays {
+   setup::FlatTree flat;
+   std::vector<int32_t> phi_idx, dphi_idx, out_idx;
+   std::vector<double> phi_s, dphi_s, jump;
+};
+
+// Region maps of SurfaceOperator_multiply (SurfaceOperator.c:51-158) for every region.
+void gather_regions(const ref::SurfaceOperator* so, std::vector<std::unique_ptr<RegionArrays>>& out) {
+   if (so->tree && so->tree->numpanels > 0) {
+      auto R = std::make_unique<RegionArrays>();
+      for (unsigned k = 0; k < so->mynumpanels; k++) {
+         R->phi_idx.push_back((int32_t)(so->startphi + k));
+         R->phi_s.push_back(1.0);
+         R->dphi_idx.push_back((int32_t)(so->startdphi + k));
+         R->dphi_s.push_back(-1.0);
+         R->out_idx.push_back((int32_t)(so->startphi + k));
+         R->jump.push_back(0.0);
+      }
+      for (unsigned c = 0; c < so->numchildren; c++) {
+         const ref::SurfaceOperator* ch = so->children[c];
+         for (unsigned j = 0; j < ch->mynumpanels; j++) {
+            R->phi_idx.push_back((int32_t)(ch->startphi + j));
+            R->phi_s.push_back(-1.0);
+            R->dphi_idx.push_back((int32_t)(ch->startdphi + j));
+            R->dphi_s.push_back(ch->epsilon / so->epsilon);
+            R->out_idx.push_back((int32_t)(ch->startdphi + j));
+            R->jump.push_back(-4.0 * M_PI);
+         }
+      }
+      FFTSVD_REQUIRE(R->phi_idx.size() == so->tree->numpanels && so->tree->numpoints == so->tree->numpanels,
+                     "region panels do not match its tree (only collocation at panel centroids is supported)");
+      flatten_reference_tree(so->tree, R->flat);
+      out.push_back(std::move(R));
+   }
+   for (unsigned c = 0; c < so->numchildren; c++) gather_regions(so->children[c], out);
+}
+
+std::mutex g_cache_mutex;
+std::map<std::pair<const void*, const void*>, std::unique_ptr<fftsvd_surface>> g_cache;
+
+fftsvd_surface* surface_for(const ref::SurfaceOperator* so, const ref::Preconditioner* P, unsigned numtotalpanels) {
+   std::lock_guard<std::mutex> lock(g_cache_mutex);
+   auto key = std::make_pair((const void*)so, (const void*)P);
+   auto it = g_cache.find(key);
+   if (it != g_cache.end()) return it->second.get();
+   const int n = 2 * (int)numtotalpanels;
+   FFTSVD_REQUIRE(P && P->rows == (unsigned)n && P->columns == (unsigned)n, "preconditioner size mismatch");
+   std::vector<std::unique_ptr<RegionArrays>> regions;
+   gather_regions(so, regions);
+   FFTSVD_REQUIRE(!regions.empty(), "surface operator without panels");
+   std::vector<fftsvd_tree_flat> views(regions.size());
+   std::vector<fftsvd_region_map> maps(regions.size());
+   for (size_t r = 0; r < regions.size(); r++) {
+      regions[r]->flat.view(views[r]);
+      RegionArrays& R = *regions[r];
+      maps[r] = {R.phi_idx.data(), R.phi_s.data(), R.dphi_idx.data(), R.dphi_s.data(), R.out_idx.data(), R.jump.data()};
+   }
+   std::vector<int32_t> col_ptr(n + 1, 0), rows;
+   std::vector<double> vals;
+   for (int c = 0; c < n; c++) {
+      for (unsigned e = 0; e < P->numelements[c]; e++) {
+         rows.push_back((int32_t)P->P[c][e].row);
+         vals.push_back(P->P[c][e].value);
+      }
+      col_ptr[c + 1] = (int32_t)rows.size();
+   }
+   fftsvd_precond_csc pc{n, col_ptr.data(), rows.data(), vals.data()};
+   auto s = std::make_unique<fftsvd_surface>();
+   init_surface(s->s, n, (int)regions.size(), views.data(), maps.data(), &pc);
+   fftsvd_surface* out = s.get();
+   g_cache[key] = std::move(s);
+   return out;
+}
+
+__global__ void rhs_targets_kernel(int nt, const double* __restrict__ cent, const int32_t* __restrict__ rows, int nq,
+                                   const double* __restrict__ qpos, const double* __restrict__ q,
+                                   double* __restrict__ rhs) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= nt) return;
+   const double cx = cent[3 * i], cy = cent[3 * i + 1], cz = cent[3 * i + 2];
+   double acc = 0.0;
+   for (int j = 0; j < nq; j++) {
+      const double qj = q[j];
+      if (qj == 0.0) continue;
+      const double dx = qpos[3 * j] - cx, dy = qpos[3 * j + 1] - cy, dz = qpos[3 * j + 2] - cz;
+      acc += qj / sqrt(dx * dx + dy * dy + dz * dz);
+   }
+   rhs[rows[i]] += acc;
+}
+
+void rhs_region(const ref::SurfaceOperator* so, double* drhs) {
+   if (so->charges && so->charges->numcharges > 0) {
+      std::vector<double> cent;
+      std::vector<int32_t> rows;
+      for (unsigned j = 0; j < so->mynumpanels; j++) {
+         const ref::Vec3* c = so->tree->panels[j]->centroid;
+         cent.insert(cent.end(), {c->x, c->y, c->z});
+         rows.push_back((int32_t)(so->startphi + j));
+      }
+      for (unsigned k = 0; k < so->numchildren; k++) {
+         const ref::SurfaceOperator* ch = so->children[k];
+         for (unsigned j = 0; j < ch->mynumpanels; j++) {
+            const ref::Vec3* c = ch->tree->panels[j]->centroid;
+            cent.insert(cent.end(), {c->x, c->y, c->z});
+            rows.push_back((int32_t)(ch->startdphi + j));
+         }
+      }
+      const ref::Charge* Q = so->charges;
+      std::vector<double> qpos, qv(Q->charges, Q->charges + Q->numcharges);
+      for (unsigned i = 0; i < Q->numcharges; i++) qpos.insert(qpos.end(), {Q->points[i]->x, Q->points[i]->y, Q->points[i]->z});
+      if (!rows.empty()) {
+         DevBuf<double> dc, dq, dqp;
+         DevBuf<int32_t> dr;
+         dc.upload(cent);
+         dr.upload(rows);
+         dq.upload(qv);
+         dqp.upload(qpos);
+         const int nt = (int)rows.size();
+         rhs_targets_kernel<<<(nt + 255) / 256, 256>>>(nt, dc.get(), dr.get(), (int)qv.size(), dqp.get(), dq.get(), drhs);
+         FFTSVD_CHECK_LAUNCH();
+         FFTSVD_CUDA(cudaDeviceSynchronize());
+      }
+   }
+   for (unsigned k = 0; k < so->numchildren; k++) rhs_region(so->children[k], drhs);
+}
+
+}  // namespace
+}  // namespace fftsvd
+
+using namespace fftsvd;
+
+extern "C" void solveSurfaceOperator(double** solution, struct _SurfaceOperator* pbesurfaceoperator,
+                                     struct _Preconditioner* preconditioner, double* rhs, unsigned int numtotalpanels) {
+   if (!solution) return;
+   *solution = nullptr;
+   const double tol = &errortolerance ? errortolerance : 1e-6;
+   try {
+      FFTSVD_REQUIRE(pbesurfaceoperator && preconditioner && rhs && numtotalpanels > 0, "null argument");
+      fftsvd_surface* s = surface_for(reinterpret_cast<const ref::SurfaceOperator*>(pbesurfaceoperator),
+                                      reinterpret_cast<const ref::Preconditioner*>(preconditioner), numtotalpanels);
+      const int n = 2 * (int)numtotalpanels;
+      int precision = FFTSVD_PREC_MIXED;
+      if (const char* e = std::getenv("FFTSVD_B200_PRECISION")) {
+         if (!strcmp(e, "fp64")) precision = FFTSVD_PREC_FP64;
+         else if (!strcmp(e, "fp32")) precision = FFTSVD_PREC_FP32;
+      }
+      double* out = static_cast<double*>(std::calloc((size_t)n, sizeof(double)));
+      FFTSVD_REQUIRE(out, "host allocation failed");
+      fftsvd_solve_info info{};
+      const int rc = fftsvd_b200_solve(s, precision, rhs, out, tol, 1000, &info);
+      if (rc != FFTSVD_OK && rc != FFTSVD_ERR_NOT_CONVERGED) {
+         std::free(out);
+         throw Error(rc, fftsvd_b200_last_error());
+      }
+      *solution = out;
+   } catch (const std::exception& e) {
+      set_last_error(e.what());
+      std::fprintf(stderr, "fftsvd_b200 solveSurfaceOperator: %s\n", e.what());
+   }
+}
+
+extern "C" void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceoperator, unsigned int numtotalpanels) {
+   if (!rhs) return;
+   *rhs = nullptr;
+   try {
+      FFTSVD_REQUIRE(pbesurfaceoperator && numtotalpanels > 0, "null argument");
+      const int n = 2 * (int)numtotalpanels;
+      DevBuf<double> d(n);
+      d.zero();
+      rhs_region(reinterpret_cast<const ref::SurfaceOperator*>(pbesurfaceoperator), d.get());
+      double* out = static_cast<double*>(std::calloc((size_t)n, sizeof(double)));
+      FFTSVD_REQUIRE(out, "host allocation failed");
+      FFTSVD_CUDA(cudaMemcpy(out, d.get(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+      *rhs = out;
+   } catch (const std::exception& e) {
+      set_last_error(e.what());
+      std::fprintf(stderr, "fftsvd_b200 generateRHS: %s\n", e.what());
+   }
+}

@@ -283,6 +283,34 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       FFTSVD_REQUIRE(L.point_out[k] >= 0 && L.point_out[k] < num_unknowns, "point without an output row");
       FFTSVD_REQUIRE(L.point_panel[k] >= -1 && L.point_panel[k] < L.total_panels - 1, "jump panel index");
    }
+   // algorithmic bytes per kernel (each operator element, spectrum and vector entry counted once)
+   {
+      KernelBytes& kb = L.kernel_bytes;
+      const double np = (double)(L.total_panels - 1), nq = (double)L.total_points;
+      kb.fixed[0] = np * (8.0 + 2 * 4.0 + 2 * 8.0);  // x reads, two indices, two scales
+      kb.elems[0] = 2.0 * np;                         // {xs, xd} writes
+      double vt = 0, pv = 0, spec = 0, uti = 0, u = 0, dpairs = 0, lcols = 0, lrows = 0;
+      for (const SrcDesc& sd : L.src) {
+         vt += (double)sd.r * sd.m;
+         pv += 2.0 * sd.r * sd.n * sd.n * sd.n;
+         spec += 2.0 * (2 * sd.n - 1) * (2 * sd.n - 1) * sd.n;
+      }
+      for (const DstDesc& dd : L.dst) {
+         uti += (double)dd.r * dd.n * dd.n * dd.n;
+         u += (double)dd.r * dd.p;
+      }
+      for (const LeafDesc& ld : L.leaves) {
+         dpairs += 2.0 * ld.nrows * ld.ncols;
+         lcols += ld.ncols;
+         lrows += ld.nrows;
+      }
+      kb.elems[1] = vt + pv + spec + 2.0 * (double)L.src_panels.size();  // + gathered {xs, xd}
+      kb.fixed[1] = 4.0 * (double)L.src_panels.size();
+      kb.elems[2] = spec + (double)L.t_elems + uti + u + nq;              // spectra, T, UTI, U, staging writes
+      kb.fixed[2] = 4.0 * (double)L.dst_points.size() + 16.0 * (double)(L.inter_pairs.size() / 2);
+      kb.elems[3] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
+      kb.fixed[3] = 4.0 * (lcols + lrows) + nq * (8.0 + 4.0 + 4.0 + 8.0); // indices, y, maps, jump
+   }
    // heavy source cubes first so the long blocks start early
    std::stable_sort(L.src.begin(), L.src.end(),
                     [](const SrcDesc& a, const SrcDesc& b) { return (int64_t)a.r * a.m > (int64_t)b.r * b.m; });
@@ -670,10 +698,11 @@ void DeviceOperator<T>::enable_timing(bool on) {
 }
 
 template <typename T>
-void DeviceOperator<T>::stage_ms(float* near_ms, float* fwd_ms, float* bwd_ms) const {
-   *near_ms = *fwd_ms = *bwd_ms = 0.f;
+void DeviceOperator<T>::stage_ms(float* join_ms, float* fwd_ms, float* bwd_ms, float* near_ms) const {
+   *join_ms = *near_ms = *fwd_ms = *bwd_ms = 0.f;
    if (!ev_[0]) return;
    FFTSVD_CUDA(cudaEventSynchronize(ev_[4]));
+   FFTSVD_CUDA(cudaEventElapsedTime(join_ms, ev_[0], ev_[1]));
    FFTSVD_CUDA(cudaEventElapsedTime(fwd_ms, ev_[1], ev_[2]));
    FFTSVD_CUDA(cudaEventElapsedTime(bwd_ms, ev_[2], ev_[3]));
    FFTSVD_CUDA(cudaEventElapsedTime(near_ms, ev_[3], ev_[4]));

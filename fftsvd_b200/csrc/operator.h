@@ -51,6 +51,13 @@ struct LeafDesc {       // one leaf with points
    int64_t d_off;       // into d (element pairs), nrows x ncols
 };
 
+// Algorithmic bytes of each matvec kernel [join, far_forward, far_backward, near]:
+// elems * (operator element size) + fixed (FP64 vectors and int32 indices).
+struct KernelBytes {
+   double elems[4] = {0, 0, 0, 0};
+   double fixed[4] = {0, 0, 0, 0};
+};
+
 // Host-side relayout product, independent of the element type.
 struct OperatorLayout {
    int num_unknowns = 0;
@@ -85,6 +92,7 @@ struct OperatorLayout {
    // algorithmic bytes per matvec at 4-byte or 8-byte element size (excluding vectors)
    int64_t operator_elems = 0;          // D pairs*2 + VT + PV*2 + UTI + U
    int64_t t_elems = 0;                 // unique translation operator reals
+   KernelBytes kernel_bytes;
 };
 
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
@@ -99,7 +107,7 @@ class DeviceOperator {
    void apply(const double* x, double* y, cudaStream_t stream);
    // per-stage events for timing (recorded when enabled)
    void enable_timing(bool on);
-   void stage_ms(float* near_ms, float* fwd_ms, float* bwd_ms) const;
+   void stage_ms(float* join_ms, float* fwd_ms, float* bwd_ms, float* near_ms) const;
    size_t device_bytes() const;
    int num_launches_per_apply() const { return full_cover_ ? 4 : 5; }
 

@@ -13,6 +13,7 @@
 
 namespace fftsvd {
 
+std::atomic<long long> g_kernel_launches{0};
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -297,6 +298,7 @@ void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree
    OperatorLayout L = build_layout(num_unknowns, num_trees, trees, maps);
    S.operator_elems = L.operator_elems;
    S.t_elems = L.t_elems;
+   S.kernel_bytes = L.kernel_bytes;
    S.op64.upload(L);
    S.op32.upload(L);
    S.precond.build(*P, num_unknowns);
@@ -419,6 +421,43 @@ int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, d
    });
    if (rc != FFTSVD_OK) return rc;
    return status;
+}
+
+long long fftsvd_b200_launch_count(void) { return g_kernel_launches.load(); }
+
+void* fftsvd_b200_surface_stream(const fftsvd_surface* s) { return s ? (void*)s->s.stream : nullptr; }
+
+int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes4) {
+   if (!s || !bytes4) return FFTSVD_ERR_ARGUMENT;
+   const KernelBytes& kb = s->s.kernel_bytes;
+   const double es = precision == FFTSVD_PREC_FP64 ? 8.0 : 4.0;
+   for (int k = 0; k < 4; k++) bytes4[k] = kb.elems[k] * es + kb.fixed[k];
+   return FFTSVD_OK;
+}
+
+int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y, int32_t reps,
+                               double* ms4) {
+   if (!s || !x || !y || !ms4 || reps <= 0) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      Surface& S = s->s;
+      double acc[4] = {0, 0, 0, 0};
+      for (int r = 0; r < reps; r++) {
+         float t[4];
+         if (precision == FFTSVD_PREC_FP64) {
+            S.op64.enable_timing(true);
+            S.op64.apply(x, y, S.stream);
+            S.op64.stage_ms(&t[0], &t[1], &t[2], &t[3]);
+            S.op64.enable_timing(false);
+         } else {
+            S.op32.enable_timing(true);
+            S.op32.apply(x, y, S.stream);
+            S.op32.stage_ms(&t[0], &t[1], &t[2], &t[3]);
+            S.op32.enable_timing(false);
+         }
+         for (int k = 0; k < 4; k++) acc[k] += t[k];
+      }
+      for (int k = 0; k < 4; k++) ms4[k] = acc[k] / reps;
+   });
 }
 
 int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes) {

@@ -33,6 +33,7 @@ struct Surface {
    DeviceOperator<float> op32;
    Preconditioner precond;
    int64_t operator_elems = 0, t_elems = 0;
+   KernelBytes kernel_bytes;
    double eps_in = 1.0;
    // inner region (interior, Laplace) tree panel -> unknown rows, for RHS and collection
    std::vector<int32_t> inner_phi_row, inner_dphi_row;

@@ -28,7 +28,8 @@ EXPORTED = [
     "fftsvd_b200_reaction_potentials", "fftsvd_b200_reaction_potentials_device", "fftsvd_b200_energy",
     "fftsvd_b200_matvec_bytes", "fftsvd_b200_surface_stats", "fftsvd_b200_host_setup",
     "fftsvd_b200_host_operator_tree", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
-    "solveSurfaceOperator", "generateRHS",
+    "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
+    "fftsvd_b200_launch_count", "solveSurfaceOperator", "generateRHS",
 ]
 
 
@@ -77,6 +78,11 @@ def load():
     lib.fftsvd_b200_host_operator_tree.argtypes = [sp, C.c_int32, C.POINTER(TreeFlat)]
     lib.fftsvd_b200_host_operator_precond.argtypes = [sp, C.POINTER(PrecondCSC)]
     lib.fftsvd_b200_host_operator_free.argtypes = [sp]
+    lib.fftsvd_b200_matvec_kernel_bytes.argtypes = [sp, C.c_int32, _f64p]
+    lib.fftsvd_b200_profile_matvec.argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, _f64p]
+    lib.fftsvd_b200_surface_stream.argtypes = [sp]
+    lib.fftsvd_b200_surface_stream.restype = C.c_void_p
+    lib.fftsvd_b200_launch_count.restype = C.c_longlong
     _lib = lib
     return lib
 
