@@ -38,6 +38,8 @@ CONFIGS = {
                  level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1),
     "born": dict(name="Born ion L5 (20480 panels, R 10 A, +1 e, eps 1/80)", kind="born", level=5, radius=10.0,
                  nq=1, eps_in=1.0, eps_out=80.0, kappa=0.0, seed=0),
+    "blob5": dict(name="blob L5 (20480 panels, R 22 A, 2500 charges, eps 4/80, kappa 0.125)", kind="blob",
+                  level=5, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1),
     "large": dict(name="large blob L7 (327680 panels, R 60 A, 30000 charges, eps 4/80, kappa 0.125)", kind="blob",
                   level=7, radius=60.0, nq=30000, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=3),
 }
@@ -346,8 +348,28 @@ def run_ours(args, cfg, ws, rank, local):
     s.close()
 
 
+def run_matvec_only(args, cfg, local):
+    """Build the surface and run `--reps` FP32 and FP64 matvecs (for profiler captures)."""
+    import torch
+    from fftsvd_b200.surface import Surface
+
+    torch.cuda.set_device(local)
+    tri, qpos, q = make_workload(cfg)
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    x = torch.randn(s.n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    for prec in ("fp32", "fp64"):
+        for _ in range(args.reps):
+            s.matvec_device(x.data_ptr(), y.data_ptr(), prec)
+    torch.cuda.synchronize()
+    print(json.dumps({"matvec_only": cfg["name"], "reps": args.reps, "norm": float(y.norm())}))
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--matvec-only", action="store_true", help="only run --reps matvecs (profiling)")
+    ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -360,7 +382,9 @@ def main():
     cfg = CONFIGS[args.config]
     ws, rank, local = dist_init()
     try:
-        if args.impl == "reference":
+        if args.matvec_only:
+            run_matvec_only(args, cfg, local)
+        elif args.impl == "reference":
             run_reference(args, cfg, ws, rank)
         else:
             run_ours(args, cfg, ws, rank, local)

@@ -311,12 +311,36 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       kb.elems[3] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
       kb.fixed[3] = 4.0 * (lcols + lrows) + nq * (8.0 + 4.0 + 4.0 + 8.0); // indices, y, maps, jump
    }
-   // heavy source cubes first so the long blocks start early
-   std::stable_sort(L.src.begin(), L.src.end(),
-                    [](const SrcDesc& a, const SrcDesc& b) { return (int64_t)a.r * a.m > (int64_t)b.r * b.m; });
-   std::stable_sort(L.dst.begin(), L.dst.end(), [](const DstDesc& a, const DstDesc& b) {
-      return (int64_t)a.inter_cnt * a.n * a.n * a.n > (int64_t)b.inter_cnt * b.n * b.n * b.n;
+   // group by grid size (largest first), heavy cubes first within a group so the
+   // long blocks start early; each group is one launch with its own shared memory
+   std::stable_sort(L.src.begin(), L.src.end(), [](const SrcDesc& a, const SrcDesc& b) {
+      if (a.n != b.n) return a.n > b.n;
+      return (int64_t)a.r * a.m > (int64_t)b.r * b.m;
    });
+   std::stable_sort(L.dst.begin(), L.dst.end(), [](const DstDesc& a, const DstDesc& b) {
+      if (a.n != b.n) return a.n > b.n;
+      return (int64_t)a.inter_cnt * a.r > (int64_t)b.inter_cnt * b.r;
+   });
+   auto src_need = [](const SrcDesc& s) {
+      const int n = s.n, Np = 2 * n - 1, H = n, ch = std::min(s.m, 1024);
+      return 2 * ch + 2 * s.r + n * n * n + 2 * Np + 2 * (n * n * H) + 2 * (n * Np * H) + 16;
+   };
+   auto dst_need = [](const DstDesc& d) {
+      const int n = d.n, Np = 2 * n - 1, H = n, pg = Np * Np * H;
+      return 2 * pg + 2 * (n * Np * H) + 2 * (n * n * H) + n * n * n + d.r + 2 * Np + 16;
+   };
+   for (int i = 0; i < (int)L.src.size(); i++) {
+      if (L.src_groups.empty() || L.src_groups.back().n != L.src[i].n) L.src_groups.push_back({L.src[i].n, i, 0, 0});
+      LaunchGroup& g = L.src_groups.back();
+      g.count++;
+      g.smem_elems = std::max(g.smem_elems, src_need(L.src[i]));
+   }
+   for (int i = 0; i < (int)L.dst.size(); i++) {
+      if (L.dst_groups.empty() || L.dst_groups.back().n != L.dst[i].n) L.dst_groups.push_back({L.dst[i].n, i, 0, 0});
+      LaunchGroup& g = L.dst_groups.back();
+      g.count++;
+      g.smem_elems = std::max(g.smem_elems, dst_need(L.dst[i]));
+   }
    return L;
 }
 
@@ -674,8 +698,12 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    staging_.alloc(std::max<int64_t>((int64_t)L.stage_levels * L.total_points, 1));
    staging_.zero();
    // entries of the zero slot and staging rows nobody writes must stay zero
-   src_smem_ = (int)(L.max_src_smem_elems * sizeof(T) + 128);
-   dst_smem_ = (int)(L.max_dst_smem_elems * sizeof(T) + 128);
+   src_groups_ = L.src_groups;
+   dst_groups_ = L.dst_groups;
+   src_smem_ = 0;
+   dst_smem_ = 0;
+   for (const LaunchGroup& g : src_groups_) src_smem_ = std::max(src_smem_, (int)(g.smem_elems * sizeof(T) + 128));
+   for (const LaunchGroup& g : dst_groups_) dst_smem_ = std::max(dst_smem_, (int)(g.smem_elems * sizeof(T) + 128));
    int maxcols = 0;
    for (const auto& l : L.leaves) maxcols = std::max(maxcols, l.ncols);
    leaf_smem_max_ = (int)(maxcols * sizeof(T2) + 16);
@@ -721,15 +749,17 @@ void DeviceOperator<T>::apply(const double* x, double* y, cudaStream_t stream) {
       FFTSVD_CHECK_LAUNCH();
    }
    if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[1], stream));
-   if (n_src_ > 0) {
-      far_forward_kernel<T><<<n_src_, kFarThreads, src_smem_, stream>>>(src_.get(), src_panels_.get(), xsd_.get(),
-                                                                        vt_.get(), pv_.get(), spectra_.get());
+   for (const LaunchGroup& g : src_groups_) {
+      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+      far_forward_kernel<T><<<g.count, kFarThreads, smem, stream>>>(src_.get() + g.begin, src_panels_.get(),
+                                                                    xsd_.get(), vt_.get(), pv_.get(), spectra_.get());
       FFTSVD_CHECK_LAUNCH();
    }
    if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[2], stream));
-   if (n_dst_ > 0) {
-      far_backward_kernel<T><<<n_dst_, kFarThreads, dst_smem_, stream>>>(
-          dst_.get(), dst_points_.get(), inter_.get(), t_.get(), spectra_.get(), uti_.get(), u_.get(),
+   for (const LaunchGroup& g : dst_groups_) {
+      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+      far_backward_kernel<T><<<g.count, kFarThreads, smem, stream>>>(
+          dst_.get() + g.begin, dst_points_.get(), inter_.get(), t_.get(), spectra_.get(), uti_.get(), u_.get(),
           staging_.get(), total_points_);
       FFTSVD_CHECK_LAUNCH();
    }

@@ -51,6 +51,15 @@ struct LeafDesc {       // one leaf with points
    int64_t d_off;       // into d (element pairs), nrows x ncols
 };
 
+// A contiguous range of source or destination cubes of one grid size, launched
+// together with shared memory sized for that range.
+struct LaunchGroup {
+   int n = 0;
+   int begin = 0;
+   int count = 0;
+   int smem_elems = 0;  // in units of the operator element type
+};
+
 // Algorithmic bytes of each matvec kernel [join, far_forward, far_backward, near]:
 // elems * (operator element size) + fixed (FP64 vectors and int32 indices).
 struct KernelBytes {
@@ -89,6 +98,7 @@ struct OperatorLayout {
    std::vector<double> t_pairs;        // translation operators {re, im}
    int64_t spectra_elems = 0;
    int max_src_smem_elems = 0, max_dst_smem_elems = 0;
+   std::vector<LaunchGroup> src_groups, dst_groups;
    // algorithmic bytes per matvec at 4-byte or 8-byte element size (excluding vectors)
    int64_t operator_elems = 0;          // D pairs*2 + VT + PV*2 + UTI + U
    int64_t t_elems = 0;                 // unique translation operator reals
@@ -109,7 +119,6 @@ class DeviceOperator {
    void enable_timing(bool on);
    void stage_ms(float* join_ms, float* fwd_ms, float* bwd_ms, float* near_ms) const;
    size_t device_bytes() const;
-   int num_launches_per_apply() const { return full_cover_ ? 4 : 5; }
 
  private:
    int num_unknowns_ = 0;
@@ -118,6 +127,7 @@ class DeviceOperator {
    bool full_cover_ = true;
    int n_src_ = 0, n_dst_ = 0, n_leaf_ = 0;
    int src_smem_ = 0, dst_smem_ = 0, leaf_smem_max_ = 0;
+   std::vector<LaunchGroup> src_groups_, dst_groups_;
    DevBuf<int32_t> join_phi_idx_, join_dphi_idx_;
    DevBuf<double> join_phi_scale_, join_dphi_scale_;
    DevBuf<T2> xsd_;

@@ -153,7 +153,8 @@ double Surface::pnorm(const double* v) {
    return std::sqrt(s);
 }
 
-int Surface::gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status) {
+int Surface::gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
+                   bool absolute_zero_check) {
    const int nb = vec_blocks(n);
    const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
    ensure_capacity(maxit + 1);
@@ -167,7 +168,7 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       *res = normr;
       return 0;
    }
-   if (normr < tol) {  // hand back zero solution
+   if (absolute_zero_check && normr < tol) {  // hand back zero solution (GMRES.c:461-465)
       *res = 0.0;
       return 0;
    }
@@ -256,11 +257,15 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
       res = 1.0;
       if (!std::isfinite(bn)) status = FFTSVD_ERR_NONFINITE;
       else if (bn < tol) res = 0.0;
+      // Each inner solve targets an absolute preconditioned error of 0.3 tol ||P^-1 b||: the
+      // first one therefore runs to 0.3 tol, a correction to 0.3 tol / (current residual).
+      // The FP32 operator differs from the FP64 one by ~1e-7 relative, so one correction is
+      // rarely needed and the FP64 operator is applied once per refinement only.
       for (refinements = 0; status == FFTSVD_OK && res >= tol && refinements < 8; refinements++) {
          double inner_res = 0.0;
          int st2 = FFTSVD_OK;
-         // inner solve to tol relative to the current residual
-         iters += gmres(FFTSVD_PREC_FP32, t1.get(), xout.get(), std::max(tol, 1e-12), maxit, &inner_res, &st2);
+         const double inner_tol = std::min(0.1, std::max(0.3 * tol / res, 1e-13));
+         iters += gmres(FFTSVD_PREC_FP32, t1.get(), xout.get(), inner_tol, maxit, &inner_res, &st2, false);
          if (st2 == FFTSVD_ERR_NONFINITE) { status = st2; break; }
          add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x);
          FFTSVD_CHECK_LAUNCH();

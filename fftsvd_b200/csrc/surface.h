@@ -58,7 +58,8 @@ struct Surface {
    double pnorm(const double* v);  // ||v|| on device, synchronous
    // Left-preconditioned un-restarted GMRES (GMRES.c:446-539) with operator `precision`;
    // x overwritten.  Returns iterations; residual via *res.
-   int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status);
+   int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
+             bool absolute_zero_check = true);
    int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
 };
 
