@@ -128,13 +128,26 @@ def dist_init():
 
 
 def barrier_max(value: float, ws: int) -> float:
+    """Max of a per-rank value over all ranks (timings are reported as the slowest rank)."""
     if ws == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_shares(num_units: int, ws: int):
+    """Contiguous, disjoint shares of independent units (surfaces or right-hand sides) per rank."""
+    base, extra = divmod(num_units, ws)
+    out, start = [], 0
+    for r in range(ws):
+        cnt = base + (1 if r < extra else 0)
+        out.append(range(start, start + cnt))
+        start += cnt
+    return out
 
 
 def barrier(ws):

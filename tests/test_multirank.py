@@ -1,0 +1,50 @@
+"""Multi-rank host logic on CPU (gloo, world size 2): max-over-ranks timing and
+the replica partition of independent units."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import bench
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, ws, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(ws))
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    try:
+        got = bench.barrier_max(float(rank + 1) * 1.5, ws)
+        out[rank] = got
+    finally:
+        dist.destroy_process_group()
+
+
+def test_barrier_max_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0] == out[1] == 3.0
+
+
+@pytest.mark.parametrize("n,ws", [(64, 8), (7, 2), (3, 4), (1, 1), (0, 3)])
+def test_replica_shares_partition(n, ws):
+    shares = bench.replica_shares(n, ws)
+    assert len(shares) == ws
+    flat = [i for s in shares for i in s]
+    assert flat == list(range(n))
+    sizes = [len(s) for s in shares]
+    assert max(sizes) - min(sizes) <= 1
