@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "nbody.h"
@@ -228,6 +230,77 @@ int fftsvd_b200_reaction_potentials_device(fftsvd_surface* s, const double* sol,
       reaction_device(s->s, sol, phi);
       return FFTSVD_OK;
    } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   }
+}
+
+}  // extern "C"
+
+namespace fftsvd {
+
+// Scratch of fftsvd_b200_reaction_potentials_noalloc: the per-chunk partial
+// sums of the collection, at most kNoAllocScratchDoubles doubles (4 MiB).
+// Every GPU that loads this library holds one copy until the process exits.
+constexpr size_t kNoAllocScratchDoubles = 524288;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of the scratch array per device ordinal, looked up once per
+// device with that device current.  In host code the array's name is only a
+// host-side stand-in, so kernels are always given this looked-up address.
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_addr[128] = {nullptr};
+
+static double* noalloc_scratch(int device) {
+   FFTSVD_REQUIRE(device >= 0 && device < 128, "device ordinal out of range");
+   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+   if (!g_noalloc_addr[device]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+         throw Error(FFTSVD_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+      g_noalloc_addr[device] = static_cast<double*>(p);
+   }
+   return g_noalloc_addr[device];
+}
+
+}  // namespace fftsvd
+
+extern "C" {
+
+// Reaction potentials without any device allocation: for callers that cannot
+// call cudaMalloc (see include/fftsvd_b200.h).  sol and phi are device pointers.
+int fftsvd_b200_reaction_potentials_noalloc(fftsvd_surface* s, const double* sol, double* phi) {
+   if (!s || !sol || !phi) return FFTSVD_ERR_ARGUMENT;
+   int previous = -1;
+   try {
+      Surface& S = s->s;
+      FFTSVD_REQUIRE(S.geom, "surface has no panel geometry");
+      const int nq = S.num_charges, np = S.geom->num_panels;
+      if (nq == 0) return FFTSVD_OK;
+      if ((size_t)nq > kNoAllocScratchDoubles)
+         throw Error(FFTSVD_ERR_ARGUMENT, "fftsvd_b200_reaction_potentials_noalloc: " + std::to_string(nq) +
+                                              " charges exceed the scratch limit of " +
+                                              std::to_string(kNoAllocScratchDoubles) + " charges");
+      FFTSVD_CUDA(cudaGetDevice(&previous));
+      if (previous != S.device) FFTSVD_CUDA(cudaSetDevice(S.device));
+      double* scratch = noalloc_scratch(S.device);
+      // same chunking as the allocating path, reduced until chunks x charges fits the scratch
+      int chunks = std::max(1, std::min(kReactChunks, (np + kReactPanelTile - 1) / kReactPanelTile));
+      chunks = std::max(1, std::min<int>(chunks, (int)(kNoAllocScratchDoubles / (size_t)nq)));
+      dim3 grid((nq + kReactThreads - 1) / kReactThreads, chunks);
+      // every scratch entry the reduction reads is written by the partial kernel of this call
+      reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
+                                                                    S.geom->dphi_row.get(), sol, nq,
+                                                                    S.charge_pos.get(), scratch);
+      FFTSVD_CHECK_LAUNCH();
+      reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, scratch, phi);
+      FFTSVD_CHECK_LAUNCH();
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+      if (previous != S.device) FFTSVD_CUDA(cudaSetDevice(previous));
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      if (previous >= 0) cudaSetDevice(previous);
       set_last_error(e.what());
       return e.code;
    }

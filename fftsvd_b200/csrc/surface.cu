@@ -299,6 +299,7 @@ void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree
       throw Error(FFTSVD_ERR_NO_DEVICE, "no CUDA device visible");
    FFTSVD_REQUIRE(trees && maps && P, "null operator description");
    S.n = num_unknowns;
+   FFTSVD_CUDA(cudaGetDevice(&S.device));
    FFTSVD_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
    OperatorLayout L = build_layout(num_unknowns, num_trees, trees, maps);
    S.operator_elems = L.operator_elems;

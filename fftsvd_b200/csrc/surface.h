@@ -28,6 +28,7 @@ struct Preconditioner {
 
 struct Surface {
    int n = 0;  // unknowns
+   int device = 0;  // CUDA device ordinal the surface lives on
    cudaStream_t stream = nullptr;
    DeviceOperator<double> op64;
    DeviceOperator<float> op32;

@@ -219,6 +219,25 @@ int fftsvd_b200_rhs_device(fftsvd_surface* s, double* rhs);
    (SurfaceOperator.c:364-396, direct analytic panel integrals). */
 int fftsvd_b200_reaction_potentials(fftsvd_surface* s, const double* sol, double* phi);
 int fftsvd_b200_reaction_potentials_device(fftsvd_surface* s, const double* sol, double* phi);
+
+/* The same reaction potentials without any device allocation (no counterpart
+   in the reference).  For callers that cannot call cudaMalloc: programs whose
+   device memory is owned by another allocator (a framework's caching
+   allocator or a pool reserved at start-up, where a stray cudaMalloc fails or
+   fragments the pool) and latency-sensitive callers for whom the implicit
+   device synchronisation of cudaMalloc/cudaFree is not acceptable.  sol
+   (2N doubles) and phi (one double per charge) are device pointers the caller
+   allocated; the surface itself was allocated when it was created.
+   The per-chunk partial sums live in one file-scope device array of
+   524288 doubles (4 MiB), which every GPU that loads this library holds until
+   the process exits; surfaces with more than 524288 charges are rejected with
+   FFTSVD_ERR_ARGUMENT.  The first call on a device looks up that array's
+   device address with the surface's device current; make that first call
+   before any stream capture.  All calls share the one array and every call
+   overwrites the entries it reads, so nothing carries over between calls;
+   calls that overlap on the GPU (different threads or streams) race on it.
+   The call returns after its work on the surface's stream has finished. */
+int fftsvd_b200_reaction_potentials_noalloc(fftsvd_surface* s, const double* sol, double* phi);
 /* 0.5 * sum q phi * 332.112 / eps_in (FFTSVDsalt.c:167-170). */
 int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
 
