@@ -273,19 +273,31 @@ def run_ours(args, cfg, ws, rank, local):
     # matvec: per-kernel CUDA-event times on the library stream, algorithmic bytes per kernel
     xv = torch.randn(n, dtype=torch.float64, device="cuda")
     yv = torch.empty_like(xv)
-    kernels = ["join", "far_forward", "far_backward", "near"]
+    kernels = ["join", "far_forward", "translate", "far_backward", "near"]
     prof = {}
     for prec, pid in (("fp32", _abi.PREC_FP32), ("fp64", _abi.PREC_FP64)):
-        ms4 = (C.c_double * 4)()
-        b4 = (C.c_double * 4)()
-        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 3, ms4)
-        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 20, ms4)
-        lib.fftsvd_b200_matvec_kernel_bytes(s._h, pid, b4)
-        prof[prec] = {k: {"ms": ms4[i], "bytes": b4[i], "gbs": b4[i] / (ms4[i] * 1e6) if ms4[i] > 0 else None}
+        ms5 = (C.c_double * 5)()
+        b5 = (C.c_double * 5)()
+        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 3, ms5)
+        lib.fftsvd_b200_profile_matvec(s._h, pid, C.c_void_p(xv.data_ptr()), C.c_void_p(yv.data_ptr()), 20, ms5)
+        lib.fftsvd_b200_matvec_kernel_bytes(s._h, pid, b5)
+        prof[prec] = {k: {"ms": ms5[i], "bytes": b5[i], "gbs": b5[i] / (ms5[i] * 1e6) if ms5[i] > 0 else None}
                       for i, k in enumerate(kernels)}
-        prof[prec]["total_ms"] = sum(ms4[i] for i in range(4))
+        prof[prec]["total_ms"] = sum(ms5[i] for i in range(5))
     mv_bytes32 = st.matvec_bytes_fp32
     mv_bytes64 = st.matvec_bytes_fp64
+    # matvec as the solver issues it (grid-size chains and the near field on concurrent streams)
+    mv_streams = {}
+    for prec in ("fp32", "fp64"):
+        for _ in range(3):
+            s.matvec_device(xv.data_ptr(), yv.data_ptr(), prec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(20):
+            s.matvec_device(xv.data_ptr(), yv.data_ptr(), prec)
+        e1.record(stream)
+        e1.synchronize()
+        mv_streams[prec] = e0.elapsed_time(e1) / 20
 
     # e2e through the host-pointer C-ABI (pinned host buffers, copies inside the timed region)
     rhs_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -353,6 +365,7 @@ def run_ours(args, cfg, ws, rank, local):
             "iterations_fp64": info64.iterations,
             "dG_kcal_mixed": e_mixed, "dG_kcal_fp64": e64, "dG_rel_err_mixed_vs_fp64": abs(e_mixed - e64) / abs(e64),
             "matvec_ms_fp32": prof["fp32"]["total_ms"], "matvec_ms_fp64": prof["fp64"]["total_ms"],
+            "matvec_ms_fp32_streams": mv_streams["fp32"], "matvec_ms_fp64_streams": mv_streams["fp64"],
             "matvec_gbs_fp32": mv_bytes32 / (prof["fp32"]["total_ms"] * 1e6),
             "matvec_gbs_fp64": mv_bytes64 / (prof["fp64"]["total_ms"] * 1e6),
             "matvec_kernels": prof, "setup_s": setup_s,

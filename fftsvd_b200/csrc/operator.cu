@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <string>
 
@@ -26,6 +27,7 @@ namespace fftsvd {
 // ------------------------------------------------------------------ layout
 
 static int pad2(int v) { return (v + 1) & ~1; }
+static int pad16(int v) { return (v + 15) & ~15; }
 
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
                             const fftsvd_region_map* maps) {
@@ -59,6 +61,13 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
    L.point_panel.assign(nq, -1);
    L.point_jump.assign(nq, 0.0);
    std::vector<char> row_written(num_unknowns, 0);
+   struct DstExtra {
+      int key;        // tree * 64 + level
+      uint64_t morton;
+      int64_t t_base; // translation table of slot 0 of the cube's tree and level
+      int pg;
+   };
+   std::vector<DstExtra> dst_extra;  // parallel to L.dst until the tiles are built
 
    for (int t = 0; t < num_trees; t++) {
       const fftsvd_tree_flat& T = trees[t];
@@ -142,7 +151,14 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
 
       // ---- far field
       std::vector<int64_t> spec_of_cube(T.num_cubes, -1);
-      const int64_t t_base = (int64_t)(L.t_pairs.size() / 2);
+      // translation tables of this tree, each slot padded to a multiple of 16 complex values
+      std::vector<int64_t> tlev(T.depth + 1);
+      tlev[0] = (int64_t)(L.t_pairs.size() / 2);
+      for (int l = 0; l < T.depth; l++) {
+         const int nl = T.grid[l], Npl = 2 * nl - 1;
+         FFTSVD_REQUIRE(nl >= 2 && nl <= 12, "grid size out of range");
+         tlev[l + 1] = tlev[l] + 343LL * pad16(Npl * Npl * nl);
+      }
       for (int c = 0; c < T.num_cubes; c++) {
          const int lvl = T.cube_level[c];
          FFTSVD_REQUIRE(lvl >= 0 && lvl < T.depth, "cube level out of range");
@@ -163,7 +179,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          s.pv_off = (int64_t)(L.pv_pairs.size() / 2);
          s.spec_off = L.spectra_elems;
          spec_of_cube[c] = L.spectra_elems;
-         L.spectra_elems += pg;
+         L.spectra_elems += pad16(pg);
          for (int i = T.cube_panel_ptr[c]; i < T.cube_panel_ptr[c + 1]; i++) {
             FFTSVD_REQUIRE(T.cube_panels[i] >= 0 && T.cube_panels[i] < T.num_panels, "cube panel out of range");
             L.src_panels.push_back((int32_t)(po + T.cube_panels[i]));
@@ -223,7 +239,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
             FFTSVD_REQUIRE(std::abs(dx) <= 3 && std::abs(dy) <= 3 && std::abs(dz) <= 3, "interaction offset too large");
             FFTSVD_REQUIRE(std::abs(dx) > 1 || std::abs(dy) > 1 || std::abs(dz) > 1, "local cube in interaction list");
             const int slot = ((dx + 3) * 7 + (dy + 3)) * 7 + (dz + 3);
-            const int64_t toff = t_base + T.t_level_ptr[lvl] + (int64_t)slot * pg;
+            const int64_t toff = tlev[lvl] + (int64_t)slot * pad16(pg);
             FFTSVD_REQUIRE(T.t_level_ptr[lvl + 1] - T.t_level_ptr[lvl] == 343LL * pg, "translation table size mismatch");
             L.inter_pairs.push_back(spec_of_cube[s]);
             L.inter_pairs.push_back(toff);
@@ -232,19 +248,108 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          d.inter_cnt = cnt;
          int need = 2 * pg + 2 * (n * Np * H) + 2 * (n * n * H) + n3 + r + 2 * Np + 16;
          L.max_dst_smem_elems = std::max(L.max_dst_smem_elems, need);
-         if (cnt > 0) L.dst.push_back(d);
-         else L.uti.resize(d.uti_off), L.u_cm.resize(d.u_off), L.dst_points.resize(d.point_off);
+         if (cnt > 0) {
+            d.s_off = L.translated_elems;
+            L.translated_elems += pad16(pg);
+            L.dst.push_back(d);
+            const int32_t* ci = &T.cube_index[3 * c];
+            uint64_t code = 0;  // Morton order of the cube coordinates
+            for (int b = 0; b < 21; b++)
+               for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> b) & 1) << (3 * b + k);
+            dst_extra.push_back({t * 64 + lvl, code, tlev[lvl], pad16(pg)});
+         } else {
+            L.uti.resize(d.uti_off), L.u_cm.resize(d.u_off), L.dst_points.resize(d.point_off);
+         }
       }
-      // translation operators of this tree (unique tables: 316 non-local offsets per level)
-      const int64_t nt = T.t_level_ptr[T.depth];
-      L.t_pairs.insert(L.t_pairs.end(), T.t_ops, T.t_ops + 2 * nt);
+      // translation operators of this tree (unique tables: 316 non-local offsets per level),
+      // every slot padded with zeros to a multiple of 16 complex values
+      FFTSVD_REQUIRE((int64_t)(L.t_pairs.size() / 2) == tlev[0], "translation table offset");
       for (int lvl = 0; lvl < T.depth; lvl++) {
-         const int n = T.grid[lvl], Np = 2 * n - 1;
-         L.t_elems += 2LL * 316 * Np * Np * n;
+         const int n = T.grid[lvl], Np = 2 * n - 1, pg = Np * Np * n, pgp = pad16(pg);
+         FFTSVD_REQUIRE(T.t_level_ptr[lvl + 1] - T.t_level_ptr[lvl] == 343LL * pg, "translation table size mismatch");
+         for (int slot = 0; slot < 343; slot++) {
+            const double* src = T.t_ops + 2 * (T.t_level_ptr[lvl] + (int64_t)slot * pg);
+            L.t_pairs.insert(L.t_pairs.end(), src, src + 2 * pg);
+            L.t_pairs.insert(L.t_pairs.end(), 2 * (size_t)(pgp - pg), 0.0);
+         }
+         L.t_elems += 2LL * 316 * pg;
       }
+      FFTSVD_REQUIRE((int64_t)(L.t_pairs.size() / 2) == tlev[T.depth], "translation table size");
    }
    for (int o = 0; o < num_unknowns; o++)
       if (!row_written[o]) L.full_cover = false;
+
+   // ---- translation tiles: destinations of one tree and level in Morton order, greedily
+   // grouped while the tile's destinations, halo sources and interactions fit the limits
+   {
+      std::map<int, std::vector<int>> by_key;
+      for (int i = 0; i < (int)L.dst.size(); i++) by_key[dst_extra[i].key].push_back(i);
+      for (auto& kv : by_key) {
+         std::vector<int>& ids = kv.second;
+         std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return dst_extra[a].morton < dst_extra[b].morton; });
+         size_t pos = 0;
+         while (pos < ids.size()) {
+            TileDesc tile;
+            tile.ndst = tile.nsrc = tile.npairs = 0;
+            tile.pg = dst_extra[ids[pos]].pg;
+            tile.t_off = dst_extra[ids[pos]].t_base;
+            tile.dst_off = (int64_t)L.tile_dst.size();
+            tile.src_off = (int64_t)L.tile_src.size();
+            tile.pair_off = (int64_t)L.tile_pairs.size();
+            std::map<int64_t, int> halo;
+            while (pos < ids.size()) {
+               const DstDesc& d = L.dst[ids[pos]];
+               int fresh = 0;
+               for (int q = 0; q < d.inter_cnt; q++)
+                  if (!halo.count(L.inter_pairs[2 * (d.inter_off + q)])) fresh++;
+               // each destination's list is padded to whole groups of four with the zero slot
+               const int padded = (d.inter_cnt + 3) & ~3;
+               if (tile.ndst > 0 && (tile.ndst + 1 > kTileMaxDst || tile.nsrc + fresh > kTileMaxSrc ||
+                                     tile.npairs + padded > kTileMaxPairs))
+                  break;
+               FFTSVD_REQUIRE(padded <= kTileMaxPairs && fresh <= kTileMaxSrc, "interaction list too long");
+               L.tile_dst.push_back(d.s_off);
+               L.tile_dst_pairs.push_back(make_int2(tile.npairs, padded));
+               for (int q = 0; q < d.inter_cnt; q++) {
+                  const int64_t so = L.inter_pairs[2 * (d.inter_off + q)];
+                  const int64_t to = L.inter_pairs[2 * (d.inter_off + q) + 1];
+                  auto it = halo.find(so);
+                  int h;
+                  if (it == halo.end()) {
+                     h = tile.nsrc++;
+                     halo[so] = h;
+                     L.tile_src.push_back(so);
+                  } else {
+                     h = it->second;
+                  }
+                  const int64_t slot = (to - tile.t_off) / tile.pg;
+                  FFTSVD_REQUIRE(slot >= 0 && slot < 343 && (to - tile.t_off) % tile.pg == 0, "translation slot");
+                  L.tile_pairs.push_back(((uint32_t)h << 16) | (uint32_t)slot);
+               }
+               for (int q = d.inter_cnt; q < padded; q++) L.tile_pairs.push_back((uint32_t)kTileZeroSlot);
+               tile.npairs += padded;
+               tile.ndst++;
+               pos++;
+            }
+            L.tiles.push_back(tile);
+         }
+      }
+      std::stable_sort(L.tiles.begin(), L.tiles.end(), [](const TileDesc& a, const TileDesc& b) { return a.pg > b.pg; });
+      for (int i = 0; i < (int)L.tiles.size(); i++) {
+         const TileDesc& t = L.tiles[i];
+         if (L.tile_groups.empty() || L.tile_groups.back().pg != t.pg) {
+            TileGroup g;
+            g.pg = t.pg;
+            g.begin = i;
+            L.tile_groups.push_back(g);
+         }
+         TileGroup& g = L.tile_groups.back();
+         g.count++;
+         g.max_src = std::max(g.max_src, t.nsrc);
+         g.max_pairs = std::max(g.max_pairs, t.npairs);
+         g.max_dst = std::max(g.max_dst, t.ndst);
+      }
+   }
 
    // every index a kernel will form stays inside its buffer
    const int64_t npairs_d = (int64_t)L.d_pairs.size() / 2, npv = (int64_t)L.pv_pairs.size() / 2;
@@ -279,6 +384,35 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       }
    }
    for (int32_t v : L.dst_points) FFTSVD_REQUIRE(v >= 0 && v < L.total_points, "destination point index");
+   for (const DstDesc& d : L.dst) {
+      const int64_t pg = (int64_t)(2 * d.n - 1) * (2 * d.n - 1) * d.n;
+      FFTSVD_REQUIRE(d.s_off >= 0 && d.s_off + pg <= L.translated_elems, "translated spectrum out of range");
+   }
+   for (const TileDesc& t : L.tiles) {
+      FFTSVD_REQUIRE(t.ndst > 0 && t.ndst <= kTileMaxDst && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
+                         t.npairs > 0 && t.npairs <= kTileMaxPairs && t.pg > 0,
+                     "tile descriptor");
+      FFTSVD_REQUIRE(t.dst_off + t.ndst <= (int64_t)L.tile_dst.size(), "tile destinations out of range");
+      FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)L.tile_src.size(), "tile sources out of range");
+      FFTSVD_REQUIRE(t.pair_off + t.npairs <= (int64_t)L.tile_pairs.size(), "tile pairs out of range");
+      FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
+      FFTSVD_REQUIRE(t.pair_off % 4 == 0, "tile pairs not aligned");
+      for (int i = 0; i < t.ndst; i++) {
+         const int2 dp = L.tile_dst_pairs[t.dst_off + i];
+         FFTSVD_REQUIRE(dp.x >= 0 && dp.y >= 0 && dp.x + dp.y <= t.npairs && dp.x % 4 == 0 && dp.y % 4 == 0,
+                        "tile destination pairs out of range");
+         const int64_t so = L.tile_dst[t.dst_off + i];
+         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= L.translated_elems, "tile destination spectrum out of range");
+      }
+      for (int i = 0; i < t.nsrc; i++) {
+         const int64_t so = L.tile_src[t.src_off + i];
+         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= L.spectra_elems, "tile source spectrum out of range");
+      }
+      for (int i = 0; i < t.npairs; i++) {
+         const uint32_t pr = L.tile_pairs[t.pair_off + i];
+         FFTSVD_REQUIRE((int)(pr >> 16) < t.nsrc && (pr & 0xffffu) <= (uint32_t)kTileZeroSlot, "tile pair out of range");
+      }
+   }
    for (int64_t k = 0; k < (int64_t)L.point_out.size(); k++) {
       FFTSVD_REQUIRE(L.point_out[k] >= 0 && L.point_out[k] < num_unknowns, "point without an output row");
       FFTSVD_REQUIRE(L.point_panel[k] >= -1 && L.point_panel[k] < L.total_panels - 1, "jump panel index");
@@ -306,10 +440,13 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       }
       kb.elems[1] = vt + pv + spec + 2.0 * (double)L.src_panels.size();  // + gathered {xs, xd}
       kb.fixed[1] = 4.0 * (double)L.src_panels.size();
-      kb.elems[2] = spec + (double)L.t_elems + uti + u + nq;              // spectra, T, UTI, U, staging writes
-      kb.fixed[2] = 4.0 * (double)L.dst_points.size() + 16.0 * (double)(L.inter_pairs.size() / 2);
-      kb.elems[3] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
-      kb.fixed[3] = 4.0 * (lcols + lrows) + nq * (8.0 + 4.0 + 4.0 + 8.0); // indices, y, maps, jump
+      const double sbuf = 2.0 * (double)L.translated_elems;
+      kb.elems[2] = spec + (double)L.t_elems + sbuf;                      // spectra, T, translated writes
+      kb.fixed[2] = 4.0 * (double)L.tile_pairs.size() + 8.0 * (double)(L.tile_src.size() + L.tile_dst.size());
+      kb.elems[3] = sbuf + uti + u + nq;                                  // translated, UTI, U, staging writes
+      kb.fixed[3] = 4.0 * (double)L.dst_points.size();
+      kb.elems[4] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
+      kb.fixed[4] = 4.0 * (lcols + lrows) + nq * (8.0 + 4.0 + 4.0 + 8.0); // indices, y, maps, jump
    }
    // group by grid size (largest first), heavy cubes first within a group so the
    // long blocks start early; each group is one launch with its own shared memory
@@ -330,16 +467,18 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       return 2 * pg + 2 * (n * Np * H) + 2 * (n * n * H) + n * n * n + d.r + 2 * Np + 16;
    };
    for (int i = 0; i < (int)L.src.size(); i++) {
-      if (L.src_groups.empty() || L.src_groups.back().n != L.src[i].n) L.src_groups.push_back({L.src[i].n, i, 0, 0});
+      if (L.src_groups.empty() || L.src_groups.back().n != L.src[i].n) L.src_groups.push_back({L.src[i].n, i, 0, 0, 0});
       LaunchGroup& g = L.src_groups.back();
       g.count++;
       g.smem_elems = std::max(g.smem_elems, src_need(L.src[i]));
+      g.max_rank = std::max(g.max_rank, L.src[i].r);
    }
    for (int i = 0; i < (int)L.dst.size(); i++) {
-      if (L.dst_groups.empty() || L.dst_groups.back().n != L.dst[i].n) L.dst_groups.push_back({L.dst[i].n, i, 0, 0});
+      if (L.dst_groups.empty() || L.dst_groups.back().n != L.dst[i].n) L.dst_groups.push_back({L.dst[i].n, i, 0, 0, 0});
       LaunchGroup& g = L.dst_groups.back();
       g.count++;
       g.smem_elems = std::max(g.smem_elems, dst_need(L.dst[i]));
+      g.max_rank = std::max(g.max_rank, L.dst[i].r);
    }
    return L;
 }
@@ -402,7 +541,13 @@ __global__ void join_kernel(int64_t total, const int32_t* __restrict__ phi_idx, 
    }
 }
 
-constexpr int kFarThreads = 128;
+constexpr int kFarThreads = 512;  // upper bound; each launch group picks its own block size
+
+// block size of a block-per-cube launch: enough threads for the spectrum of one cube
+static int far_threads(int n) {
+   const int pg = (2 * n - 1) * (2 * n - 1) * n;
+   return pg <= 256 ? 128 : pg <= 512 ? 256 : 512;
+}
 constexpr int kChunk = 1024;
 
 // One block per source cube: a = VT x (both layers), g = PV_s a_s + PV_d a_d on
@@ -502,14 +647,155 @@ __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
    }
 }
 
-// One block per destination cube: S = sum over interacting sources of
-// T[offset] .* F_source, c2r DFT cropped at offset n/2 and scaled by 1/(2n-1)^3,
-// u = UTI g, values U u written to this level's staging row of each point.
+constexpr int kTileRowBytes = 128;                               // shared-memory row per slot/source and chunk
+constexpr int kTranslateThreads = kTileMaxDst * kTileRowBytes / 16;  // one thread per destination unit
+
+__device__ inline void cp_async16(void* smem, const void* gmem) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() {
+   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// 16 bytes of spectrum: two FP32 complex values or one FP64 complex value
+template <typename T> struct Pack16;
+template <> struct Pack16<float> {
+   using V = float4;
+   __device__ static inline V zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+   __device__ static inline void add(V& a, const V& b) {
+      a.x += b.x;
+      a.y += b.y;
+      a.z += b.z;
+      a.w += b.w;
+   }
+   __device__ static inline void fma(V& acc, const V& a, const V& b) {  // acc += a * b, two complex
+      acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
+      acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
+      acc.z = fmaf(a.z, b.z, fmaf(-a.w, b.w, acc.z));
+      acc.w = fmaf(a.z, b.w, fmaf(a.w, b.z, acc.w));
+   }
+};
+template <> struct Pack16<double> {
+   using V = double2;
+   __device__ static inline V zero() { return make_double2(0.0, 0.0); }
+   __device__ static inline void add(V& a, const V& b) {
+      a.x += b.x;
+      a.y += b.y;
+   }
+   __device__ static inline void fma(V& acc, const V& a, const V& b) {
+      acc.x = ::fma(a.x, b.x, ::fma(-a.y, b.y, acc.x));
+      acc.y = ::fma(a.x, b.y, ::fma(a.y, b.x, acc.y));
+   }
+};
+
+// One block per (tile, range of frequency chunks): S[d][f] = sum over the
+// interactions of destination d of T[slot][f] * F[source][f] (Cube_multiply_T,
+// Cube.c:2062-2111).  Frequencies are processed in chunks of one kTileRowBytes
+// row per slot/source.  The chunk of all 343 translation slots of the tile's
+// tree and level and the chunk of every halo source spectrum are copied to
+// shared memory with cp.async, one chunk ahead of the computation (double
+// buffer), so each table entry and spectrum crosses L2 once per tile instead of
+// once per interaction.  Rows are padded to a multiple of 16 complex values, so
+// every copy is a full aligned 16 bytes.  Each thread owns one 16-byte unit
+// (two FP32 or one FP64 complex) of one destination's row.
+template <typename T>
+__global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
+    const TileDesc* __restrict__ tiles, const int64_t* __restrict__ tile_src, const int64_t* __restrict__ tile_dst,
+    const int2* __restrict__ tile_dst_pairs, const uint32_t* __restrict__ tile_pairs,
+    const typename Vec2<T>::type* __restrict__ tops, const typename Vec2<T>::type* __restrict__ spectra,
+    typename Vec2<T>::type* __restrict__ S, int chunks_per_block) {
+   using T2 = typename Vec2<T>::type;
+   using V = typename Pack16<T>::V;
+   constexpr int U = kTileRowBytes / 16;                 // 16-byte units per row
+   constexpr int CH = kTileRowBytes / (int)sizeof(T2);   // complex values per row
+   constexpr int PER16 = 16 / (int)sizeof(T2);           // complex values per unit
+   extern __shared__ __align__(16) char smem_raw[];
+   const TileDesc t = tiles[blockIdx.x];
+   const int nchunks = t.pg / CH;
+   const int kbeg = blockIdx.y * chunks_per_block;
+   if (kbeg >= nchunks) return;
+   const int kend = min(nchunks, kbeg + chunks_per_block);
+   char* p = smem_raw;
+   T2* Tb0 = carve<T2>(p, (kTileZeroSlot + 1) * CH);  // 343 slots and the zero row
+   T2* Tb1 = carve<T2>(p, (kTileZeroSlot + 1) * CH);
+   T2* Fb0 = carve<T2>(p, t.nsrc * CH);
+   T2* Fb1 = carve<T2>(p, t.nsrc * CH);
+   uint32_t* pairs = carve<uint32_t>(p, t.npairs);
+   int2* dinfo = carve<int2>(p, t.ndst);
+   int64_t* srcoff = carve<int64_t>(p, t.nsrc);
+   int64_t* dstoff = carve<int64_t>(p, t.ndst);
+   // pairs pre-scaled to unit offsets of the chunk rows: (source row << 16) | slot row
+   for (int i = threadIdx.x; i < t.npairs; i += blockDim.x) {
+      const uint32_t pr = tile_pairs[t.pair_off + i];
+      pairs[i] = ((pr >> 16) * (uint32_t)U) << 16 | ((pr & 0xffffu) * (uint32_t)U);
+   }
+   for (int i = threadIdx.x; i < t.ndst; i += blockDim.x) {
+      dinfo[i] = tile_dst_pairs[t.dst_off + i];
+      dstoff[i] = tile_dst[t.dst_off + i];
+   }
+   for (int i = threadIdx.x; i < t.nsrc; i += blockDim.x) srcoff[i] = tile_src[t.src_off + i];
+   for (int i = threadIdx.x; i < CH; i += blockDim.x) {
+      Tb0[kTileZeroSlot * CH + i] = Cx<T>::make(T(0), T(0));
+      Tb1[kTileZeroSlot * CH + i] = Cx<T>::make(T(0), T(0));
+   }
+   __syncthreads();
+   auto stage = [&](int k, T2* Tb, T2* Fb) {
+      const int f0 = k * CH;
+      for (int i = threadIdx.x; i < kTileZeroSlot * U; i += blockDim.x) {
+         const int s = i / U, u = i % U;
+         cp_async16(&Tb[s * CH + u * PER16], &tops[t.t_off + (int64_t)s * t.pg + f0 + u * PER16]);
+      }
+      for (int i = threadIdx.x; i < t.nsrc * U; i += blockDim.x) {
+         const int s = i / U, u = i % U;
+         cp_async16(&Fb[s * CH + u * PER16], &spectra[srcoff[s] + f0 + u * PER16]);
+      }
+      cp_async_commit();
+   };
+   stage(kbeg, Tb0, Fb0);
+   for (int k = kbeg; k < kend; k++) {
+      const bool odd = (k - kbeg) & 1;
+      if (k + 1 < kend) {
+         stage(k + 1, odd ? Tb0 : Tb1, odd ? Fb0 : Fb1);
+         cp_async_wait<1>();
+      } else {
+         cp_async_wait<0>();
+      }
+      __syncthreads();
+      const V* Ts = reinterpret_cast<const V*>(odd ? Tb1 : Tb0);
+      const V* Fs = reinterpret_cast<const V*>(odd ? Fb1 : Fb0);
+      const int f0 = k * CH;
+      // thread -> (destination, unit)
+      for (int item = threadIdx.x; item < t.ndst * U; item += blockDim.x) {
+         const int d = item / U, u = item % U;
+         const int2 di = dinfo[d];
+         V acc = Pack16<T>::zero(), acc1 = Pack16<T>::zero();  // two chains of dependent FMAs
+         // four pairs per 16-byte load; lists are padded to groups of four with the zero row
+         const uint4* pp = reinterpret_cast<const uint4*>(pairs + di.x);
+         for (int q = 0; q < (di.y >> 2); q++) {
+            const uint4 pr = pp[q];
+            Pack16<T>::fma(acc, Ts[(pr.x & 0xffffu) + u], Fs[(pr.x >> 16) + u]);
+            Pack16<T>::fma(acc1, Ts[(pr.y & 0xffffu) + u], Fs[(pr.y >> 16) + u]);
+            Pack16<T>::fma(acc, Ts[(pr.z & 0xffffu) + u], Fs[(pr.z >> 16) + u]);
+            Pack16<T>::fma(acc1, Ts[(pr.w & 0xffffu) + u], Fs[(pr.w >> 16) + u]);
+         }
+         Pack16<T>::add(acc, acc1);
+         *reinterpret_cast<V*>(&S[dstoff[d] + f0 + u * PER16]) = acc;
+      }
+      __syncthreads();  // this buffer is refilled by the stage issued in the next iteration
+   }
+}
+
+// One block per destination cube: the translated spectrum S, c2r DFT cropped at
+// offset n/2 and scaled by 1/(2n-1)^3, u = UTI g, values U u written to this
+// level's staging row of each point (Cube_multiply_U_UTI_IFFT, Cube.c:2156-2225).
 template <typename T>
 __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
-    const DstDesc* __restrict__ cubes, const int32_t* __restrict__ dst_points, const longlong2* __restrict__ inter,
-    const typename Vec2<T>::type* __restrict__ tops, const typename Vec2<T>::type* __restrict__ spectra,
-    const T* __restrict__ uti, const T* __restrict__ ucm, T* __restrict__ staging, int64_t total_points) {
+    const DstDesc* __restrict__ cubes, const int32_t* __restrict__ dst_points,
+    const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
+    T* __restrict__ staging, int64_t total_points) {
    using T2 = typename Vec2<T>::type;
    extern __shared__ __align__(16) char smem_raw[];
    const DstDesc c = cubes[blockIdx.x];
@@ -529,15 +815,7 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
       Cx<T>::cis(k, Np, &cs, &sn);
       tw[k] = Cx<T>::make(cs, sn);
    }
-   // translation: accumulate over sources, frequencies across threads
-   for (int f = tid; f < pg; f += blockDim.x) {
-      T2 acc = Cx<T>::make(T(0), T(0));
-      for (int q = 0; q < c.inter_cnt; q++) {
-         const longlong2 pr = inter[c.inter_off + q];
-         acc = Cx<T>::fma(tops[pr.y + f], spectra[pr.x + f], acc);
-      }
-      S[f] = acc;
-   }
+   for (int f = tid; f < pg; f += blockDim.x) S[f] = translated[c.s_off + f];
    __syncthreads();
    // inverse along i (output i < n only)
    for (int idx = tid; idx < n * Np * H; idx += blockDim.x) {
@@ -587,6 +865,435 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
    }
 }
 
+// ---- one warp per cube for the small grids of the fine levels
+//
+// Most cubes sit on the finest levels, where the grid is 4^3 and a cube holds a
+// few panels: a whole block per cube spends its time on launch and barrier
+// latency.  These kernels give each cube one warp (several cubes per block),
+// replace barriers by __syncwarp, and fix the grid edge at compile time.  The
+// arithmetic is the block kernels' (same DFT factorisation and twiddles).
+
+constexpr int kWarpCubes = 4;  // cubes (warps) per block
+constexpr int kWarpThreads = 32 * kWarpCubes;
+
+template <int N>
+struct SmallGrid {
+   static constexpr int Np = 2 * N - 1, H = N, OFF = N / 2, N3 = N * N * N;
+   static constexpr int NA = N * N * H, NB = N * Np * H, PG = Np * Np * H;
+   static constexpr int kFwdElems = NA + NB + (N3 + 1) / 2;  // A, B and the real grid g, in complex units
+   static constexpr int kBwdElems = PG + NB;                 // S (later P2, u) and P1 (later g)
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(kWarpThreads, 12) far_forward_warp_kernel(
+    const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
+    const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra) {
+   using T2 = typename Vec2<T>::type;
+   using G = SmallGrid<N>;
+   constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   __shared__ __align__(16) T2 work[kWarpCubes][G::kFwdElems];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(-2 pi i k / Np)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, -sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const SrcDesc c = cubes[cube];
+   T2* A = work[warp];
+   T2* B = A + G::NA;
+   T* g = reinterpret_cast<T*>(B + G::NB);
+   const int m = c.m, r = c.r;  // r <= 32: lane j owns row j of VT
+   // a = VT x, panels broadcast from the lane that loaded them, 32 at a time
+   T as = T(0), ad = T(0);
+   const T* row = vt + c.vt_off + (int64_t)min(lane, r - 1) * m;
+   for (int base = 0; base < m; base += 32) {
+      T2 xv = Cx<T>::make(T(0), T(0));
+      if (base + lane < m) xv = xsd[src_panels[c.panel_off + base + lane]];
+      const int cnt = min(32, m - base);
+#pragma unroll 8
+      for (int i = 0; i < cnt; i++) {
+         const T xs = __shfl_sync(kAll, xv.x, i), xd = __shfl_sync(kAll, xv.y, i);
+         if (lane < r) {
+            const T v = row[base + i];
+            as += v * xs;
+            ad += v * xd;
+         }
+      }
+   }
+   // grid charges g = PV_s a_s + PV_d a_d, lanes over grid points
+   constexpr int QT = (N3 + 31) / 32;
+   T acc[QT];
+#pragma unroll
+   for (int t = 0; t < QT; t++) acc[t] = T(0);
+   const T2* pvc = pv + c.pv_off;
+#pragma unroll 4
+   for (int j = 0; j < r; j++) {
+      const T s = __shfl_sync(kAll, as, j), d = __shfl_sync(kAll, ad, j);
+#pragma unroll
+      for (int t = 0; t < QT; t++) {
+         const int q = lane + 32 * t;
+         if (q < N3) {
+            const T2 w = pvc[(int64_t)j * N3 + q];
+            acc[t] += w.x * s + w.y * d;
+         }
+      }
+   }
+#pragma unroll
+   for (int t = 0; t < QT; t++)
+      if (lane + 32 * t < N3) g[lane + 32 * t] = acc[t];
+   __syncwarp();
+   // DFT along k (input index k + OFF), half spectrum kf < H
+   for (int idx = lane; idx < G::NA; idx += 32) {
+      const int kf = idx % H, ij = idx / H;
+      const T* line = g + ij * N;
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+         const T2 w = tw[((k + OFF) * kf) % Np];
+         a.x += line[k] * w.x;
+         a.y += line[k] * w.y;
+      }
+      A[idx] = a;
+   }
+   __syncwarp();
+   // along j
+   for (int idx = lane; idx < G::NB; idx += 32) {
+      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int j = 0; j < N; j++) a = Cx<T>::fma(A[(i * N + j) * H + kf], tw[((j + OFF) * jf) % Np], a);
+      B[idx] = a;
+   }
+   __syncwarp();
+   // along i, straight to global
+   T2* out = spectra + c.spec_off;
+   for (int idx = lane; idx < G::PG; idx += 32) {
+      const int kf = idx % H, jf = (idx / H) % Np, fi = idx / (H * Np);
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int i = 0; i < N; i++) a = Cx<T>::fma(B[(i * Np + jf) * H + kf], tw[((i + OFF) * fi) % Np], a);
+      out[idx] = a;
+   }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(kWarpThreads) far_backward_warp_kernel(
+    const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
+    const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
+    T* __restrict__ staging, int64_t total_points) {
+   using T2 = typename Vec2<T>::type;
+   using G = SmallGrid<N>;
+   constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   __shared__ __align__(16) T2 work[kWarpCubes][G::kBwdElems];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(+2 pi i k / Np)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const DstDesc c = cubes[cube];
+   T2* S = work[warp];
+   T2* P1 = S + G::PG;
+   for (int f = lane; f < G::PG; f += 32) S[f] = translated[c.s_off + f];
+   __syncwarp();
+   // inverse along i (output i < N only)
+   for (int idx = lane; idx < G::NB; idx += 32) {
+      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int fi = 0; fi < Np; fi++) a = Cx<T>::fma(S[(fi * Np + jf) * H + kf], tw[((i + OFF) * fi) % Np], a);
+      P1[idx] = a;
+   }
+   __syncwarp();
+   // inverse along j (output j < N only), into the space of S
+   T2* P2 = S;
+   for (int idx = lane; idx < G::NA; idx += 32) {
+      const int kf = idx % H, j = (idx / H) % N, i = idx / (H * N);
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int jf = 0; jf < Np; jf++) a = Cx<T>::fma(P1[(i * Np + jf) * H + kf], tw[((j + OFF) * jf) % Np], a);
+      P2[idx] = a;
+   }
+   __syncwarp();
+   // Hermitian half along k -> real, cropped, scaled; into the space of P1
+   T* g = reinterpret_cast<T*>(P1);
+   const T scale = T(1) / (T)(Np * Np * Np);
+   for (int q = lane; q < N3; q += 32) {
+      const int k = q % N, ij = q / N;
+      const T2* line = P2 + ij * H;
+      T a = line[0].x;
+#pragma unroll
+      for (int kf = 1; kf < H; kf++) {
+         const T2 w = tw[((k + OFF) * kf) % Np];
+         a += T(2) * (line[kf].x * w.x - line[kf].y * w.y);
+      }
+      g[q] = a * scale;
+   }
+   __syncwarp();
+   // u = UTI g: four lanes per row, eight rows per pass; u into the space of S
+   T* u = reinterpret_cast<T*>(S);
+   const int r = c.r, quarter = lane & 3;
+   for (int j0 = 0; j0 < r; j0 += 8) {
+      const int j = j0 + (lane >> 2);
+      T s = T(0);
+      if (j < r) {
+         const T* urow = uti + c.uti_off + (int64_t)j * N3;
+#pragma unroll 8
+         for (int q = quarter; q < N3; q += 4) s += urow[q] * g[q];
+      }
+      s += __shfl_xor_sync(kAll, s, 1);
+      s += __shfl_xor_sync(kAll, s, 2);
+      if (quarter == 0 && j < r) u[j] = s;
+   }
+   __syncwarp();
+   // U u -> staging (each point belongs to exactly one cube of this level)
+   T* stage = staging + (int64_t)c.stage * total_points;
+   const T* ucol = ucm + c.u_off;
+   for (int q = lane; q < c.p; q += 32) {
+      T a = T(0);
+#pragma unroll 4
+      for (int j = 0; j < r; j++) a += ucol[(int64_t)j * c.p + q] * u[j];
+      stage[dst_points[c.point_off + q]] = a;
+   }
+}
+
+// ---- the 4^3 grid (7 x 7 x 4 half spectrum) with the DFT held in registers
+//
+// Lane L = 16 hi + 4 jp + kq and register h address grid point q = L + 32 h, i.e.
+// (i, j, k) = (2 h + hi, jp, kq).  Each separable DFT stage gathers its inputs
+// with shuffles from the lanes that hold them, and every twiddle is either a
+// compile-time entry of the 7-point table or precomputed per lane, so the
+// stages run without index arithmetic.  Spectrum row fi (28 complex values,
+// (jf, kf) = (jp + 4 hi, kq)) is written or read by lanes 0..27 as one
+// contiguous segment.  Same factorisation and twiddles as the generic kernels.
+
+template <typename T>
+__device__ inline typename Vec2<T>::type shfl_c(typename Vec2<T>::type v, int src) {
+   v.x = __shfl_sync(0xffffffffu, v.x, src);
+   v.y = __shfl_sync(0xffffffffu, v.y, src);
+   return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forward_n4_kernel(
+    const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
+    const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra) {
+   using T2 = typename Vec2<T>::type;
+   constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;  // ROW: complex values per fi
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(-2 pi i k / 7)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, -sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const SrcDesc c = cubes[cube];
+   const int m = c.m, r = c.r;  // r <= 32: lane j owns row j of VT
+   const int kq = lane & 3, jp = (lane >> 2) & 3, hi = lane >> 4;
+   // per-lane twiddles: stage k (kf = kq) and stage j (jf = jp, jp + 4)
+   T2 w1[N], w2[2][N], W[Np];
+#pragma unroll
+   for (int k = 0; k < N; k++) w1[k] = tw[((k + OFF) * kq) % Np];
+#pragma unroll
+   for (int sl = 0; sl < 2; sl++)
+#pragma unroll
+      for (int j = 0; j < N; j++) w2[sl][j] = tw[((j + OFF) * (jp + 4 * sl)) % Np];
+#pragma unroll
+   for (int q = 0; q < Np; q++) W[q] = tw[q];
+   // a = VT x
+   T as = T(0), ad = T(0);
+   const T* row = vt + c.vt_off + (int64_t)min(lane, r - 1) * m;
+   for (int base = 0; base < m; base += 32) {
+      T2 xv = Cx<T>::make(T(0), T(0));
+      if (base + lane < m) xv = xsd[src_panels[c.panel_off + base + lane]];
+      const int cnt = min(32, m - base);
+#pragma unroll 8
+      for (int i = 0; i < cnt; i++) {
+         const T xs = __shfl_sync(kAll, xv.x, i), xd = __shfl_sync(kAll, xv.y, i);
+         if (lane < r) {
+            const T v = row[base + i];
+            as += v * xs;
+            ad += v * xd;
+         }
+      }
+   }
+   // grid charges at q = lane and lane + 32
+   T g0 = T(0), g1 = T(0);
+   const T2* pvc = pv + c.pv_off + lane;
+#pragma unroll 4
+   for (int j = 0; j < r; j++) {
+      const T s = __shfl_sync(kAll, as, j), d = __shfl_sync(kAll, ad, j);
+      const T2 w0 = pvc[(int64_t)j * N3], w1v = pvc[(int64_t)j * N3 + 32];
+      g0 += w0.x * s + w0.y * d;
+      g1 += w1v.x * s + w1v.y * d;
+   }
+   // along k: lane computes kf = kq of line (i, jp) from the four lanes of its quad
+   T2 A[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T g = h ? g1 : g0;
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+         const T gk = __shfl_sync(kAll, g, (lane & ~3) | k);
+         a.x += gk * w1[k].x;
+         a.y += gk * w1[k].y;
+      }
+      A[h] = a;
+   }
+   // along j: lane computes jf = jp and jp + 4 of column (i, kq)
+   T2 B[2][2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      T2 Aj[N];
+#pragma unroll
+      for (int j = 0; j < N; j++) Aj[j] = shfl_c<T>(A[h], (lane & ~12) | (j << 2));
+#pragma unroll
+      for (int sl = 0; sl < 2; sl++) {
+         T2 b = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int j = 0; j < N; j++) b = Cx<T>::fma(Aj[j], w2[sl][j], b);
+         B[h][sl] = b;
+      }
+   }
+   // along i: lanes hi = 0 finish jf = jp, lanes hi = 1 jf = jp + 4, exchanging
+   // with lane ^ 16 the two values of i (2 h + hi) that the partner needs
+   T2 Bi[N];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T2 mine = hi ? B[h][1] : B[h][0];
+      const T2 recv = shfl_c<T>(hi ? B[h][0] : B[h][1], lane ^ 16);
+      Bi[2 * h] = hi ? recv : mine;
+      Bi[2 * h + 1] = hi ? mine : recv;
+   }
+   T2* out = spectra + c.spec_off + lane;
+   if (lane < ROW) {
+#pragma unroll
+      for (int fi = 0; fi < Np; fi++) {
+         T2 o = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int i = 0; i < N; i++) o = Cx<T>::fma(Bi[i], W[((i + OFF) * fi) % Np], o);
+         out[fi * ROW] = o;
+      }
+   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_backward_n4_kernel(
+    const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
+    const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
+    T* __restrict__ staging, int64_t total_points) {
+   using T2 = typename Vec2<T>::type;
+   constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   __shared__ __align__(16) T2 work[kWarpCubes][N * ROW];  // P1 [i][jf][kf], later g and u
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(+2 pi i k / 7)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const DstDesc c = cubes[cube];
+   const int kq = lane & 3, jp = (lane >> 2) & 3;
+   T2 W[Np], w2[Np], w3[N];
+#pragma unroll
+   for (int q = 0; q < Np; q++) W[q] = tw[q];
+#pragma unroll
+   for (int jf = 0; jf < Np; jf++) w2[jf] = tw[((jp + OFF) * jf) % Np];
+#pragma unroll
+   for (int kf = 0; kf < N; kf++) w3[kf] = tw[((kq + OFF) * kf) % Np];
+   T2* P1 = work[warp];
+   // inverse along i (i < 4) of column (jf, kf) = (jp + 4 hi, kq), straight from global
+   if (lane < ROW) {
+      T2 S[Np];
+      const T2* in = translated + c.s_off + lane;
+#pragma unroll
+      for (int fi = 0; fi < Np; fi++) S[fi] = in[fi * ROW];
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+         T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int fi = 0; fi < Np; fi++) a = Cx<T>::fma(S[fi], W[((i + OFF) * fi) % Np], a);
+         P1[i * ROW + lane] = a;
+      }
+   }
+   __syncwarp();
+   // inverse along j (j = jp < 4) for i = 2 h + hi, kf = kq
+   T2 P2[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const int i = 2 * h + (lane >> 4);
+      T2 a = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int jf = 0; jf < Np; jf++) a = Cx<T>::fma(P1[i * ROW + jf * N + kq], w2[jf], a);
+      P2[h] = a;
+   }
+   // Hermitian half along k -> real grid value (i, jp, k = kq), cropped and scaled
+   const T scale = T(1) / (T)(Np * Np * Np);
+   T g[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T2 p0 = shfl_c<T>(P2[h], lane & ~3);
+      T a = p0.x;
+#pragma unroll
+      for (int kf = 1; kf < N; kf++) {
+         const T2 pk = shfl_c<T>(P2[h], (lane & ~3) | kf);
+         a += T(2) * (pk.x * w3[kf].x - pk.y * w3[kf].y);
+      }
+      g[h] = a * scale;
+   }
+   __syncwarp();  // P1 is reused for g and u
+   T* gs = reinterpret_cast<T*>(P1);
+   gs[lane] = g[0];
+   gs[lane + 32] = g[1];
+   T* u = gs + N3;
+   __syncwarp();
+   // u = UTI g: four lanes per row, eight rows per pass
+   const int r = c.r, quarter = lane & 3;
+   for (int j0 = 0; j0 < r; j0 += 8) {
+      const int j = j0 + (lane >> 2);
+      T sum = T(0);
+      if (j < r) {
+         const T* urow = uti + c.uti_off + (int64_t)j * N3;
+#pragma unroll
+         for (int q = quarter; q < N3; q += 4) sum += urow[q] * gs[q];
+      }
+      sum += __shfl_xor_sync(kAll, sum, 1);
+      sum += __shfl_xor_sync(kAll, sum, 2);
+      if (quarter == 0 && j < r) u[j] = sum;
+   }
+   __syncwarp();
+   // U u -> staging (each point belongs to exactly one cube of this level)
+   T* stage = staging + (int64_t)c.stage * total_points;
+   const T* ucol = ucm + c.u_off;
+   for (int q = lane; q < c.p; q += 32) {
+      T a = T(0);
+#pragma unroll 4
+      for (int j = 0; j < r; j++) a += ucol[(int64_t)j * c.p + q] * u[j];
+      stage[dst_points[c.point_off + q]] = a;
+   }
+}
+
 constexpr int kNearThreads = 128;
 
 template <typename T> struct NearLoad;
@@ -606,35 +1313,73 @@ template <> struct NearLoad<double> {
    }
 };
 
-// One block per leaf: y[out(p)] = (D_s xs + D_d xd)[p] + sum_levels staging[p] + jump(p) xd(p).
+// One warp per leaf, blockDim.x / 32 leaves per block, each warp with xl_stride
+// complex values of shared memory for its gathered panel values:
+// y[out(p)] = (D_s xs + D_d xd)[p] + jump(p) xd(p).  The far field is added
+// afterwards by far_add_kernel, so this kernel does not wait for it.
 template <typename T>
 __global__ void __launch_bounds__(kNearThreads) near_kernel(
-    const LeafDesc* __restrict__ leaves, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
-    const typename Vec2<T>::type* __restrict__ d, const typename Vec2<T>::type* __restrict__ xsd,
-    const T* __restrict__ staging, int stage_levels, int64_t total_points, const int32_t* __restrict__ point_out,
+    const LeafDesc* __restrict__ leaves, int n_leaf, int xl_stride, const int32_t* __restrict__ rows,
+    const int32_t* __restrict__ cols, const typename Vec2<T>::type* __restrict__ d,
+    const typename Vec2<T>::type* __restrict__ xsd, const int32_t* __restrict__ point_out,
     const int32_t* __restrict__ point_panel, const double* __restrict__ point_jump,
     const int32_t* __restrict__ phi_idx, const double* __restrict__ phi_scale, const double* __restrict__ x,
     double* __restrict__ y) {
    using T2 = typename Vec2<T>::type;
    extern __shared__ __align__(16) char smem_raw[];
-   const LeafDesc L = leaves[blockIdx.x];
-   T2* xl = reinterpret_cast<T2*>(smem_raw);
-   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-   for (int i = tid; i < L.ncols; i += blockDim.x) xl[i] = xsd[cols[L.col_off + i]];
-   __syncthreads();
-   for (int rr = warp; rr < L.nrows; rr += nwarps) {
-      const T2* row = d + L.d_off + (int64_t)rr * L.ncols;
-      T acc = T(0);
-      for (int c = 2 * lane; c < L.ncols; c += 64) acc += NearLoad<T>::dot2(row, c, xl);
-      acc = warp_sum(acc);
-      if (lane == 0) {
-         const int pnt = rows[L.row_off + rr];
-         double v = (double)acc;
-         for (int l = 0; l < stage_levels; l++) v += (double)staging[(int64_t)l * total_points + pnt];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int leaf = blockIdx.x * (blockDim.x >> 5) + warp;
+   if (leaf >= n_leaf) return;
+   const LeafDesc L = leaves[leaf];
+   T2* xl = reinterpret_cast<T2*>(smem_raw) + (size_t)warp * xl_stride;
+   for (int i = lane; i < L.ncols; i += 32) xl[i] = xsd[cols[L.col_off + i]];
+   __syncwarp();
+   for (int r0 = 0; r0 < L.nrows; r0 += 32) {
+      const int rend = min(32, L.nrows - r0);
+      // row sums, two rows at a time; lane rr keeps the sum of row r0 + rr
+      T mine = T(0);
+      int rr = 0;
+      for (; rr + 1 < rend; rr += 2) {
+         const T2* row0 = d + L.d_off + (int64_t)(r0 + rr) * L.ncols;
+         const T2* row1 = row0 + L.ncols;
+         T a0 = T(0), a1 = T(0);
+         for (int c = 2 * lane; c < L.ncols; c += 64) {
+            a0 += NearLoad<T>::dot2(row0, c, xl);
+            a1 += NearLoad<T>::dot2(row1, c, xl);
+         }
+         a0 = warp_sum(a0);
+         a1 = warp_sum(a1);
+         if (lane == rr) mine = a0;
+         if (lane == rr + 1) mine = a1;
+      }
+      if (rr < rend) {
+         const T2* row0 = d + L.d_off + (int64_t)(r0 + rr) * L.ncols;
+         T a0 = T(0);
+         for (int c = 2 * lane; c < L.ncols; c += 64) a0 += NearLoad<T>::dot2(row0, c, xl);
+         a0 = warp_sum(a0);
+         if (lane == rr) mine = a0;
+      }
+      if (lane < rend) {
+         const int pnt = rows[L.row_off + r0 + lane];
+         double v = (double)mine;
          const int k = point_panel[pnt];
          if (k >= 0) v += point_jump[pnt] * (phi_scale[k] * x[phi_idx[k]]);
          y[point_out[pnt]] = v;
       }
+   }
+}
+
+// y[out(p)] += sum over levels of staging[level][p], for every leaf row p (each
+// output row has exactly one leaf row, so every element has one writer).
+template <typename T>
+__global__ void far_add_kernel(int64_t nrows, const int32_t* __restrict__ rows, const T* __restrict__ staging,
+                               int stage_levels, int64_t total_points, const int32_t* __restrict__ point_out,
+                               double* __restrict__ y) {
+   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x) {
+      const int pnt = rows[i];
+      double v = 0.0;
+      for (int l = 0; l < stage_levels; l++) v += (double)staging[(int64_t)l * total_points + pnt];
+      y[point_out[pnt]] += v;
    }
 }
 
@@ -678,6 +1423,7 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    point_jump_.upload(L.point_jump);
    leaves_.upload(L.leaves);
    leaf_rows_.upload(L.leaf_rows);
+   n_rows_ = (int64_t)L.leaf_rows.size();
    leaf_cols_.upload(L.leaf_cols);
    upload_pairs<T>(d_, L.d_pairs);
    src_.upload(L.src);
@@ -688,13 +1434,17 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    dst_points_.upload(L.dst_points);
    upload_cast<T>(uti_, L.uti);
    upload_cast<T>(u_, L.u_cm);
-   {
-      std::vector<longlong2> ip(L.inter_pairs.size() / 2);
-      for (size_t i = 0; i < ip.size(); i++) { ip[i].x = L.inter_pairs[2 * i]; ip[i].y = L.inter_pairs[2 * i + 1]; }
-      inter_.upload(ip);
-   }
    upload_pairs<T>(t_, L.t_pairs);
+   tiles_.upload(L.tiles);
+   tile_src_.upload(L.tile_src);
+   tile_dst_.upload(L.tile_dst);
+   tile_dst_pairs_.upload(L.tile_dst_pairs);
+   tile_pairs_.upload(L.tile_pairs);
+   tile_groups_ = L.tile_groups;
+   translated_.alloc(std::max<int64_t>(L.translated_elems, 1));
    spectra_.alloc(std::max<int64_t>(L.spectra_elems, 1));
+   spectra_.zero();      // row padding is read by the translation and must stay zero
+   translated_.zero();
    staging_.alloc(std::max<int64_t>((int64_t)L.stage_levels * L.total_points, 1));
    staging_.zero();
    // entries of the zero slot and staging rows nobody writes must stay zero
@@ -704,17 +1454,25 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    dst_smem_ = 0;
    for (const LaunchGroup& g : src_groups_) src_smem_ = std::max(src_smem_, (int)(g.smem_elems * sizeof(T) + 128));
    for (const LaunchGroup& g : dst_groups_) dst_smem_ = std::max(dst_smem_, (int)(g.smem_elems * sizeof(T) + 128));
-   int maxcols = 0;
+   int maxcols = 2;
    for (const auto& l : L.leaves) maxcols = std::max(maxcols, l.ncols);
-   leaf_smem_max_ = (int)(maxcols * sizeof(T2) + 16);
    int dev = 0, optin = 0;
    FFTSVD_CUDA(cudaGetDevice(&dev));
    FFTSVD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin)
+   // one warp per leaf; as many leaves per block (up to four) as the gathered columns allow
+   near_stride_ = maxcols;
+   near_warps_ = (int)std::max<size_t>(1, std::min<size_t>(kNearThreads / 32, (size_t)optin / (maxcols * sizeof(T2))));
+   leaf_smem_max_ = (int)(near_warps_ * maxcols * sizeof(T2));
+   int tile_smem = 0;
+   for (const TileGroup& g : tile_groups_) tile_smem = std::max(tile_smem, translate_smem(g));
+   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || tile_smem > optin)
       throw Error(FFTSVD_ERR_UNSUPPORTED, "operator block needs more shared memory than the device offers");
+   if (tile_smem > 0)
+      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
    FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, src_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dst_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(near_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, leaf_smem_max_));
+   build_chains();
    FFTSVD_CUDA(cudaDeviceSynchronize());
 }
 
@@ -726,14 +1484,90 @@ void DeviceOperator<T>::enable_timing(bool on) {
 }
 
 template <typename T>
-void DeviceOperator<T>::stage_ms(float* join_ms, float* fwd_ms, float* bwd_ms, float* near_ms) const {
-   *join_ms = *near_ms = *fwd_ms = *bwd_ms = 0.f;
+int DeviceOperator<T>::translate_smem(const TileGroup& g) const {
+   // two chunk rows per slot (and the zero row) and per halo source, pairs, per-destination
+   // {begin, count} and offsets, halo offsets; each carve aligned to 16 bytes
+   return (int)(2 * (kTileZeroSlot + 1) * kTileRowBytes + (size_t)2 * g.max_src * kTileRowBytes + (size_t)g.max_pairs * sizeof(uint32_t) +
+                (size_t)g.max_dst * (sizeof(int2) + sizeof(int64_t)) + (size_t)g.max_src * sizeof(int64_t) + 128);
+}
+
+template <typename T>
+void DeviceOperator<T>::stage_ms(float* ms) const {
+   for (int k = 0; k < kNumKernels; k++) ms[k] = 0.f;
    if (!ev_[0]) return;
-   FFTSVD_CUDA(cudaEventSynchronize(ev_[4]));
-   FFTSVD_CUDA(cudaEventElapsedTime(join_ms, ev_[0], ev_[1]));
-   FFTSVD_CUDA(cudaEventElapsedTime(fwd_ms, ev_[1], ev_[2]));
-   FFTSVD_CUDA(cudaEventElapsedTime(bwd_ms, ev_[2], ev_[3]));
-   FFTSVD_CUDA(cudaEventElapsedTime(near_ms, ev_[3], ev_[4]));
+   FFTSVD_CUDA(cudaEventSynchronize(ev_[kNumKernels]));
+   for (int k = 0; k < kNumKernels; k++) FFTSVD_CUDA(cudaEventElapsedTime(&ms[k], ev_[k], ev_[k + 1]));
+}
+
+static bool warp_path(const LaunchGroup& g) {
+   return g.n >= kWarpMinN && g.n <= kWarpMaxN && g.max_rank >= 1 && g.max_rank <= kWarpMaxRank &&
+          g.count >= kWarpMinCubes;
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_forward(const LaunchGroup& g, cudaStream_t stream) {
+   if (warp_path(g)) {
+      const int blocks = (g.count + kWarpCubes - 1) / kWarpCubes;
+      const SrcDesc* c = src_.get() + g.begin;
+      if (g.n == 3)
+         far_forward_warp_kernel<T, 3><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
+                                                                           vt_.get(), pv_.get(), spectra_.get());
+      else if (g.n == 4)
+         far_forward_n4_kernel<T><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
+                                                                       vt_.get(), pv_.get(), spectra_.get());
+      else
+         far_forward_warp_kernel<T, 5><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
+                                                                           vt_.get(), pv_.get(), spectra_.get());
+   } else {
+      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+      far_forward_kernel<T><<<g.count, far_threads(g.n), smem, stream>>>(src_.get() + g.begin, src_panels_.get(),
+                                                                         xsd_.get(), vt_.get(), pv_.get(), spectra_.get());
+   }
+   FFTSVD_CHECK_LAUNCH();
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_translate(const TileGroup& g, cudaStream_t stream) {
+   // split each tile's frequency chunks over several blocks so that even the few
+   // tiles of the coarse levels fill the device (about eight blocks per SM in total)
+   const int nchunks = g.pg / (kTileRowBytes / (int)sizeof(T2));
+   const int total = g.count * nchunks;
+   const int cpb = std::max(1, std::min(nchunks, total / (8 * 148)));
+   const dim3 grid(g.count, (nchunks + cpb - 1) / cpb);
+   translate_kernel<T><<<grid, kTranslateThreads, translate_smem(g), stream>>>(
+       tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(), t_.get(),
+       spectra_.get(), translated_.get(), cpb);
+   FFTSVD_CHECK_LAUNCH();
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_backward(const LaunchGroup& g, cudaStream_t stream) {
+   if (warp_path(g)) {
+      const int blocks = (g.count + kWarpCubes - 1) / kWarpCubes;
+      const DstDesc* c = dst_.get() + g.begin;
+      if (g.n == 3)
+         far_backward_warp_kernel<T, 3><<<blocks, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+      else if (g.n == 4)
+         far_backward_n4_kernel<T><<<blocks, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+      else
+         far_backward_warp_kernel<T, 5><<<blocks, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+   } else {
+      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+      far_backward_kernel<T><<<g.count, far_threads(g.n), smem, stream>>>(
+          dst_.get() + g.begin, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(),
+          total_points_);
+   }
+   FFTSVD_CHECK_LAUNCH();
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_chain(const Chain& ch, cudaStream_t stream) {
+   for (int i : ch.src) launch_forward(src_groups_[i], stream);
+   for (int i : ch.tile) launch_translate(tile_groups_[i], stream);
+   for (int i : ch.dst) launch_backward(dst_groups_[i], stream);
 }
 
 template <typename T>
@@ -748,30 +1582,98 @@ void DeviceOperator<T>::apply(const double* x, double* y, cudaStream_t stream) {
                                                  join_dphi_idx_.get(), join_dphi_scale_.get(), x, xsd_.get());
       FFTSVD_CHECK_LAUNCH();
    }
-   if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[1], stream));
-   for (const LaunchGroup& g : src_groups_) {
-      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_forward_kernel<T><<<g.count, kFarThreads, smem, stream>>>(src_.get() + g.begin, src_panels_.get(),
-                                                                    xsd_.get(), vt_.get(), pv_.get(), spectra_.get());
+   if (timing_) {
+      // stage by stage on one stream, so that each stage can be timed
+      FFTSVD_CUDA(cudaEventRecord(ev_[1], stream));
+      for (const LaunchGroup& g : src_groups_) launch_forward(g, stream);
+      FFTSVD_CUDA(cudaEventRecord(ev_[2], stream));
+      for (const TileGroup& g : tile_groups_) launch_translate(g, stream);
+      FFTSVD_CUDA(cudaEventRecord(ev_[3], stream));
+      for (const LaunchGroup& g : dst_groups_) launch_backward(g, stream);
+      FFTSVD_CUDA(cudaEventRecord(ev_[4], stream));
+      launch_near(x, y, stream);
+   } else {
+      // the near field and the far-field chains of each grid size (forward -> translate
+      // -> backward) only share the joined input: all but the largest chain run on their
+      // own streams, forked after the join and joined back before the far field is added
+      // (the longest chain on a high-priority stream: it is the critical path)
+      FFTSVD_CUDA(cudaEventRecord(fork_, stream));
+      for (size_t c = 0; c < chains_.size(); c++) {
+         FFTSVD_CUDA(cudaStreamWaitEvent(chains_[c].stream, fork_, 0));
+         launch_chain(chains_[c], chains_[c].stream);
+         FFTSVD_CUDA(cudaEventRecord(chains_[c].done, chains_[c].stream));
+      }
+      FFTSVD_CUDA(cudaStreamWaitEvent(near_stream_, fork_, 0));
+      launch_near(x, y, near_stream_);
+      FFTSVD_CUDA(cudaEventRecord(near_done_, near_stream_));
+      for (size_t c = 0; c < chains_.size(); c++) FFTSVD_CUDA(cudaStreamWaitEvent(stream, chains_[c].done, 0));
+      FFTSVD_CUDA(cudaStreamWaitEvent(stream, near_done_, 0));
+   }
+   if (n_rows_ > 0 && stage_levels_ > 0) {
+      const int blocks = (int)std::min<int64_t>((n_rows_ + 255) / 256, 148 * 8);
+      far_add_kernel<T><<<blocks, 256, 0, stream>>>(n_rows_, leaf_rows_.get(), staging_.get(), stage_levels_,
+                                                    total_points_, point_out_.get(), y);
       FFTSVD_CHECK_LAUNCH();
    }
-   if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[2], stream));
-   for (const LaunchGroup& g : dst_groups_) {
-      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_backward_kernel<T><<<g.count, kFarThreads, smem, stream>>>(
-          dst_.get() + g.begin, dst_points_.get(), inter_.get(), t_.get(), spectra_.get(), uti_.get(), u_.get(),
-          staging_.get(), total_points_);
-      FFTSVD_CHECK_LAUNCH();
+   if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[5], stream));
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_near(const double* x, double* y, cudaStream_t stream) {
+   if (n_leaf_ == 0) return;
+   near_kernel<T><<<(n_leaf_ + near_warps_ - 1) / near_warps_, 32 * near_warps_, leaf_smem_max_, stream>>>(
+       leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), xsd_.get(),
+       point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(), join_phi_scale_.get(), x, y);
+   FFTSVD_CHECK_LAUNCH();
+}
+
+template <typename T>
+void DeviceOperator<T>::build_chains() {
+   release_chains();
+   std::map<int, Chain> by_n;
+   for (int i = 0; i < (int)src_groups_.size(); i++) by_n[src_groups_[i].n].src.push_back(i);
+   for (int i = 0; i < (int)dst_groups_.size(); i++) by_n[dst_groups_[i].n].dst.push_back(i);
+   for (auto& kv : by_n) {
+      const int n = kv.first, pgp = ((2 * n - 1) * (2 * n - 1) * n + 15) & ~15;
+      kv.second.n = n;
+      for (int i = 0; i < (int)tile_groups_.size(); i++)
+         if (tile_groups_[i].pg == pgp) kv.second.tile.push_back(i);
+      // destinations and their interactions: a measure of the chain's length
+      for (int i : kv.second.dst) kv.second.work += (double)dst_groups_[i].count * pgp;
    }
-   if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[3], stream));
-   if (n_leaf_ > 0) {
-      near_kernel<T><<<n_leaf_, kNearThreads, leaf_smem_max_, stream>>>(
-          leaves_.get(), leaf_rows_.get(), leaf_cols_.get(), d_.get(), xsd_.get(), staging_.get(), stage_levels_,
-          total_points_, point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(),
-          join_phi_scale_.get(), x, y);
-      FFTSVD_CHECK_LAUNCH();
+   for (auto& kv : by_n) chains_.push_back(kv.second);
+   std::stable_sort(chains_.begin(), chains_.end(), [](const Chain& a, const Chain& b) { return a.work > b.work; });
+   int least = 0, greatest = 0;
+   FFTSVD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+   FFTSVD_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+   FFTSVD_CUDA(cudaStreamCreateWithPriority(&near_stream_, cudaStreamNonBlocking, least));
+   FFTSVD_CUDA(cudaEventCreateWithFlags(&near_done_, cudaEventDisableTiming));
+   for (size_t c = 0; c < chains_.size(); c++) {
+      FFTSVD_CUDA(cudaStreamCreateWithPriority(&chains_[c].stream, cudaStreamNonBlocking, c == 0 ? greatest : least));
+      FFTSVD_CUDA(cudaEventCreateWithFlags(&chains_[c].done, cudaEventDisableTiming));
    }
-   if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[4], stream));
+}
+
+template <typename T>
+void DeviceOperator<T>::release_chains() {
+   for (Chain& c : chains_) {
+      if (c.stream) cudaStreamDestroy(c.stream);
+      if (c.done) cudaEventDestroy(c.done);
+   }
+   chains_.clear();
+   if (fork_) cudaEventDestroy(fork_);
+   if (near_stream_) cudaStreamDestroy(near_stream_);
+   if (near_done_) cudaEventDestroy(near_done_);
+   fork_ = nullptr;
+   near_stream_ = nullptr;
+   near_done_ = nullptr;
+}
+
+template <typename T>
+DeviceOperator<T>::~DeviceOperator() {
+   release_chains();
+   for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
 }
 
 template <typename T>
@@ -780,7 +1682,8 @@ size_t DeviceOperator<T>::device_bytes() const {
           xsd_.bytes() + point_out_.bytes() + point_panel_.bytes() + point_jump_.bytes() + leaves_.bytes() +
           leaf_rows_.bytes() + leaf_cols_.bytes() + d_.bytes() + src_.bytes() + src_panels_.bytes() +
           vt_.bytes() + pv_.bytes() + dst_.bytes() + dst_points_.bytes() + uti_.bytes() + u_.bytes() +
-          inter_.bytes() + t_.bytes() + spectra_.bytes() + staging_.bytes();
+          t_.bytes() + spectra_.bytes() + staging_.bytes() + tiles_.bytes() + tile_src_.bytes() +
+          tile_dst_.bytes() + tile_dst_pairs_.bytes() + tile_pairs_.bytes() + translated_.bytes();
 }
 
 template class DeviceOperator<float>;

@@ -41,7 +41,35 @@ struct DstDesc {        // one far-field destination cube (points > 0, column ra
    int32_t inter_cnt;
    int32_t stage;       // staging slot (level)
    int32_t pad;
+   int64_t s_off;       // into the translated spectra, (2n-1)^2 n complex
 };
+
+// Translation tile: destination cubes of one tree and level that share a halo
+// of source spectra; all of them, the halo and the level's 343 translation
+// slots are staged through shared memory one frequency chunk at a time.
+struct TileDesc {
+   int32_t ndst;        // destinations in the tile
+   int32_t nsrc;        // halo sources
+   int32_t npairs;      // (destination, source) interactions
+   int32_t pg;          // frequencies per cube, (2n-1)^2 n
+   int64_t dst_off;     // into tile_dst (S offsets) and tile_dst_pairs
+   int64_t src_off;     // into tile_src (spectrum offsets)
+   int64_t pair_off;    // into tile_pairs: packed (halo index << 16) | slot, grouped per destination,
+                        // each destination's list padded to a multiple of four
+   int64_t t_off;       // translation table of slot 0 of this tree and level (complex elements)
+};
+
+struct TileGroup {      // tiles with the same frequency count, one launch
+   int pg = 0;
+   int begin = 0, count = 0;
+   int max_src = 0, max_pairs = 0, max_dst = 0;
+};
+
+constexpr int kTileMaxDst = 64;
+constexpr int kTileMaxSrc = 256;
+constexpr int kTileMaxPairs = 4096;
+constexpr int kTileChunk = 16;  // frequencies per shared-memory chunk
+constexpr int kTileZeroSlot = 343;  // all-zero translation row that pads pair lists to groups of four
 
 struct LeafDesc {       // one leaf with points
    int32_t row_off;     // into leaf_rows
@@ -58,13 +86,22 @@ struct LaunchGroup {
    int begin = 0;
    int count = 0;
    int smem_elems = 0;  // in units of the operator element type
+   int max_rank = 0;    // largest row (sources) or column (destinations) rank
 };
 
-// Algorithmic bytes of each matvec kernel [join, far_forward, far_backward, near]:
+// Small grids (n <= kWarpMaxN) whose cubes all have rank <= 32 run one cube per
+// warp instead of one cube per block.
+constexpr int kWarpMinN = 3;
+constexpr int kWarpMaxN = 5;
+constexpr int kWarpMaxRank = 32;
+constexpr int kWarpMinCubes = 4096;  // fewer cubes leave too few warps per SM to hide latency
+
+// Algorithmic bytes of each matvec kernel [join, far_forward, translate, far_backward, near]:
 // elems * (operator element size) + fixed (FP64 vectors and int32 indices).
+constexpr int kNumKernels = 5;
 struct KernelBytes {
-   double elems[4] = {0, 0, 0, 0};
-   double fixed[4] = {0, 0, 0, 0};
+   double elems[kNumKernels] = {0, 0, 0, 0, 0};
+   double fixed[kNumKernels] = {0, 0, 0, 0, 0};
 };
 
 // Host-side relayout product, independent of the element type.
@@ -97,8 +134,15 @@ struct OperatorLayout {
    std::vector<int64_t> inter_pairs;   // {spectrum offset, T offset} packed as 2 x int64
    std::vector<double> t_pairs;        // translation operators {re, im}
    int64_t spectra_elems = 0;
+   int64_t translated_elems = 0;       // S buffer, complex elements
    int max_src_smem_elems = 0, max_dst_smem_elems = 0;
    std::vector<LaunchGroup> src_groups, dst_groups;
+   // translation tiles, grouped by frequency count (one launch per group)
+   std::vector<TileDesc> tiles;
+   std::vector<int64_t> tile_src, tile_dst;
+   std::vector<int2> tile_dst_pairs;   // {begin, count} relative to the tile's pair_off
+   std::vector<uint32_t> tile_pairs;
+   std::vector<TileGroup> tile_groups;
    // algorithmic bytes per matvec at 4-byte or 8-byte element size (excluding vectors)
    int64_t operator_elems = 0;          // D pairs*2 + VT + PV*2 + UTI + U
    int64_t t_elems = 0;                 // unique translation operator reals
@@ -112,22 +156,56 @@ template <typename T>
 class DeviceOperator {
  public:
    using T2 = typename Vec2<T>::type;
+   DeviceOperator() = default;
+   DeviceOperator(const DeviceOperator&) = delete;
+   DeviceOperator& operator=(const DeviceOperator&) = delete;
+   ~DeviceOperator();
    void upload(const OperatorLayout& L);
    // y = A x on `stream`; x, y device pointers of num_unknowns doubles.
    void apply(const double* x, double* y, cudaStream_t stream);
    // per-stage events for timing (recorded when enabled)
    void enable_timing(bool on);
-   void stage_ms(float* join_ms, float* fwd_ms, float* bwd_ms, float* near_ms) const;
+   // milliseconds of [join, far_forward, translate, far_backward, near] of the last timed apply
+   void stage_ms(float* ms) const;
    size_t device_bytes() const;
 
  private:
+   // launch groups of one grid size: forward, translate and backward depend only on
+   // each other, so the chains of different grid sizes run concurrently
+   struct Chain {
+      int n = 0;
+      double work = 0;
+      std::vector<int> src, tile, dst;  // indices into the launch groups
+      cudaStream_t stream = nullptr;    // own stream (the first, longest chain at high priority)
+      cudaEvent_t done = nullptr;
+   };
+   int translate_smem(const TileGroup& g) const;
+   void launch_forward(const LaunchGroup& g, cudaStream_t stream);
+   void launch_translate(const TileGroup& g, cudaStream_t stream);
+   void launch_backward(const LaunchGroup& g, cudaStream_t stream);
+   void launch_chain(const Chain& ch, cudaStream_t stream);
+   void launch_near(const double* x, double* y, cudaStream_t stream);
+   void build_chains();
+   void release_chains();
+   std::vector<Chain> chains_;
+   cudaEvent_t fork_ = nullptr;
+   cudaStream_t near_stream_ = nullptr;
+   cudaEvent_t near_done_ = nullptr;
+   int64_t n_rows_ = 0;  // leaf rows (one per written output row)
    int num_unknowns_ = 0;
    int64_t total_panels_ = 0, total_points_ = 0;
    int stage_levels_ = 0;
    bool full_cover_ = true;
    int n_src_ = 0, n_dst_ = 0, n_leaf_ = 0;
    int src_smem_ = 0, dst_smem_ = 0, leaf_smem_max_ = 0;
+   int near_warps_ = 1, near_stride_ = 2;
    std::vector<LaunchGroup> src_groups_, dst_groups_;
+   std::vector<TileGroup> tile_groups_;
+   DevBuf<TileDesc> tiles_;
+   DevBuf<int64_t> tile_src_, tile_dst_;
+   DevBuf<int2> tile_dst_pairs_;
+   DevBuf<uint32_t> tile_pairs_;
+   DevBuf<typename Vec2<T>::type> translated_;
    DevBuf<int32_t> join_phi_idx_, join_dphi_idx_;
    DevBuf<double> join_phi_scale_, join_dphi_scale_;
    DevBuf<T2> xsd_;
@@ -143,12 +221,11 @@ class DeviceOperator {
    DevBuf<DstDesc> dst_;
    DevBuf<int32_t> dst_points_;
    DevBuf<T> uti_, u_;
-   DevBuf<longlong2> inter_;
    DevBuf<T2> t_;
    DevBuf<T2> spectra_;
    DevBuf<T> staging_;
    bool timing_ = false;
-   cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+   cudaEvent_t ev_[kNumKernels + 1] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 }  // namespace fftsvd

@@ -433,36 +433,36 @@ long long fftsvd_b200_launch_count(void) { return g_kernel_launches.load(); }
 
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s) { return s ? (void*)s->s.stream : nullptr; }
 
-int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes4) {
-   if (!s || !bytes4) return FFTSVD_ERR_ARGUMENT;
+int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes5) {
+   if (!s || !bytes5) return FFTSVD_ERR_ARGUMENT;
    const KernelBytes& kb = s->s.kernel_bytes;
    const double es = precision == FFTSVD_PREC_FP64 ? 8.0 : 4.0;
-   for (int k = 0; k < 4; k++) bytes4[k] = kb.elems[k] * es + kb.fixed[k];
+   for (int k = 0; k < kNumKernels; k++) bytes5[k] = kb.elems[k] * es + kb.fixed[k];
    return FFTSVD_OK;
 }
 
 int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y, int32_t reps,
-                               double* ms4) {
-   if (!s || !x || !y || !ms4 || reps <= 0) return FFTSVD_ERR_ARGUMENT;
+                               double* ms5) {
+   if (!s || !x || !y || !ms5 || reps <= 0) return FFTSVD_ERR_ARGUMENT;
    return guarded([&] {
       Surface& S = s->s;
-      double acc[4] = {0, 0, 0, 0};
+      double acc[kNumKernels] = {0, 0, 0, 0, 0};
       for (int r = 0; r < reps; r++) {
-         float t[4];
+         float t[kNumKernels];
          if (precision == FFTSVD_PREC_FP64) {
             S.op64.enable_timing(true);
             S.op64.apply(x, y, S.stream);
-            S.op64.stage_ms(&t[0], &t[1], &t[2], &t[3]);
+            S.op64.stage_ms(t);
             S.op64.enable_timing(false);
          } else {
             S.op32.enable_timing(true);
             S.op32.apply(x, y, S.stream);
-            S.op32.stage_ms(&t[0], &t[1], &t[2], &t[3]);
+            S.op32.stage_ms(t);
             S.op32.enable_timing(false);
          }
-         for (int k = 0; k < 4; k++) acc[k] += t[k];
+         for (int k = 0; k < kNumKernels; k++) acc[k] += t[k];
       }
-      for (int k = 0; k < 4; k++) ms4[k] = acc[k] / reps;
+      for (int k = 0; k < kNumKernels; k++) ms5[k] = acc[k] / reps;
    });
 }
 

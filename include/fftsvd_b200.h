@@ -246,12 +246,12 @@ int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
    and the FP64 input and output vectors. */
 int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes);
 
-/* Algorithmic bytes of each matvec kernel: [join, far_forward, far_backward, near]. */
-int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes4);
+/* Algorithmic bytes of each matvec kernel: [join, far_forward, translate, far_backward, near]. */
+int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes5);
 /* Run `reps` matvecs on device vectors with CUDA events around each kernel on
-   the library stream; average milliseconds per kernel in ms4 (same order). */
+   the library stream; average milliseconds per kernel in ms5 (same order). */
 int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const double* x, double* y, int32_t reps,
-                               double* ms4);
+                               double* ms5);
 /* The CUDA stream all work of this surface is issued on (cudaStream_t). */
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s);
 /* Kernel launches issued by this library since it was loaded. */
