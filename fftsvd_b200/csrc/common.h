@@ -25,6 +25,24 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// Runs f and turns exceptions into a status code (and the last-error text).
+template <typename F>
+inline int guarded(F&& f) {
+   try {
+      f();
+      return FFTSVD_OK;
+   } catch (const Error& e) {
+      set_last_error(e.what());
+      return e.code;
+   } catch (const std::bad_alloc&) {
+      set_last_error("host allocation failed");
+      return FFTSVD_ERR_ARGUMENT;
+   } catch (const std::exception& e) {
+      set_last_error(e.what());
+      return FFTSVD_ERR_ARGUMENT;
+   }
+}
+
 #define FFTSVD_CUDA(call)                                                                              \
    do {                                                                                               \
       cudaError_t err_ = (call);                                                                      \

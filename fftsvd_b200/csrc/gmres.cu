@@ -18,7 +18,9 @@ __device__ inline double warp_sum_d(double v) {
 
 __global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
                                const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
-                               const double* __restrict__ r, double* __restrict__ z) {
+                               const double* __restrict__ r, double* __restrict__ z, int64_t col) {
+   r += blockIdx.y * col;
+   z += blockIdx.y * col;
    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += gridDim.x * blockDim.x) {
       const int p0 = blk_ptr[b], k = blk_ptr[b + 1] - p0;
       double in[8], out[8];
@@ -73,16 +75,22 @@ __device__ inline void dots_of(int64_t n, int nvec, const double* __restrict__ V
 
 __global__ void __launch_bounds__(kVecThreads) dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V,
                                                                    int64_t ldv, const double* __restrict__ w,
-                                                                   double* __restrict__ partial) {
+                                                                   double* __restrict__ partial, int64_t col,
+                                                                   int64_t pcol) {
    __shared__ double red[kVecThreads / 32 * 8 + 8];
+   V += blockIdx.y * col;
+   w += blockIdx.y * col;
+   partial += blockIdx.y * pcol;
    const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
    const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
    dots_of(n, nvec, V, ldv, k0, k1, w0, w1, partial, red);
 }
 
 __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
-                                      int accumulate) {
+                                      int accumulate, int64_t pcol, int64_t hcol) {
    __shared__ double red[32];
+   partial += blockIdx.y * pcol;
+   out += blockIdx.y * hcol;
    const int j = blockIdx.x;
    if (j >= nvec) return;
    double s = 0.0;
@@ -99,8 +107,13 @@ __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restri
 
 __global__ void __launch_bounds__(kVecThreads) update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V,
                                                                   int64_t ldv, const double* __restrict__ h,
-                                                                  double* __restrict__ w, double* __restrict__ partial) {
+                                                                  double* __restrict__ w, double* __restrict__ partial,
+                                                                  int64_t col, int64_t pcol, int64_t hcol) {
    extern __shared__ double sh[];  // [nvec] h, then reduction scratch
+   V += blockIdx.y * col;
+   w += blockIdx.y * col;
+   partial += blockIdx.y * pcol;
+   h += blockIdx.y * hcol;
    double* hs = sh;
    double* red = sh + ((nvec + 1) & ~1);
    for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
@@ -121,8 +134,14 @@ __global__ void __launch_bounds__(kVecThreads) update_norm_kernel(int64_t n, int
                                                                   int64_t ldv, const double* __restrict__ h,
                                                                   const double* __restrict__ w,
                                                                   double* __restrict__ out,
-                                                                  double* __restrict__ partial) {
+                                                                  double* __restrict__ partial, int64_t col,
+                                                                  int64_t pcol, int64_t hcol) {
    extern __shared__ double sh[];
+   V += blockIdx.y * col;
+   w += blockIdx.y * col;
+   out += blockIdx.y * col;
+   partial += blockIdx.y * pcol;
+   h += blockIdx.y * hcol;
    double* hs = sh;
    double* red = sh + ((nvec + 1) & ~1);
    for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
@@ -142,8 +161,11 @@ __global__ void __launch_bounds__(kVecThreads) update_norm_kernel(int64_t n, int
 }
 
 __global__ void __launch_bounds__(kVecThreads) norm_partial_kernel(int64_t n, const double* __restrict__ w,
-                                                                   double* __restrict__ partial) {
+                                                                   double* __restrict__ partial, int64_t col,
+                                                                   int64_t pcol) {
    __shared__ double red[kVecThreads / 32 * 8 + 8];
+   w += blockIdx.y * col;
+   partial += blockIdx.y * pcol;
    const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
    const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
    double acc[8] = {w0 * w0 + w1 * w1, 0, 0, 0, 0, 0, 0, 0};
@@ -160,8 +182,23 @@ __device__ inline void rotate(double c, double s, double* a, double* b) {  // GM
 __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
                               const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
-                              GivensState* __restrict__ st) {
+                              GivensState* __restrict__ st, int64_t hcol, int64_t pcol,
+                              const int32_t* __restrict__ active) {
    __shared__ double red[256];
+   // column blockIdx.x of a batch: its own Hessenberg (ldh x ldh), rotations, g and state
+   const int colx = blockIdx.x;
+   H += (int64_t)colx * ldh * ldh;
+   h1 += colx * hcol;
+   h2 += colx * hcol;
+   norm_partial += colx * pcol;
+   cs += (int64_t)colx * ldh;
+   sn += (int64_t)colx * ldh;
+   g += (int64_t)colx * ldh;
+   st += colx;
+   if (active && !active[colx]) {  // finished column: its next basis vectors become zero
+      if (threadIdx.x == 0) st->inv_beta = 0.0;
+      return;
+   }
    double s = 0.0;
    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += norm_partial[b];
    red[threadIdx.x] = s;
@@ -202,15 +239,20 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
 }
 
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
-                             double factor, double* __restrict__ dst) {
-   const double f = factor_ptr ? *factor_ptr : factor;
+                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol) {
+   src += blockIdx.y * col;
+   dst += blockIdx.y * col;
+   const double f = factor_ptr ? factor_ptr[blockIdx.y * fcol] : factor;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] = src[k] * f;
 }
 
 __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                               const double* __restrict__ y, double* __restrict__ x) {
+                               const double* __restrict__ y, double* __restrict__ x, int64_t col, int64_t ycol) {
    extern __shared__ double ys[];
+   V += blockIdx.y * col;
+   x += blockIdx.y * col;
+   y += blockIdx.y * ycol;
    for (int j = threadIdx.x; j < nvec; j += blockDim.x) ys[j] = y[j];
    __syncthreads();
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -221,12 +263,17 @@ __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V
 }
 
 __global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                           double* __restrict__ dst) {
+                           double* __restrict__ dst, int64_t col) {
+   a += blockIdx.y * col;
+   b += blockIdx.y * col;
+   dst += blockIdx.y * col;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] = a[k] - b[k];
 }
 
-__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst) {
+__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst, int64_t col) {
+   a += blockIdx.y * col;
+   dst += blockIdx.y * col;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] += a[k];
 }

@@ -1,5 +1,11 @@
 // Device kernels of the GMRES solve (GMRES.c:446-539) and the block-diagonal
 // preconditioner (Preconditioner.c:272-294).  FP64 throughout.
+//
+// Every kernel also runs a batch of independent columns: column c = blockIdx.y
+// (blockIdx.x for givens_kernel) shifts each vector argument by c times its
+// column stride (col for vectors and basis columns, pcol for partial sums, hcol
+// for Gram-Schmidt coefficients, fcol for scale factors, ycol for combination
+// weights).  Strides of zero and a one-column grid give the single solve.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -15,23 +21,26 @@ constexpr int kRowsPerBlock = kVecThreads * kRowsPerThread;
 // z[idx] = inv * r[idx] for every preconditioner block (blocks of size <= 8).
 __global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
                                const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
-                               const double* __restrict__ r, double* __restrict__ z);
+                               const double* __restrict__ r, double* __restrict__ z, int64_t col);
 
 // partial[j * nblk + b] = sum over rows of block b of V[j][k] * w[k], j < nvec
 __global__ void dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                                    const double* __restrict__ w, double* __restrict__ partial);
+                                    const double* __restrict__ w, double* __restrict__ partial, int64_t col,
+                                    int64_t pcol);
 // out[j] = (accumulate ? out[j] : 0) + sum_b partial[j * nblk + b]; one block per j
 __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
-                                      int accumulate);
+                                      int accumulate, int64_t pcol, int64_t hcol);
 // w -= V h; then partial dots of the updated w against V (second Gram-Schmidt pass)
 __global__ void update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                                   const double* __restrict__ h, double* __restrict__ w, double* __restrict__ partial);
+                                   const double* __restrict__ h, double* __restrict__ w, double* __restrict__ partial,
+                                   int64_t col, int64_t pcol, int64_t hcol);
 // out = w - V h (written to out, may alias w); partial[b] = sum of squares of out over block b
 __global__ void update_norm_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
                                    const double* __restrict__ h, const double* __restrict__ w, double* __restrict__ out,
-                                   double* __restrict__ partial);
+                                   double* __restrict__ partial, int64_t col, int64_t pcol, int64_t hcol);
 // partial[b] = sum of squares of w over block b
-__global__ void norm_partial_kernel(int64_t n, const double* __restrict__ w, double* __restrict__ partial);
+__global__ void norm_partial_kernel(int64_t n, const double* __restrict__ w, double* __restrict__ partial, int64_t col,
+                                    int64_t pcol);
 
 struct GivensState {
    double normr;      // preconditioned rhs norm
@@ -43,23 +52,26 @@ struct GivensState {
 
 // Completes Arnoldi step i: H column from the two Gram-Schmidt passes and the
 // norm partials, applies the previous rotations, forms the new one, updates g
-// (GMRES.c:485-503).  Single block.
+// (GMRES.c:485-503).  One block per column; a column whose active flag is 0
+// (active may be null: all active) only zeroes its inv_beta.
 __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
                               const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
-                              GivensState* __restrict__ st);
+                              GivensState* __restrict__ st, int64_t hcol, int64_t pcol,
+                              const int32_t* __restrict__ active);
 
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
-                             double factor, double* __restrict__ dst);
+                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol);
 
 // x += V y  (y on device)
 __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                               const double* __restrict__ y, double* __restrict__ x);
+                               const double* __restrict__ y, double* __restrict__ x, int64_t col, int64_t ycol);
 
 // dst = a - b
-__global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst);
+__global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst,
+                           int64_t col);
 // dst += a
-__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst);
+__global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst, int64_t col);
 
 inline int vec_blocks(int64_t n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
 

@@ -53,11 +53,21 @@ constexpr int kRhsTile = 256;
 
 // One thread per panel; charges streamed through shared memory in order, so each
 // panel accumulates over charges in the reference's order (charge-major loop).
+// With gptr, blockIdx.y is a charge group: charges [gptr[g], gptr[g+1]) and
+// output column rhs + g * col.
 __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, const FlatPanel* __restrict__ panels,
                                                           const int32_t* __restrict__ phi_row, int nq,
                                                           const double* __restrict__ qpos,
-                                                          const double* __restrict__ q, double* __restrict__ rhs) {
+                                                          const double* __restrict__ q, double* __restrict__ rhs,
+                                                          const int32_t* __restrict__ gptr, int64_t col) {
    __shared__ double4 tile[kRhsTile];
+   if (gptr) {
+      const int q0 = gptr[blockIdx.y];
+      nq = gptr[blockIdx.y + 1] - q0;
+      qpos += 3 * (int64_t)q0;
+      q += q0;
+      rhs += blockIdx.y * col;
+   }
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    double c[3] = {0, 0, 0};
    if (i < np) { c[0] = panels[i].centroid[0]; c[1] = panels[i].centroid[1]; c[2] = panels[i].centroid[2]; }
@@ -85,13 +95,22 @@ constexpr int kReactChunks = 64;
 
 // Block (charge chunk, panel chunk): each thread owns one charge and sums the
 // panel integrals of its panel chunk; panels staged through shared memory.
+// With gptr, blockIdx.z is a charge group: its charges [gptr[g], gptr[g+1])
+// against its own solution column sol + g * col (partial still indexed by the
+// global charge number).
 __global__ void __launch_bounds__(kReactThreads) reaction_partial_kernel(
     int np, const FlatPanel* __restrict__ panels, const int32_t* __restrict__ phi_row,
     const int32_t* __restrict__ dphi_row, const double* __restrict__ sol, int nq, const double* __restrict__ qpos,
-    double* __restrict__ partial) {
+    double* __restrict__ partial, const int32_t* __restrict__ gptr, int64_t col) {
    __shared__ FlatPanel tile[kReactPanelTile];
    __shared__ double2 dens[kReactPanelTile];
-   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+   const int nq_all = nq;
+   int j = blockIdx.x * blockDim.x + threadIdx.x;
+   if (gptr) {
+      const int q0 = gptr[blockIdx.z], q1 = gptr[blockIdx.z + 1];
+      j = q0 + j < q1 ? q0 + j : nq_all;  // past the group: idle
+      sol += blockIdx.z * col;
+   }
    const int per = (np + gridDim.y - 1) / gridDim.y;
    const int p0 = blockIdx.y * per, p1 = min(np, p0 + per);
    double pt[3] = {0, 0, 0};
@@ -119,7 +138,7 @@ __global__ void __launch_bounds__(kReactThreads) reaction_partial_kernel(
                acc -= 4.0 * M_PI * dn.x;
          }
    }
-   if (j < nq) partial[(size_t)blockIdx.y * nq + j] = acc;
+   if (j < nq) partial[(size_t)blockIdx.y * nq_all + j] = acc;
 }
 
 __global__ void reaction_reduce_kernel(int nq, int chunks, const double* __restrict__ partial, double* __restrict__ phi) {
@@ -135,7 +154,8 @@ void rhs_device(Surface& S, double* rhs) {
    FFTSVD_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * S.n, S.stream));
    const int np = S.geom->num_panels;
    rhs_kernel<<<(np + kRhsThreads - 1) / kRhsThreads, kRhsThreads, 0, S.stream>>>(
-       np, S.geom->panels.get(), S.geom->phi_row.get(), S.num_charges, S.charge_pos.get(), S.charge_q.get(), rhs);
+       np, S.geom->panels.get(), S.geom->phi_row.get(), S.num_charges, S.charge_pos.get(), S.charge_q.get(), rhs,
+       nullptr, 0);
    FFTSVD_CHECK_LAUNCH();
 }
 
@@ -148,7 +168,7 @@ void reaction_device(Surface& S, const double* sol, double* phi) {
    dim3 grid((nq + kReactThreads - 1) / kReactThreads, chunks);
    reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
                                                                  S.geom->dphi_row.get(), sol, nq,
-                                                                 S.charge_pos.get(), partial.get());
+                                                                 S.charge_pos.get(), partial.get(), nullptr, 0);
    FFTSVD_CHECK_LAUNCH();
    reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, partial.get(), phi);
    FFTSVD_CHECK_LAUNCH();
@@ -163,6 +183,60 @@ double energy_device(Surface& S, const double* phi) {
    double e = 0.0;
    for (int c = 0; c < S.num_charges; c++) e += 0.5 * S.charge_q_host[c] * h[c];
    return e * 332.112 / S.eps_in;
+}
+
+// Host group boundaries: group g is charges [gptr[g], gptr[g+1]), increasing, within the charge list.
+static void check_groups(const Surface& S, int ngroups, const int32_t* gptr, int* max_size) {
+   FFTSVD_REQUIRE(ngroups > 0 && ngroups <= 65535 && gptr, "charge groups");
+   FFTSVD_REQUIRE(gptr[0] >= 0 && gptr[ngroups] <= S.num_charges, "charge group outside the charge list");
+   *max_size = 0;
+   for (int g = 0; g < ngroups; g++) {
+      FFTSVD_REQUIRE(gptr[g + 1] >= gptr[g], "charge group boundaries must not decrease");
+      *max_size = std::max(*max_size, gptr[g + 1] - gptr[g]);
+   }
+}
+
+void rhs_groups_device(Surface& S, int ngroups, const int32_t* gptr_host, double* rhs) {
+   FFTSVD_REQUIRE(S.geom, "surface has no panel geometry");
+   int maxg = 0;
+   check_groups(S, ngroups, gptr_host, &maxg);
+   DevBuf<int32_t> gptr;
+   gptr.upload(gptr_host, ngroups + 1);
+   FFTSVD_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * S.n * ngroups, S.stream));
+   const int np = S.geom->num_panels;
+   rhs_kernel<<<dim3((np + kRhsThreads - 1) / kRhsThreads, ngroups), kRhsThreads, 0, S.stream>>>(
+       np, S.geom->panels.get(), S.geom->phi_row.get(), 0, S.charge_pos.get(), S.charge_q.get(), rhs, gptr.get(), S.n);
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+}
+
+void group_energies_device(Surface& S, int ngroups, const int32_t* gptr_host, const double* sol, double* energies) {
+   FFTSVD_REQUIRE(S.geom, "surface has no panel geometry");
+   int maxg = 0;
+   check_groups(S, ngroups, gptr_host, &maxg);
+   const int nq = S.num_charges, np = S.geom->num_panels;
+   for (int g = 0; g < ngroups; g++) energies[g] = 0.0;
+   if (nq == 0 || maxg == 0) return;
+   DevBuf<int32_t> gptr;
+   gptr.upload(gptr_host, ngroups + 1);
+   const int chunks = std::max(1, std::min(kReactChunks, (np + kReactPanelTile - 1) / kReactPanelTile));
+   DevBuf<double> partial((size_t)chunks * nq), phi(nq);
+   partial.zero(S.stream);
+   dim3 grid((maxg + kReactThreads - 1) / kReactThreads, chunks, ngroups);
+   reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
+                                                                 S.geom->dphi_row.get(), sol, nq, S.charge_pos.get(),
+                                                                 partial.get(), gptr.get(), S.n);
+   FFTSVD_CHECK_LAUNCH();
+   reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, partial.get(), phi.get());
+   FFTSVD_CHECK_LAUNCH();
+   std::vector<double> h(nq);
+   FFTSVD_CUDA(cudaMemcpyAsync(h.data(), phi.get(), sizeof(double) * nq, cudaMemcpyDeviceToHost, S.stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   for (int g = 0; g < ngroups; g++) {
+      double e = 0.0;
+      for (int c = gptr_host[g]; c < gptr_host[g + 1]; c++) e += 0.5 * S.charge_q_host[c] * h[c];
+      energies[g] = e * 332.112 / S.eps_in;
+   }
 }
 
 }  // namespace fftsvd
@@ -292,7 +366,7 @@ int fftsvd_b200_reaction_potentials_noalloc(fftsvd_surface* s, const double* sol
       // every scratch entry the reduction reads is written by the partial kernel of this call
       reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
                                                                     S.geom->dphi_row.get(), sol, nq,
-                                                                    S.charge_pos.get(), scratch);
+                                                                    S.charge_pos.get(), scratch, nullptr, 0);
       FFTSVD_CHECK_LAUNCH();
       reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, scratch, phi);
       FFTSVD_CHECK_LAUNCH();
@@ -312,6 +386,17 @@ int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy) {
    for (int c = 0; c < s->s.num_charges; c++) e += 0.5 * s->s.charge_q_host[c] * phi[c];
    *energy = e * 332.112 / s->s.eps_in;
    return FFTSVD_OK;
+}
+
+int fftsvd_b200_rhs_groups_device(fftsvd_surface* s, int32_t ngroups, const int32_t* group_ptr, double* rhs) {
+   if (!s || !group_ptr || !rhs) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] { rhs_groups_device(s->s, ngroups, group_ptr, rhs); });
+}
+
+int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const int32_t* group_ptr, const double* sol,
+                                      double* energies) {
+   if (!s || !group_ptr || !sol || !energies) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] { group_energies_device(s->s, ngroups, group_ptr, sol, energies); });
 }
 
 }  // extern "C"

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -531,8 +532,10 @@ __device__ inline T* carve(char*& p, int count) {
 template <typename T>
 __global__ void join_kernel(int64_t total, const int32_t* __restrict__ phi_idx, const double* __restrict__ phi_scale,
                             const int32_t* __restrict__ dphi_idx, const double* __restrict__ dphi_scale,
-                            const double* __restrict__ x, typename Vec2<T>::type* __restrict__ xsd) {
+                            const double* __restrict__ x, typename Vec2<T>::type* __restrict__ xsd, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   x += blockIdx.y * bs.n;
+   xsd += blockIdx.y * bs.panels;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
       T2 v;
       v.x = (T)(dphi_scale[k] * x[dphi_idx[k]]);
@@ -556,8 +559,10 @@ template <typename T>
 __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
     const SrcDesc* __restrict__ cubes, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
-    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra) {
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
+   spectra += blockIdx.y * bs.spectra;
    extern __shared__ __align__(16) char smem_raw[];
    const SrcDesc c = cubes[blockIdx.x];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n;
@@ -693,64 +698,78 @@ template <> struct Pack16<double> {
 
 // One block per (tile, range of frequency chunks): S[d][f] = sum over the
 // interactions of destination d of T[slot][f] * F[source][f] (Cube_multiply_T,
-// Cube.c:2062-2111).  Frequencies are processed in chunks of one kTileRowBytes
-// row per slot/source.  The chunk of all 343 translation slots of the tile's
-// tree and level and the chunk of every halo source spectrum are copied to
-// shared memory with cp.async, one chunk ahead of the computation (double
-// buffer), so each table entry and spectrum crosses L2 once per tile instead of
-// once per interaction.  Rows are padded to a multiple of 16 complex values, so
-// every copy is a full aligned 16 bytes.  Each thread owns one 16-byte unit
-// (two FP32 or one FP64 complex) of one destination's row.
-template <typename T>
+// Cube.c:2062-2111).  The chunk of all 343 translation slots of the tile's tree
+// and level and the chunk of every halo source spectrum are copied to shared
+// memory with cp.async, one chunk ahead of the computation (double buffer), so
+// each table entry and spectrum crosses L2 once per tile instead of once per
+// interaction.  Rows are padded to a multiple of 16 complex values, so every
+// copy is a full aligned 16 bytes.  Each thread owns one 16-byte unit of one
+// destination's kTileRowBytes row.
+//
+// Single right-hand side: a row is kTileRowBytes of consecutive frequencies of
+// one spectrum (8 units); the slot rows are as wide.
+// Batch (BATCH, blockIdx.z = group of 8 right-hand sides in planar buffers): a
+// row is one 16-byte unit (2 FP32 or 1 FP64 frequency) of each of the 8
+// right-hand sides, and a slot row is the single unit of those frequencies, read
+// once and applied to all 8.
+template <typename T, bool BATCH>
 __global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
     const TileDesc* __restrict__ tiles, const int64_t* __restrict__ tile_src, const int64_t* __restrict__ tile_dst,
     const int2* __restrict__ tile_dst_pairs, const uint32_t* __restrict__ tile_pairs,
     const typename Vec2<T>::type* __restrict__ tops, const typename Vec2<T>::type* __restrict__ spectra,
-    typename Vec2<T>::type* __restrict__ S, int chunks_per_block) {
+    typename Vec2<T>::type* __restrict__ S, int chunks_per_block, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
    using V = typename Pack16<T>::V;
-   constexpr int U = kTileRowBytes / 16;                 // 16-byte units per row
-   constexpr int CH = kTileRowBytes / (int)sizeof(T2);   // complex values per row
-   constexpr int PER16 = 16 / (int)sizeof(T2);           // complex values per unit
+   constexpr int U = kTileRowBytes / 16;                          // 16-byte units per row
+   constexpr int PER16 = 16 / (int)sizeof(T2);                    // complex values per unit
+   constexpr int CH = BATCH ? PER16 : kTileRowBytes / (int)sizeof(T2);  // frequencies per chunk
+   constexpr int TU = BATCH ? 1 : U;                              // units per slot row
    extern __shared__ __align__(16) char smem_raw[];
+   if (BATCH) {
+      spectra += (int64_t)blockIdx.z * U * bs.spectra;  // first right-hand side of this group
+      S += (int64_t)blockIdx.z * U * bs.translated;
+   }
    const TileDesc t = tiles[blockIdx.x];
    const int nchunks = t.pg / CH;
    const int kbeg = blockIdx.y * chunks_per_block;
    if (kbeg >= nchunks) return;
    const int kend = min(nchunks, kbeg + chunks_per_block);
    char* p = smem_raw;
-   T2* Tb0 = carve<T2>(p, (kTileZeroSlot + 1) * CH);  // 343 slots and the zero row
-   T2* Tb1 = carve<T2>(p, (kTileZeroSlot + 1) * CH);
-   T2* Fb0 = carve<T2>(p, t.nsrc * CH);
-   T2* Fb1 = carve<T2>(p, t.nsrc * CH);
+   V* Tb0 = carve<V>(p, (kTileZeroSlot + 1) * TU);  // 343 slots and the zero row
+   V* Tb1 = carve<V>(p, (kTileZeroSlot + 1) * TU);
+   V* Fb0 = carve<V>(p, t.nsrc * U);
+   V* Fb1 = carve<V>(p, t.nsrc * U);
    uint32_t* pairs = carve<uint32_t>(p, t.npairs);
    int2* dinfo = carve<int2>(p, t.ndst);
    int64_t* srcoff = carve<int64_t>(p, t.nsrc);
    int64_t* dstoff = carve<int64_t>(p, t.ndst);
-   // pairs pre-scaled to unit offsets of the chunk rows: (source row << 16) | slot row
+   // pairs pre-scaled to unit offsets: (source row << 16) | slot row
    for (int i = threadIdx.x; i < t.npairs; i += blockDim.x) {
       const uint32_t pr = tile_pairs[t.pair_off + i];
-      pairs[i] = ((pr >> 16) * (uint32_t)U) << 16 | ((pr & 0xffffu) * (uint32_t)U);
+      pairs[i] = ((pr >> 16) * (uint32_t)U) << 16 | ((pr & 0xffffu) * (uint32_t)TU);
    }
    for (int i = threadIdx.x; i < t.ndst; i += blockDim.x) {
       dinfo[i] = tile_dst_pairs[t.dst_off + i];
       dstoff[i] = tile_dst[t.dst_off + i];
    }
    for (int i = threadIdx.x; i < t.nsrc; i += blockDim.x) srcoff[i] = tile_src[t.src_off + i];
-   for (int i = threadIdx.x; i < CH; i += blockDim.x) {
-      Tb0[kTileZeroSlot * CH + i] = Cx<T>::make(T(0), T(0));
-      Tb1[kTileZeroSlot * CH + i] = Cx<T>::make(T(0), T(0));
+   for (int i = threadIdx.x; i < TU; i += blockDim.x) {
+      Tb0[kTileZeroSlot * TU + i] = Pack16<T>::zero();
+      Tb1[kTileZeroSlot * TU + i] = Pack16<T>::zero();
    }
    __syncthreads();
-   auto stage = [&](int k, T2* Tb, T2* Fb) {
+   auto stage = [&](int k, V* Tb, V* Fb) {
       const int f0 = k * CH;
-      for (int i = threadIdx.x; i < kTileZeroSlot * U; i += blockDim.x) {
-         const int s = i / U, u = i % U;
-         cp_async16(&Tb[s * CH + u * PER16], &tops[t.t_off + (int64_t)s * t.pg + f0 + u * PER16]);
+      for (int i = threadIdx.x; i < kTileZeroSlot * TU; i += blockDim.x) {
+         const int s = i / TU, u = i % TU;
+         cp_async16(&Tb[i], &tops[t.t_off + (int64_t)s * t.pg + f0 + u * PER16]);
       }
       for (int i = threadIdx.x; i < t.nsrc * U; i += blockDim.x) {
          const int s = i / U, u = i % U;
-         cp_async16(&Fb[s * CH + u * PER16], &spectra[srcoff[s] + f0 + u * PER16]);
+         if (BATCH)
+            cp_async16(&Fb[i], &spectra[u * bs.spectra + srcoff[s] + f0]);
+         else
+            cp_async16(&Fb[i], &spectra[srcoff[s] + f0 + u * PER16]);
       }
       cp_async_commit();
    };
@@ -764,25 +783,29 @@ __global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
          cp_async_wait<0>();
       }
       __syncthreads();
-      const V* Ts = reinterpret_cast<const V*>(odd ? Tb1 : Tb0);
-      const V* Fs = reinterpret_cast<const V*>(odd ? Fb1 : Fb0);
+      const V* Ts = odd ? Tb1 : Tb0;
+      const V* Fs = odd ? Fb1 : Fb0;
       const int f0 = k * CH;
       // thread -> (destination, unit)
       for (int item = threadIdx.x; item < t.ndst * U; item += blockDim.x) {
          const int d = item / U, u = item % U;
+         const int tu = BATCH ? 0 : u;
          const int2 di = dinfo[d];
          V acc = Pack16<T>::zero(), acc1 = Pack16<T>::zero();  // two chains of dependent FMAs
          // four pairs per 16-byte load; lists are padded to groups of four with the zero row
          const uint4* pp = reinterpret_cast<const uint4*>(pairs + di.x);
          for (int q = 0; q < (di.y >> 2); q++) {
             const uint4 pr = pp[q];
-            Pack16<T>::fma(acc, Ts[(pr.x & 0xffffu) + u], Fs[(pr.x >> 16) + u]);
-            Pack16<T>::fma(acc1, Ts[(pr.y & 0xffffu) + u], Fs[(pr.y >> 16) + u]);
-            Pack16<T>::fma(acc, Ts[(pr.z & 0xffffu) + u], Fs[(pr.z >> 16) + u]);
-            Pack16<T>::fma(acc1, Ts[(pr.w & 0xffffu) + u], Fs[(pr.w >> 16) + u]);
+            Pack16<T>::fma(acc, Ts[(pr.x & 0xffffu) + tu], Fs[(pr.x >> 16) + u]);
+            Pack16<T>::fma(acc1, Ts[(pr.y & 0xffffu) + tu], Fs[(pr.y >> 16) + u]);
+            Pack16<T>::fma(acc, Ts[(pr.z & 0xffffu) + tu], Fs[(pr.z >> 16) + u]);
+            Pack16<T>::fma(acc1, Ts[(pr.w & 0xffffu) + tu], Fs[(pr.w >> 16) + u]);
          }
          Pack16<T>::add(acc, acc1);
-         *reinterpret_cast<V*>(&S[dstoff[d] + f0 + u * PER16]) = acc;
+         if (BATCH)
+            *reinterpret_cast<V*>(&S[u * bs.translated + dstoff[d] + f0]) = acc;
+         else
+            *reinterpret_cast<V*>(&S[dstoff[d] + f0 + u * PER16]) = acc;
       }
       __syncthreads();  // this buffer is refilled by the stage issued in the next iteration
    }
@@ -795,8 +818,10 @@ template <typename T>
 __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
     const DstDesc* __restrict__ cubes, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
-    T* __restrict__ staging, int64_t total_points) {
+    T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
+   staging += blockIdx.y * bs.staging;
    extern __shared__ __align__(16) char smem_raw[];
    const DstDesc c = cubes[blockIdx.x];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n, pg = Np * Np * H;
@@ -888,8 +913,10 @@ template <typename T, int N>
 __global__ void __launch_bounds__(kWarpThreads, 12) far_forward_warp_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
-    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra) {
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
+   spectra += blockIdx.y * bs.spectra;
    using G = SmallGrid<N>;
    constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
    constexpr unsigned kAll = 0xffffffffu;
@@ -986,8 +1013,10 @@ template <typename T, int N>
 __global__ void __launch_bounds__(kWarpThreads) far_backward_warp_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
-    T* __restrict__ staging, int64_t total_points) {
+    T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
+   staging += blockIdx.y * bs.staging;
    using G = SmallGrid<N>;
    constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
    constexpr unsigned kAll = 0xffffffffu;
@@ -1089,8 +1118,10 @@ template <typename T>
 __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forward_n4_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
-    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra) {
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
+   spectra += blockIdx.y * bs.spectra;
    constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;  // ROW: complex values per fi
    constexpr unsigned kAll = 0xffffffffu;
    __shared__ T2 tw[Np];
@@ -1198,8 +1229,10 @@ template <typename T>
 __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_backward_n4_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
-    T* __restrict__ staging, int64_t total_points) {
+    T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
+   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
+   staging += blockIdx.y * bs.staging;
    constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;
    constexpr unsigned kAll = 0xffffffffu;
    __shared__ T2 tw[Np];
@@ -1324,9 +1357,12 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
     const typename Vec2<T>::type* __restrict__ xsd, const int32_t* __restrict__ point_out,
     const int32_t* __restrict__ point_panel, const double* __restrict__ point_jump,
     const int32_t* __restrict__ phi_idx, const double* __restrict__ phi_scale, const double* __restrict__ x,
-    double* __restrict__ y) {
+    double* __restrict__ y, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
    extern __shared__ __align__(16) char smem_raw[];
+   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
+   x += blockIdx.y * bs.n;
+   y += blockIdx.y * bs.n;
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    const int leaf = blockIdx.x * (blockDim.x >> 5) + warp;
    if (leaf >= n_leaf) return;
@@ -1374,7 +1410,9 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
 template <typename T>
 __global__ void far_add_kernel(int64_t nrows, const int32_t* __restrict__ rows, const T* __restrict__ staging,
                                int stage_levels, int64_t total_points, const int32_t* __restrict__ point_out,
-                               double* __restrict__ y) {
+                               double* __restrict__ y, BatchStrides bs) {
+   staging += blockIdx.y * bs.staging;  // right-hand side blockIdx.y of a batch
+   y += blockIdx.y * bs.n;
    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x) {
       const int pnt = rows[i];
       double v = 0.0;
@@ -1463,12 +1501,24 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    near_stride_ = maxcols;
    near_warps_ = (int)std::max<size_t>(1, std::min<size_t>(kNearThreads / 32, (size_t)optin / (maxcols * sizeof(T2))));
    leaf_smem_max_ = (int)(near_warps_ * maxcols * sizeof(T2));
-   int tile_smem = 0;
-   for (const TileGroup& g : tile_groups_) tile_smem = std::max(tile_smem, translate_smem(g));
+   int tile_smem = 0, tile_smem_b = 0;
+   for (const TileGroup& g : tile_groups_) {
+      tile_smem = std::max(tile_smem, translate_smem(g, false));
+      tile_smem_b = std::max(tile_smem_b, translate_smem(g, true));
+   }
    if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || tile_smem > optin)
       throw Error(FFTSVD_ERR_UNSUPPORTED, "operator block needs more shared memory than the device offers");
-   if (tile_smem > 0)
-      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
+   if (tile_smem > 0) {
+      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
+      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem_b));
+   }
+   // FFTSVD_B200_WARP_MIN_CUBES overrides the cube count from which small grids run
+   // one cube per warp (tests set 0 to cover those kernels on small surfaces)
+   warp_min_cubes_ = kWarpMinCubes;
+   if (const char* e = std::getenv("FFTSVD_B200_WARP_MIN_CUBES")) warp_min_cubes_ = std::max(0, std::atoi(e));
+   spectra_elems_ = std::max<int64_t>(L.spectra_elems, 1);
+   translated_elems_ = std::max<int64_t>(L.translated_elems, 1);
+   batch_capacity_ = 0;
    FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, src_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dst_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(near_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, leaf_smem_max_));
@@ -1484,11 +1534,13 @@ void DeviceOperator<T>::enable_timing(bool on) {
 }
 
 template <typename T>
-int DeviceOperator<T>::translate_smem(const TileGroup& g) const {
+int DeviceOperator<T>::translate_smem(const TileGroup& g, bool batch) const {
    // two chunk rows per slot (and the zero row) and per halo source, pairs, per-destination
    // {begin, count} and offsets, halo offsets; each carve aligned to 16 bytes
-   return (int)(2 * (kTileZeroSlot + 1) * kTileRowBytes + (size_t)2 * g.max_src * kTileRowBytes + (size_t)g.max_pairs * sizeof(uint32_t) +
-                (size_t)g.max_dst * (sizeof(int2) + sizeof(int64_t)) + (size_t)g.max_src * sizeof(int64_t) + 128);
+   const size_t slot_row = batch ? 16 : kTileRowBytes;
+   return (int)(2 * (kTileZeroSlot + 1) * slot_row + (size_t)2 * g.max_src * kTileRowBytes +
+                (size_t)g.max_pairs * sizeof(uint32_t) + (size_t)g.max_dst * (sizeof(int2) + sizeof(int64_t)) +
+                (size_t)g.max_src * sizeof(int64_t) + 128);
 }
 
 template <typename T>
@@ -1499,99 +1551,155 @@ void DeviceOperator<T>::stage_ms(float* ms) const {
    for (int k = 0; k < kNumKernels; k++) FFTSVD_CUDA(cudaEventElapsedTime(&ms[k], ev_[k], ev_[k + 1]));
 }
 
-static bool warp_path(const LaunchGroup& g) {
+template <typename T>
+bool DeviceOperator<T>::warp_path(const LaunchGroup& g) const {
    return g.n >= kWarpMinN && g.n <= kWarpMaxN && g.max_rank >= 1 && g.max_rank <= kWarpMaxRank &&
-          g.count >= kWarpMinCubes;
+          g.count >= warp_min_cubes_;
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_forward(const LaunchGroup& g, cudaStream_t stream) {
+void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream) {
    if (warp_path(g)) {
-      const int blocks = (g.count + kWarpCubes - 1) / kWarpCubes;
+      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes, b.nrhs);
       const SrcDesc* c = src_.get() + g.begin;
       if (g.n == 3)
-         far_forward_warp_kernel<T, 3><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
-                                                                           vt_.get(), pv_.get(), spectra_.get());
+         far_forward_warp_kernel<T, 3><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd,
+                                                                         vt_.get(), pv_.get(), b.spectra, b.bs);
       else if (g.n == 4)
-         far_forward_n4_kernel<T><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
-                                                                       vt_.get(), pv_.get(), spectra_.get());
+         far_forward_n4_kernel<T><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd, vt_.get(),
+                                                                     pv_.get(), b.spectra, b.bs);
       else
-         far_forward_warp_kernel<T, 5><<<blocks, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), xsd_.get(),
-                                                                           vt_.get(), pv_.get(), spectra_.get());
+         far_forward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd,
+                                                                         vt_.get(), pv_.get(), b.spectra, b.bs);
    } else {
       const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_forward_kernel<T><<<g.count, far_threads(g.n), smem, stream>>>(src_.get() + g.begin, src_panels_.get(),
-                                                                         xsd_.get(), vt_.get(), pv_.get(), spectra_.get());
+      far_forward_kernel<T><<<dim3(g.count, b.nrhs), far_threads(g.n), smem, stream>>>(
+          src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
    }
    FFTSVD_CHECK_LAUNCH();
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_translate(const TileGroup& g, cudaStream_t stream) {
+void DeviceOperator<T>::launch_translate(const TileGroup& g, const Bufs& b, cudaStream_t stream) {
    // split each tile's frequency chunks over several blocks so that even the few
    // tiles of the coarse levels fill the device (about eight blocks per SM in total)
-   const int nchunks = g.pg / (kTileRowBytes / (int)sizeof(T2));
-   const int total = g.count * nchunks;
-   const int cpb = std::max(1, std::min(nchunks, total / (8 * 148)));
-   const dim3 grid(g.count, (nchunks + cpb - 1) / cpb);
-   translate_kernel<T><<<grid, kTranslateThreads, translate_smem(g), stream>>>(
-       tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(), t_.get(),
-       spectra_.get(), translated_.get(), cpb);
+   const bool batch = b.nrhs > 1;
+   const int groups = batch ? b.nrhs / kBatchGroup : 1;
+   const int nchunks = g.pg / (batch ? 16 / (int)sizeof(T2) : kTileRowBytes / (int)sizeof(T2));
+   const int64_t total = (int64_t)g.count * nchunks * groups;
+   const int cpb = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, total / (8 * 148)));
+   const dim3 grid(g.count, (nchunks + cpb - 1) / cpb, groups);
+   if (batch)
+      translate_kernel<T, true><<<grid, kTranslateThreads, translate_smem(g, true), stream>>>(
+          tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(),
+          t_.get(), b.spectra, b.translated, cpb, b.bs);
+   else
+      translate_kernel<T, false><<<grid, kTranslateThreads, translate_smem(g, false), stream>>>(
+          tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(),
+          t_.get(), b.spectra, b.translated, cpb, b.bs);
    FFTSVD_CHECK_LAUNCH();
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_backward(const LaunchGroup& g, cudaStream_t stream) {
+void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream) {
    if (warp_path(g)) {
-      const int blocks = (g.count + kWarpCubes - 1) / kWarpCubes;
+      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes, b.nrhs);
       const DstDesc* c = dst_.get() + g.begin;
       if (g.n == 3)
-         far_backward_warp_kernel<T, 3><<<blocks, kWarpThreads, 0, stream>>>(
-             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+         far_backward_warp_kernel<T, 3><<<grid, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
       else if (g.n == 4)
-         far_backward_n4_kernel<T><<<blocks, kWarpThreads, 0, stream>>>(
-             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+         far_backward_n4_kernel<T><<<grid, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
       else
-         far_backward_warp_kernel<T, 5><<<blocks, kWarpThreads, 0, stream>>>(
-             c, g.count, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(), total_points_);
+         far_backward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(
+             c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
    } else {
       const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_backward_kernel<T><<<g.count, far_threads(g.n), smem, stream>>>(
-          dst_.get() + g.begin, dst_points_.get(), translated_.get(), uti_.get(), u_.get(), staging_.get(),
-          total_points_);
+      far_backward_kernel<T><<<dim3(g.count, b.nrhs), far_threads(g.n), smem, stream>>>(
+          dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
    }
    FFTSVD_CHECK_LAUNCH();
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_chain(const Chain& ch, cudaStream_t stream) {
-   for (int i : ch.src) launch_forward(src_groups_[i], stream);
-   for (int i : ch.tile) launch_translate(tile_groups_[i], stream);
-   for (int i : ch.dst) launch_backward(dst_groups_[i], stream);
+void DeviceOperator<T>::launch_chain(const Chain& ch, const Bufs& b, cudaStream_t stream) {
+   for (int i : ch.src) launch_forward(src_groups_[i], b, stream);
+   for (int i : ch.tile) launch_translate(tile_groups_[i], b, stream);
+   for (int i : ch.dst) launch_backward(dst_groups_[i], b, stream);
 }
 
 template <typename T>
 void DeviceOperator<T>::apply(const double* x, double* y, cudaStream_t stream) {
+   Bufs b;
+   b.xsd = xsd_.get();
+   b.spectra = spectra_.get();
+   b.translated = translated_.get();
+   b.staging = staging_.get();
+   b.nrhs = 1;
+   apply_bufs(x, y, b, stream);
+}
+
+template <typename T>
+void DeviceOperator<T>::apply_batch(const double* x, double* y, int nrhs, cudaStream_t stream) {
+   FFTSVD_REQUIRE(nrhs > 0 && nrhs % kBatchGroup == 0 && nrhs <= kMaxBatch, "batch size");
+   if (nrhs > batch_capacity_) {
+      // planar buffers, one copy of every intermediate per right-hand side; padding
+      // entries, the zero slot and unwritten staging rows stay zero
+      xsd_b_.alloc((int64_t)nrhs * total_panels_);
+      xsd_b_.zero();
+      spectra_b_.alloc((int64_t)nrhs * spectra_elems_);
+      spectra_b_.zero();
+      translated_b_.alloc((int64_t)nrhs * translated_elems_);
+      translated_b_.zero();
+      staging_b_.alloc(std::max<int64_t>((int64_t)nrhs * stage_levels_ * total_points_, 1));
+      staging_b_.zero();
+      FFTSVD_CUDA(cudaDeviceSynchronize());
+      batch_capacity_ = nrhs;
+   }
+   Bufs b;
+   b.xsd = xsd_b_.get();
+   b.spectra = spectra_b_.get();
+   b.translated = translated_b_.get();
+   b.staging = staging_b_.get();
+   b.nrhs = nrhs;
+   b.bs.n = num_unknowns_;
+   b.bs.panels = total_panels_;
+   b.bs.spectra = spectra_elems_;
+   b.bs.translated = translated_elems_;
+   b.bs.staging = (int64_t)stage_levels_ * total_points_;
+   apply_bufs(x, y, b, stream);
+}
+
+template <typename T>
+size_t DeviceOperator<T>::batch_bytes_per_rhs() const {
+   return sizeof(T2) * (size_t)(total_panels_ + spectra_elems_ + translated_elems_) +
+          sizeof(T) * (size_t)stage_levels_ * total_points_;
+}
+
+template <typename T>
+void DeviceOperator<T>::apply_bufs(const double* x, double* y, const Bufs& b, cudaStream_t stream) {
    if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[0], stream));
-   if (!full_cover_) FFTSVD_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * num_unknowns_, stream));
+   if (!full_cover_) FFTSVD_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * num_unknowns_ * b.nrhs, stream));
    {
       const int64_t total = total_panels_ - 1;  // the zero slot is never written
       int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
       if (blocks < 1) blocks = 1;
-      join_kernel<T><<<blocks, 256, 0, stream>>>(total, join_phi_idx_.get(), join_phi_scale_.get(),
-                                                 join_dphi_idx_.get(), join_dphi_scale_.get(), x, xsd_.get());
+      join_kernel<T><<<dim3(blocks, b.nrhs), 256, 0, stream>>>(total, join_phi_idx_.get(), join_phi_scale_.get(),
+                                                              join_dphi_idx_.get(), join_dphi_scale_.get(), x, b.xsd,
+                                                              b.bs);
       FFTSVD_CHECK_LAUNCH();
    }
    if (timing_) {
       // stage by stage on one stream, so that each stage can be timed
       FFTSVD_CUDA(cudaEventRecord(ev_[1], stream));
-      for (const LaunchGroup& g : src_groups_) launch_forward(g, stream);
+      for (const LaunchGroup& g : src_groups_) launch_forward(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[2], stream));
-      for (const TileGroup& g : tile_groups_) launch_translate(g, stream);
+      for (const TileGroup& g : tile_groups_) launch_translate(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[3], stream));
-      for (const LaunchGroup& g : dst_groups_) launch_backward(g, stream);
+      for (const LaunchGroup& g : dst_groups_) launch_backward(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[4], stream));
-      launch_near(x, y, stream);
+      launch_near(x, y, b, stream);
    } else {
       // the near field and the far-field chains of each grid size (forward -> translate
       // -> backward) only share the joined input: all but the largest chain run on their
@@ -1600,30 +1708,31 @@ void DeviceOperator<T>::apply(const double* x, double* y, cudaStream_t stream) {
       FFTSVD_CUDA(cudaEventRecord(fork_, stream));
       for (size_t c = 0; c < chains_.size(); c++) {
          FFTSVD_CUDA(cudaStreamWaitEvent(chains_[c].stream, fork_, 0));
-         launch_chain(chains_[c], chains_[c].stream);
+         launch_chain(chains_[c], b, chains_[c].stream);
          FFTSVD_CUDA(cudaEventRecord(chains_[c].done, chains_[c].stream));
       }
       FFTSVD_CUDA(cudaStreamWaitEvent(near_stream_, fork_, 0));
-      launch_near(x, y, near_stream_);
+      launch_near(x, y, b, near_stream_);
       FFTSVD_CUDA(cudaEventRecord(near_done_, near_stream_));
       for (size_t c = 0; c < chains_.size(); c++) FFTSVD_CUDA(cudaStreamWaitEvent(stream, chains_[c].done, 0));
       FFTSVD_CUDA(cudaStreamWaitEvent(stream, near_done_, 0));
    }
    if (n_rows_ > 0 && stage_levels_ > 0) {
       const int blocks = (int)std::min<int64_t>((n_rows_ + 255) / 256, 148 * 8);
-      far_add_kernel<T><<<blocks, 256, 0, stream>>>(n_rows_, leaf_rows_.get(), staging_.get(), stage_levels_,
-                                                    total_points_, point_out_.get(), y);
+      far_add_kernel<T><<<dim3(blocks, b.nrhs), 256, 0, stream>>>(n_rows_, leaf_rows_.get(), b.staging, stage_levels_,
+                                                                 total_points_, point_out_.get(), y, b.bs);
       FFTSVD_CHECK_LAUNCH();
    }
    if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[5], stream));
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_near(const double* x, double* y, cudaStream_t stream) {
+void DeviceOperator<T>::launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream) {
    if (n_leaf_ == 0) return;
-   near_kernel<T><<<(n_leaf_ + near_warps_ - 1) / near_warps_, 32 * near_warps_, leaf_smem_max_, stream>>>(
-       leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), xsd_.get(),
-       point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(), join_phi_scale_.get(), x, y);
+   near_kernel<T><<<dim3((n_leaf_ + near_warps_ - 1) / near_warps_, b.nrhs), 32 * near_warps_, leaf_smem_max_,
+                    stream>>>(leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), b.xsd,
+                              point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(),
+                              join_phi_scale_.get(), x, y, b.bs);
    FFTSVD_CHECK_LAUNCH();
 }
 

@@ -89,6 +89,19 @@ struct LaunchGroup {
    int max_rank = 0;    // largest row (sources) or column (destinations) rank
 };
 
+// Per-right-hand-side strides of the planar batch buffers: right-hand side r of a
+// batched launch (blockIdx.y, or group blockIdx.z of kBatchGroup in the
+// translation) reads and writes base + r * stride.  All zero for a single vector.
+struct BatchStrides {
+   int64_t n = 0;           // x, y (FP64 unknowns)
+   int64_t panels = 0;      // joined panel values
+   int64_t spectra = 0;     // source spectra (complex)
+   int64_t translated = 0;  // translated spectra (complex)
+   int64_t staging = 0;     // far-field staging rows
+};
+constexpr int kBatchGroup = 8;   // right-hand sides per batched translation row
+constexpr int kMaxBatch = 65535; // grid y limit
+
 // Small grids (n <= kWarpMaxN) whose cubes all have rank <= 32 run one cube per
 // warp instead of one cube per block.
 constexpr int kWarpMinN = 3;
@@ -163,6 +176,12 @@ class DeviceOperator {
    void upload(const OperatorLayout& L);
    // y = A x on `stream`; x, y device pointers of num_unknowns doubles.
    void apply(const double* x, double* y, cudaStream_t stream);
+   // Y = A X for nrhs right-hand sides (a multiple of kBatchGroup, at most kMaxBatch),
+   // X and Y column-major (right-hand side r at x + r * num_unknowns).  Every column
+   // goes through the same arithmetic as apply(); the batch buffers grow on demand.
+   void apply_batch(const double* x, double* y, int nrhs, cudaStream_t stream);
+   // device bytes of the batch buffers per right-hand side
+   size_t batch_bytes_per_rhs() const;
    // per-stage events for timing (recorded when enabled)
    void enable_timing(bool on);
    // milliseconds of [join, far_forward, translate, far_backward, near] of the last timed apply
@@ -179,12 +198,28 @@ class DeviceOperator {
       cudaStream_t stream = nullptr;    // own stream (the first, longest chain at high priority)
       cudaEvent_t done = nullptr;
    };
-   int translate_smem(const TileGroup& g) const;
-   void launch_forward(const LaunchGroup& g, cudaStream_t stream);
-   void launch_translate(const TileGroup& g, cudaStream_t stream);
-   void launch_backward(const LaunchGroup& g, cudaStream_t stream);
-   void launch_chain(const Chain& ch, cudaStream_t stream);
-   void launch_near(const double* x, double* y, cudaStream_t stream);
+   // intermediate buffers of one apply: the single-vector members or the planar batch
+   struct Bufs {
+      T2* xsd = nullptr;
+      T2* spectra = nullptr;
+      T2* translated = nullptr;
+      T* staging = nullptr;
+      int nrhs = 1;
+      BatchStrides bs;
+   };
+   int translate_smem(const TileGroup& g, bool batch) const;
+   void apply_bufs(const double* x, double* y, const Bufs& b, cudaStream_t stream);
+   void launch_forward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream);
+   void launch_translate(const TileGroup& g, const Bufs& b, cudaStream_t stream);
+   void launch_backward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream);
+   void launch_chain(const Chain& ch, const Bufs& b, cudaStream_t stream);
+   void launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream);
+   bool warp_path(const LaunchGroup& g) const;
+   int warp_min_cubes_ = kWarpMinCubes;
+   int64_t spectra_elems_ = 1, translated_elems_ = 1;
+   int batch_capacity_ = 0;
+   DevBuf<T2> xsd_b_, spectra_b_, translated_b_;
+   DevBuf<T> staging_b_;
    void build_chains();
    void release_chains();
    std::vector<Chain> chains_;

@@ -8,6 +8,7 @@
 #include <numeric>
 #include <string>
 
+#include "batch.h"
 #include "nbody.h"
 #include "surface.h"
 
@@ -108,7 +109,7 @@ void Preconditioner::build(const fftsvd_precond_csc& P, int n) {
 void Preconditioner::apply(const double* r, double* z, cudaStream_t s) const {
    const int threads = 256;
    const int blocks = std::max(1, std::min((nblocks + threads - 1) / threads, 148 * 8));
-   precond_kernel<<<blocks, threads, 0, s>>>(nblocks, blk_ptr.get(), blk_idx.get(), inv_off.get(), inv.get(), r, z);
+   precond_kernel<<<blocks, threads, 0, s>>>(nblocks, blk_ptr.get(), blk_idx.get(), inv_off.get(), inv.get(), r, z, 0);
    FFTSVD_CHECK_LAUNCH();
 }
 
@@ -143,9 +144,9 @@ void Surface::apply(int precision, const double* x, double* yv) {
 
 double Surface::pnorm(const double* v) {
    const int nb = vec_blocks(n);
-   norm_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, v, normpart.get());
+   norm_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, v, normpart.get(), 0, 0);
    FFTSVD_CHECK_LAUNCH();
-   reduce_partial_kernel<<<1, 256, 0, stream>>>(1, nb, normpart.get(), scal.get(), 0);
+   reduce_partial_kernel<<<1, 256, 0, stream>>>(1, nb, normpart.get(), scal.get(), 0, 0, 0);
    FFTSVD_CHECK_LAUNCH();
    double s = 0.0;
    FFTSVD_CUDA(cudaMemcpyAsync(&s, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -174,7 +175,7 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
    }
    double* Vp = V.get();
    const int64_t ldv = n;
-   scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, r.get(), nullptr, 1.0 / normr, Vp);
+   scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, r.get(), nullptr, 1.0 / normr, Vp, 0, 0);
    FFTSVD_CHECK_LAUNCH();
    FFTSVD_CUDA(cudaMemsetAsync(g.get(), 0, sizeof(double) * capacity, stream));
    FFTSVD_CUDA(cudaMemcpyAsync(g.get(), &normr, sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -191,21 +192,22 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       double* vnext = Vp + (int64_t)(i + 1) * ldv;
       apply(precision, vi, w.get());
       precond.apply(w.get(), w.get(), stream);
-      dots_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get());
+      dots_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h1.get(), 0);
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h1.get(), 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
       const size_t sh = sizeof(double) * (((nvec + 1) & ~1) + kVecThreads / 32 * 8 + 8);
-      update_dots_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), partial.get());
+      update_dots_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), partial.get(), 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h2.get(), 0);
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h2.get(), 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      update_norm_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get());
+      update_norm_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get(), 0,
+                                                           0, 0);
       FFTSVD_CHECK_LAUNCH();
       givens_kernel<<<1, 256, 0, stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb, cs.get(),
-                                           sn.get(), g.get(), st.get());
+                                           sn.get(), g.get(), st.get(), 0, 0, nullptr);
       FFTSVD_CHECK_LAUNCH();
-      scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext);
+      scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext, 0, 0);
       FFTSVD_CHECK_LAUNCH();
       FFTSVD_CUDA(cudaMemcpyAsync(st_host, st.get(), sizeof(GivensState), cudaMemcpyDeviceToHost, stream));
       FFTSVD_CUDA(cudaStreamSynchronize(stream));
@@ -233,7 +235,7 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       for (int j = q - 1; j >= 0; j--) yh[j] -= Hh[(size_t)q * capacity + j] * yh[q];
    }
    FFTSVD_CUDA(cudaMemcpyAsync(y.get(), yh.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream));
-   combine_kernel<<<ew_blocks, 256, sizeof(double) * k, stream>>>(n, k, Vp, ldv, y.get(), x);
+   combine_kernel<<<ew_blocks, 256, sizeof(double) * k, stream>>>(n, k, Vp, ldv, y.get(), x, 0, 0);
    FFTSVD_CHECK_LAUNCH();
    FFTSVD_CUDA(cudaStreamSynchronize(stream));
    *res = resid;
@@ -267,10 +269,10 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
          const double inner_tol = std::min(0.1, std::max(0.3 * tol / res, 1e-13));
          iters += gmres(FFTSVD_PREC_FP32, t1.get(), xout.get(), inner_tol, maxit, &inner_res, &st2, false);
          if (st2 == FFTSVD_ERR_NONFINITE) { status = st2; break; }
-         add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x);
+         add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x, 0);
          FFTSVD_CHECK_LAUNCH();
          op64.apply(x, t2.get(), stream);
-         sub_kernel<<<ew_blocks, 256, 0, stream>>>(n, rhs, t2.get(), t1.get());
+         sub_kernel<<<ew_blocks, 256, 0, stream>>>(n, rhs, t2.get(), t1.get(), 0);
          FFTSVD_CHECK_LAUNCH();
          precond.apply(t1.get(), t0.get(), stream);
          res = pnorm(t0.get()) / bn;
@@ -327,23 +329,6 @@ void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree
 }  // namespace fftsvd
 
 using namespace fftsvd;
-
-template <typename F>
-static int guarded(F&& f) {
-   try {
-      f();
-      return FFTSVD_OK;
-   } catch (const Error& e) {
-      set_last_error(e.what());
-      return e.code;
-   } catch (const std::bad_alloc&) {
-      set_last_error("host allocation failed");
-      return FFTSVD_ERR_ARGUMENT;
-   } catch (const std::exception& e) {
-      set_last_error(e.what());
-      return FFTSVD_ERR_ARGUMENT;
-   }
-}
 
 extern "C" {
 

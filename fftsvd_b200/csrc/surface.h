@@ -9,6 +9,7 @@
 #include <memory>
 #include <vector>
 
+#include "batch.h"
 #include "common.h"
 #include "gmres.cuh"
 #include "operator.h"
@@ -62,6 +63,21 @@ struct Surface {
    int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
              bool absolute_zero_check = true);
    int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
+
+   // ---- many right-hand sides (batch.cu); blocks of ncols vectors, column c at base + c * n
+   std::unique_ptr<BatchWorkspace> bw;
+   int batch_chunk32 = 0, batch_chunk64 = 0;  // columns per batched matvec launch sequence
+   int batch_chunk(int precision);
+   void apply_batch(int precision, const double* X, double* Y, int ncols);
+   void precond_batch(const double* r, double* z, int ncols);
+   void pnorm_batch(const double* v, int ncols, std::vector<double>& out);
+   // Lockstep GMRES over ncols columns; columns with run[c] == 0 stay zero.
+   int gmres_batch(int precision, int ncols, const double* rhs, double* x, const std::vector<double>& tol, int maxit,
+                   const std::vector<char>& run, bool absolute_zero_check, std::vector<double>& res,
+                   std::vector<int>& iters, std::vector<int>& status);
+   // k right-hand sides; info may be null or hold k entries.  Returns the first non-OK status.
+   int solve_batch(int precision, int k, const double* rhs, double* x, double tol, int maxit,
+                   fftsvd_solve_info* info);
 };
 
 void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,

@@ -30,6 +30,8 @@ EXPORTED = [
     "fftsvd_b200_host_operator_tree", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
     "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
     "fftsvd_b200_launch_count", "fftsvd_b200_reaction_potentials_noalloc", "solveSurfaceOperator", "generateRHS",
+    "fftsvd_b200_matvec_batch_device", "fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch",
+    "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
 ]
 
 
@@ -84,6 +86,12 @@ def load():
     lib.fftsvd_b200_surface_stream.restype = C.c_void_p
     lib.fftsvd_b200_launch_count.restype = C.c_longlong
     lib.fftsvd_b200_reaction_potentials_noalloc.argtypes = [sp, C.c_void_p, C.c_void_p]
+    lib.fftsvd_b200_matvec_batch_device.argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    for name in ("fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch"):
+        getattr(lib, name).argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
+                                       C.POINTER(SolveInfo)]
+    lib.fftsvd_b200_rhs_groups_device.argtypes = [sp, C.c_int32, _i32p, C.c_void_p]
+    lib.fftsvd_b200_group_energies_device.argtypes = [sp, C.c_int32, _i32p, C.c_void_p, _f64p]
     _lib = lib
     return lib
 

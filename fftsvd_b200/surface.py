@@ -238,6 +238,44 @@ class Surface:
     def reaction_potentials_device(self, sol_ptr: int, phi_ptr: int):
         check(load().fftsvd_b200_reaction_potentials_device(self._h, C.c_void_p(sol_ptr), C.c_void_p(phi_ptr)))
 
+    # ---- many right-hand sides (blocks of k vectors, one after the other)
+    def matvec_batch_device(self, x_ptr: int, y_ptr: int, nrhs: int, precision="fp32"):
+        check(load().fftsvd_b200_matvec_batch_device(self._h, _prec(precision), int(nrhs), C.c_void_p(x_ptr),
+                                                     C.c_void_p(y_ptr)))
+
+    def solve_batch_device(self, rhs_ptr: int, sol_ptr: int, nrhs: int, precision="mixed", tol=1e-6,
+                           max_iterations=1000, raise_on_error=True):
+        """Returns the per-column SolveInfo array."""
+        info = (SolveInfo * int(nrhs))()
+        rc = load().fftsvd_b200_solve_batch_device(self._h, int(nrhs), _prec(precision), C.c_void_p(rhs_ptr),
+                                                   C.c_void_p(sol_ptr), float(tol), int(max_iterations), info)
+        if raise_on_error:
+            check(rc)
+        return info
+
+    def solve_batch(self, rhs, precision="mixed", tol=1e-6, max_iterations=1000, raise_on_error=True):
+        """rhs: (k, n) host array.  Returns (solutions (k, n), per-column SolveInfo array)."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        k = rhs.shape[0]
+        sol = np.empty_like(rhs)
+        info = (SolveInfo * k)()
+        rc = load().fftsvd_b200_solve_batch(self._h, k, _prec(precision), rhs.ctypes.data, sol.ctypes.data,
+                                            float(tol), int(max_iterations), info)
+        if raise_on_error:
+            check(rc)
+        return sol, info
+
+    def rhs_groups_device(self, group_ptr, rhs_ptr: int):
+        gp = i32(group_ptr)
+        check(load().fftsvd_b200_rhs_groups_device(self._h, len(gp) - 1, ptr(gp, C.c_int32), C.c_void_p(rhs_ptr)))
+
+    def group_energies_device(self, group_ptr, sol_ptr: int):
+        gp = i32(group_ptr)
+        e = np.empty(len(gp) - 1)
+        check(load().fftsvd_b200_group_energies_device(self._h, len(gp) - 1, ptr(gp, C.c_int32), C.c_void_p(sol_ptr),
+                                                       ptr(e)))
+        return e
+
 
 def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4,
                   num_threads=0):

@@ -254,6 +254,42 @@ int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const doubl
                                double* ms5);
 /* The CUDA stream all work of this surface is issued on (cudaStream_t). */
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s);
+
+/* ---- many right-hand sides of one surface (no counterpart in the reference;
+   the batched solve named by the port's plan, fftsvd_b200_solve_batch) ----
+   Blocks of k vectors of fftsvd_b200_num_unknowns doubles are stored one vector
+   after the other (vector c at base + c * num_unknowns). */
+
+/* Y = A X for nrhs vectors, device pointers.  The multi-vector matvec reads every
+   operator element and translation table once per group of 8 right-hand sides;
+   each column goes through the same arithmetic as fftsvd_b200_matvec_device.
+   Like that call it is issued on the surface's stream and returns before it
+   finishes (when nrhs is not a multiple of 8 it waits for a padded copy). */
+int fftsvd_b200_matvec_batch_device(fftsvd_surface* s, int32_t precision, int32_t nrhs, const double* x, double* y);
+/* Solves A x_c = rhs_c for nrhs columns at once: lockstep GMRES in which every
+   column keeps its own Krylov basis, Hessenberg matrix, Givens rotations and
+   stopping test (as fftsvd_b200_solve), over the multi-vector matvec.  For
+   FFTSVD_PREC_MIXED each column is refined in FP64 as in fftsvd_b200_solve.
+   info is NULL or holds nrhs entries (solve_ms is the whole batch).  The basis
+   of all columns stays on the device: max_iterations + 1 vectors per column,
+   fewer if a third of the free device memory cannot hold them (columns that
+   reach that bound report FFTSVD_ERR_NOT_CONVERGED).  Returns the first
+   column's non-OK status, else FFTSVD_OK. */
+int fftsvd_b200_solve_batch_device(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                                   double tol, int32_t max_iterations, fftsvd_solve_info* info);
+/* Same with host pointers. */
+int fftsvd_b200_solve_batch(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                            double tol, int32_t max_iterations, fftsvd_solve_info* info);
+/* Right-hand sides of charge groups: group g is the surface's charges
+   [group_ptr[g], group_ptr[g+1]) (host array of ngroups + 1 non-decreasing
+   offsets); rhs (device) receives ngroups vectors (SurfaceOperator.c:291-321
+   restricted to the group). */
+int fftsvd_b200_rhs_groups_device(fftsvd_surface* s, int32_t ngroups, const int32_t* group_ptr, double* rhs);
+/* Solvation energy of each charge group from its own solution column (device
+   sol, ngroups vectors): 0.5 sum over the group of q phi_reac * 332.112 / eps_in,
+   phi_reac from that column only.  energies is a host array of ngroups. */
+int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const int32_t* group_ptr, const double* sol,
+                                      double* energies);
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
 

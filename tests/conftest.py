@@ -25,3 +25,11 @@ def gpu():
     if not has_gpu():
         pytest.fail("this test needs a CUDA device")
     return True
+
+
+@pytest.fixture(scope="module")
+def monkeypatch_module():
+    """A monkeypatch that lives as long as a module-scoped fixture."""
+    mp = pytest.MonkeyPatch()
+    yield mp
+    mp.undo()

@@ -72,3 +72,28 @@ def test_reaction_potentials_match_reference(case32):
     rs, s, _ = case32
     sol = np.random.default_rng(6).standard_normal(s.n)
     assert rel(s.reaction_potentials(sol), rs.reaction(sol)) < 1e-11
+
+
+@pytest.fixture(scope="module", params=["blob3", "blob4"])
+def case_warp(request, gpu, monkeypatch_module):
+    """The reference operator with every small grid (n <= 5) on the one-cube-per-warp
+    kernels (the 4^3 grid on its register DFT), which large surfaces select by cube
+    count: the threshold is lowered to zero for this surface."""
+    if not ref.available(fp64=True):
+        pytest.fail("oracle/_ref/libfftsvd_ref64.so missing")
+    monkeypatch_module.setenv("FFTSVD_B200_WARP_MIN_CUBES", "0")
+    rs64, tri, c = ref_system(request.param, fp64=True)
+    s64 = surface_from_reference(rs64, tri, c)
+    rs32, _, _ = ref_system(request.param, fp64=False)
+    s32 = surface_from_reference(rs32, tri, c)
+    monkeypatch_module.delenv("FFTSVD_B200_WARP_MIN_CUBES")
+    return rs64, s64, rs32, s32
+
+
+def test_warp_kernels_match_reference(case_warp):
+    rs64, s64, rs32, s32 = case_warp
+    rng = np.random.default_rng(12)
+    for _ in range(2):
+        x = rng.standard_normal(s64.n)
+        assert rel(s64.matvec(x, "fp64"), rs64.matvec(x)) < TOL_FP64
+        assert rel(s32.matvec(x, "fp32"), rs32.matvec(x)) < TOL_FP32
