@@ -42,6 +42,9 @@ CONFIGS = {
                   level=5, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1),
     "large": dict(name="large blob L7 (327680 panels, R 60 A, 30000 charges, eps 4/80, kappa 0.125)", kind="blob",
                   level=7, radius=60.0, nq=30000, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=3),
+    # many right-hand sides: the blob surface with its charges in 256 seeded disjoint groups
+    "batch": dict(name="blob L6 (81920 panels), 256 right-hand sides of ~10 charges each", kind="blob",
+                  level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, groups=256),
 }
 SVD_TOL = 1e-4
 GMRES_TOL = 1e-6
@@ -374,6 +377,100 @@ def run_ours(args, cfg, ws, rank, local):
     s.close()
 
 
+def charge_groups(num_charges, groups, seed):
+    """Seeded disjoint charge groups of nearly equal size: a permutation of the charges
+    (group members contiguous after it) and the group offsets."""
+    rng = np.random.default_rng(seed + 1000)
+    perm = rng.permutation(num_charges)
+    base, extra = divmod(num_charges, groups)
+    sizes = [base + (1 if g < extra else 0) for g in range(groups)]
+    gptr = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    return perm, gptr
+
+
+def run_batch(args, cfg, ws, rank, local):
+    """Batched solve: every charge group's right-hand side in one lockstep GMRES over the
+    multi-vector matvec (mixed precision, then FP64), groups sharded over ranks."""
+    import torch
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface
+
+    torch.cuda.set_device(local)
+    lib = load()
+    tri, qpos, q = make_workload(cfg)
+    perm, gptr = charge_groups(len(q), cfg["groups"], cfg["seed"])
+    qpos, q = qpos[perm], q[perm]
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    n = s.n
+    mine = replica_shares(cfg["groups"], ws)[rank]
+    sub = gptr[mine.start:mine.stop + 1].astype(np.int32)
+    k = len(sub) - 1
+    stream = torch.cuda.ExternalStream(lib.fftsvd_b200_surface_stream(s._h))
+    R = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    S = torch.empty_like(R)
+    s.rhs_groups_device(sub, R.data_ptr())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    maxit = 150
+
+    def timed(precision, steps, warm):
+        for _ in range(warm):
+            s.solve_batch_device(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
+        total, info = 0.0, None
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = s.solve_batch_device(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total, info
+
+    torch.cuda.synchronize()
+    barrier(ws)
+    launches0 = lib.fftsvd_b200_launch_count()
+    with ClockSampler(local) as clk:
+        t_mixed, info_m = timed("mixed", args.steps, max(1, args.warmup - 2))
+    launches = (lib.fftsvd_b200_launch_count() - launches0) // (args.steps + max(1, args.warmup - 2))
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_max = barrier_max(t_mixed / args.steps, ws)
+    e_mixed = s.group_energies_device(sub, S.data_ptr())
+    t64, info64 = timed("fp64", 1, 0)
+    e64 = s.group_energies_device(sub, S.data_ptr())
+    errs = [abs(a - b) / abs(b) for a, b in zip(e_mixed, e64) if b != 0.0]
+    # one right-hand side solved alone (same surface, same kernels) for the per-column comparison
+    one = R[0].clone()
+    sol1 = torch.empty_like(one)
+    for _ in range(2):
+        s.solve_device(one.data_ptr(), sol1.data_ptr(), "mixed", GMRES_TOL)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        s.solve_device(one.data_ptr(), sol1.data_ptr(), "mixed", GMRES_TOL)
+    e1.record(stream)
+    e1.synchronize()
+    single_ms = e0.elapsed_time(e1) / 3
+    if rank == 0:
+        its = [info_m[c].iterations for c in range(k)]
+        line = {
+            "metric": f"batched mixed-precision PBE solve ms ({cfg['groups']} charge-group right-hand sides)",
+            "value": t_max, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 operator, f64 Krylov vectors and refinement", "data": "synthetic",
+            "config": {"workload": cfg["name"], "groups": cfg["groups"], "rhs_per_rank": k, "gmres_tol": GMRES_TOL,
+                       "svd_tol": SVD_TOL, "l2": "256 MiB buffer written between timed solves"},
+            "ms_per_rhs": t_max / k, "fp64_batch_ms": t64, "speedup_mixed_vs_fp64": t64 / t_max,
+            "single_solve_ms": single_ms, "batch_throughput_vs_single": single_ms * k / t_max,
+            "dG_rel_err_mixed_vs_fp64_max": max(errs) if errs else None,
+            "iterations_mixed_max": max(its), "iterations_mixed_mean": sum(its) / len(its),
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    s.close()
+
+
 def run_matvec_only(args, cfg, local):
     """Build the surface and run `--reps` FP32 and FP64 matvecs (for profiler captures)."""
     import torch
@@ -382,11 +479,15 @@ def run_matvec_only(args, cfg, local):
     torch.cuda.set_device(local)
     tri, qpos, q = make_workload(cfg)
     s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
-    x = torch.randn(s.n, dtype=torch.float64, device="cuda")
+    k = 64 if "groups" in cfg else 1  # batched configuration: a 64-column multi-vector matvec
+    x = torch.randn((k, s.n), dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
     for prec in ("fp32", "fp64"):
         for _ in range(args.reps):
-            s.matvec_device(x.data_ptr(), y.data_ptr(), prec)
+            if k > 1:
+                s.matvec_batch_device(x.data_ptr(), y.data_ptr(), k, prec)
+            else:
+                s.matvec_device(x.data_ptr(), y.data_ptr(), prec)
     torch.cuda.synchronize()
     print(json.dumps({"matvec_only": cfg["name"], "reps": args.reps, "norm": float(y.norm())}))
     s.close()
@@ -412,6 +513,8 @@ def main():
             run_matvec_only(args, cfg, local)
         elif args.impl == "reference":
             run_reference(args, cfg, ws, rank)
+        elif "groups" in cfg:
+            run_batch(args, cfg, ws, rank, local)
         else:
             run_ours(args, cfg, ws, rank, local)
     finally:

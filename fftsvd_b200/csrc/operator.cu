@@ -561,10 +561,11 @@ __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
-   spectra += blockIdx.y * bs.spectra;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   xsd += rhs * bs.panels;
+   spectra += rhs * bs.spectra;
    extern __shared__ __align__(16) char smem_raw[];
-   const SrcDesc c = cubes[blockIdx.x];
+   const SrcDesc c = cubes[unit];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n;
    const int m = c.m, r = c.r;
    const int ch = min(m, kChunk);
@@ -743,10 +744,11 @@ __global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
    int2* dinfo = carve<int2>(p, t.ndst);
    int64_t* srcoff = carve<int64_t>(p, t.nsrc);
    int64_t* dstoff = carve<int64_t>(p, t.ndst);
-   // pairs pre-scaled to unit offsets: (source row << 16) | slot row
+   // pairs pre-scaled to byte offsets in the row buffers: (source row << 16) | slot row
+   // (at most 255 * U * 16 and 343 * TU * 16, both below 65536)
    for (int i = threadIdx.x; i < t.npairs; i += blockDim.x) {
       const uint32_t pr = tile_pairs[t.pair_off + i];
-      pairs[i] = ((pr >> 16) * (uint32_t)U) << 16 | ((pr & 0xffffu) * (uint32_t)TU);
+      pairs[i] = ((pr >> 16) * (uint32_t)(U * 16)) << 16 | ((pr & 0xffffu) * (uint32_t)(TU * 16));
    }
    for (int i = threadIdx.x; i < t.ndst; i += blockDim.x) {
       dinfo[i] = tile_dst_pairs[t.dst_off + i];
@@ -783,23 +785,31 @@ __global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
          cp_async_wait<0>();
       }
       __syncthreads();
-      const V* Ts = odd ? Tb1 : Tb0;
-      const V* Fs = odd ? Fb1 : Fb0;
+      // all shared accesses below are smem_raw plus a byte offset, so they compile to
+      // shared-window loads
+      const uint32_t ts = (uint32_t)((const char*)(odd ? Tb1 : Tb0) - smem_raw);
+      const uint32_t fs = (uint32_t)((const char*)(odd ? Fb1 : Fb0) - smem_raw);
+      const uint32_t ps = (uint32_t)((const char*)pairs - smem_raw);
       const int f0 = k * CH;
       // thread -> (destination, unit)
       for (int item = threadIdx.x; item < t.ndst * U; item += blockDim.x) {
          const int d = item / U, u = item % U;
-         const int tu = BATCH ? 0 : u;
+         const char* tsu = smem_raw + ts + (BATCH ? 0u : (uint32_t)u * 16u);
+         const char* fsu = smem_raw + fs + (uint32_t)u * 16u;
          const int2 di = dinfo[d];
          V acc = Pack16<T>::zero(), acc1 = Pack16<T>::zero();  // two chains of dependent FMAs
          // four pairs per 16-byte load; lists are padded to groups of four with the zero row
-         const uint4* pp = reinterpret_cast<const uint4*>(pairs + di.x);
+         const uint4* pp = reinterpret_cast<const uint4*>(smem_raw + ps + (uint32_t)di.x * 4u);
          for (int q = 0; q < (di.y >> 2); q++) {
             const uint4 pr = pp[q];
-            Pack16<T>::fma(acc, Ts[(pr.x & 0xffffu) + tu], Fs[(pr.x >> 16) + u]);
-            Pack16<T>::fma(acc1, Ts[(pr.y & 0xffffu) + tu], Fs[(pr.y >> 16) + u]);
-            Pack16<T>::fma(acc, Ts[(pr.z & 0xffffu) + tu], Fs[(pr.z >> 16) + u]);
-            Pack16<T>::fma(acc1, Ts[(pr.w & 0xffffu) + tu], Fs[(pr.w >> 16) + u]);
+            Pack16<T>::fma(acc, *reinterpret_cast<const V*>(tsu + (pr.x & 0xffffu)),
+                           *reinterpret_cast<const V*>(fsu + (pr.x >> 16)));
+            Pack16<T>::fma(acc1, *reinterpret_cast<const V*>(tsu + (pr.y & 0xffffu)),
+                           *reinterpret_cast<const V*>(fsu + (pr.y >> 16)));
+            Pack16<T>::fma(acc, *reinterpret_cast<const V*>(tsu + (pr.z & 0xffffu)),
+                           *reinterpret_cast<const V*>(fsu + (pr.z >> 16)));
+            Pack16<T>::fma(acc1, *reinterpret_cast<const V*>(tsu + (pr.w & 0xffffu)),
+                           *reinterpret_cast<const V*>(fsu + (pr.w >> 16)));
          }
          Pack16<T>::add(acc, acc1);
          if (BATCH)
@@ -820,10 +830,11 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
-   staging += blockIdx.y * bs.staging;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   translated += rhs * bs.translated;
+   staging += rhs * bs.staging;
    extern __shared__ __align__(16) char smem_raw[];
-   const DstDesc c = cubes[blockIdx.x];
+   const DstDesc c = cubes[unit];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n, pg = Np * Np * H;
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
 
@@ -915,8 +926,9 @@ __global__ void __launch_bounds__(kWarpThreads, 12) far_forward_warp_kernel(
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
-   spectra += blockIdx.y * bs.spectra;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   xsd += rhs * bs.panels;
+   spectra += rhs * bs.spectra;
    using G = SmallGrid<N>;
    constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
    constexpr unsigned kAll = 0xffffffffu;
@@ -929,7 +941,7 @@ __global__ void __launch_bounds__(kWarpThreads, 12) far_forward_warp_kernel(
       tw[threadIdx.x] = Cx<T>::make(cs, -sn);
    }
    __syncthreads();
-   const int cube = blockIdx.x * kWarpCubes + warp;
+   const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const SrcDesc c = cubes[cube];
    T2* A = work[warp];
@@ -1015,8 +1027,9 @@ __global__ void __launch_bounds__(kWarpThreads) far_backward_warp_kernel(
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
-   staging += blockIdx.y * bs.staging;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   translated += rhs * bs.translated;
+   staging += rhs * bs.staging;
    using G = SmallGrid<N>;
    constexpr int Np = G::Np, H = G::H, OFF = G::OFF, N3 = G::N3;
    constexpr unsigned kAll = 0xffffffffu;
@@ -1029,7 +1042,7 @@ __global__ void __launch_bounds__(kWarpThreads) far_backward_warp_kernel(
       tw[threadIdx.x] = Cx<T>::make(cs, sn);
    }
    __syncthreads();
-   const int cube = blockIdx.x * kWarpCubes + warp;
+   const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const DstDesc c = cubes[cube];
    T2* S = work[warp];
@@ -1120,8 +1133,9 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forw
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
-   spectra += blockIdx.y * bs.spectra;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   xsd += rhs * bs.panels;
+   spectra += rhs * bs.spectra;
    constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;  // ROW: complex values per fi
    constexpr unsigned kAll = 0xffffffffu;
    __shared__ T2 tw[Np];
@@ -1132,7 +1146,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forw
       tw[threadIdx.x] = Cx<T>::make(cs, -sn);
    }
    __syncthreads();
-   const int cube = blockIdx.x * kWarpCubes + warp;
+   const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const SrcDesc c = cubes[cube];
    const int m = c.m, r = c.r;  // r <= 32: lane j owns row j of VT
@@ -1231,8 +1245,9 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_back
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   translated += blockIdx.y * bs.translated;  // right-hand side blockIdx.y of a batch
-   staging += blockIdx.y * bs.staging;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   translated += rhs * bs.translated;
+   staging += rhs * bs.staging;
    constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;
    constexpr unsigned kAll = 0xffffffffu;
    __shared__ T2 tw[Np];
@@ -1244,7 +1259,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_back
       tw[threadIdx.x] = Cx<T>::make(cs, sn);
    }
    __syncthreads();
-   const int cube = blockIdx.x * kWarpCubes + warp;
+   const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const DstDesc c = cubes[cube];
    const int kq = lane & 3, jp = (lane >> 2) & 3;
@@ -1360,11 +1375,12 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
     double* __restrict__ y, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
    extern __shared__ __align__(16) char smem_raw[];
-   xsd += blockIdx.y * bs.panels;  // right-hand side blockIdx.y of a batch
-   x += blockIdx.y * bs.n;
-   y += blockIdx.y * bs.n;
+   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
+   xsd += rhs * bs.panels;
+   x += rhs * bs.n;
+   y += rhs * bs.n;
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   const int leaf = blockIdx.x * (blockDim.x >> 5) + warp;
+   const int leaf = unit * (blockDim.x >> 5) + warp;
    if (leaf >= n_leaf) return;
    const LeafDesc L = leaves[leaf];
    T2* xl = reinterpret_cast<T2*>(smem_raw) + (size_t)warp * xl_stride;
@@ -1560,7 +1576,7 @@ bool DeviceOperator<T>::warp_path(const LaunchGroup& g) const {
 template <typename T>
 void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream) {
    if (warp_path(g)) {
-      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes, b.nrhs);
+      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes * b.nrhs);
       const SrcDesc* c = src_.get() + g.begin;
       if (g.n == 3)
          far_forward_warp_kernel<T, 3><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd,
@@ -1573,7 +1589,7 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
                                                                          vt_.get(), pv_.get(), b.spectra, b.bs);
    } else {
       const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_forward_kernel<T><<<dim3(g.count, b.nrhs), far_threads(g.n), smem, stream>>>(
+      far_forward_kernel<T><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
           src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
    }
    FFTSVD_CHECK_LAUNCH();
@@ -1603,7 +1619,7 @@ void DeviceOperator<T>::launch_translate(const TileGroup& g, const Bufs& b, cuda
 template <typename T>
 void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream) {
    if (warp_path(g)) {
-      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes, b.nrhs);
+      const dim3 grid((g.count + kWarpCubes - 1) / kWarpCubes * b.nrhs);
       const DstDesc* c = dst_.get() + g.begin;
       if (g.n == 3)
          far_backward_warp_kernel<T, 3><<<grid, kWarpThreads, 0, stream>>>(
@@ -1616,7 +1632,7 @@ void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cud
              c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
    } else {
       const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_backward_kernel<T><<<dim3(g.count, b.nrhs), far_threads(g.n), smem, stream>>>(
+      far_backward_kernel<T><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
           dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
    }
    FFTSVD_CHECK_LAUNCH();
@@ -1668,6 +1684,7 @@ void DeviceOperator<T>::apply_batch(const double* x, double* y, int nrhs, cudaSt
    b.bs.spectra = spectra_elems_;
    b.bs.translated = translated_elems_;
    b.bs.staging = (int64_t)stage_levels_ * total_points_;
+   b.bs.nrhs = nrhs;
    apply_bufs(x, y, b, stream);
 }
 
@@ -1729,7 +1746,7 @@ void DeviceOperator<T>::apply_bufs(const double* x, double* y, const Bufs& b, cu
 template <typename T>
 void DeviceOperator<T>::launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream) {
    if (n_leaf_ == 0) return;
-   near_kernel<T><<<dim3((n_leaf_ + near_warps_ - 1) / near_warps_, b.nrhs), 32 * near_warps_, leaf_smem_max_,
+   near_kernel<T><<<(n_leaf_ + near_warps_ - 1) / near_warps_ * b.nrhs, 32 * near_warps_, leaf_smem_max_,
                     stream>>>(leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), b.xsd,
                               point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(),
                               join_phi_scale_.get(), x, y, b.bs);

@@ -90,9 +90,14 @@ struct LaunchGroup {
 };
 
 // Per-right-hand-side strides of the planar batch buffers: right-hand side r of a
-// batched launch (blockIdx.y, or group blockIdx.z of kBatchGroup in the
-// translation) reads and writes base + r * stride.  All zero for a single vector.
+// batched launch reads and writes base + r * stride.  Per-cube and per-leaf
+// kernels take r = blockIdx.x % nrhs and their unit blockIdx.x / nrhs, so the
+// blocks of one cube for all right-hand sides run together and its operator
+// data is fetched from DRAM once; the join and far-field add take r = blockIdx.y
+// and the translation group blockIdx.z of kBatchGroup.  Strides zero and nrhs 1
+// for a single vector.
 struct BatchStrides {
+   int nrhs = 1;
    int64_t n = 0;           // x, y (FP64 unknowns)
    int64_t panels = 0;      // joined panel values
    int64_t spectra = 0;     // source spectra (complex)
