@@ -30,6 +30,121 @@ namespace fftsvd {
 static int pad2(int v) { return (v + 1) & ~1; }
 static int pad16(int v) { return (v + 15) & ~15; }
 
+void TileProblem::add_output(int k, uint64_t code, int64_t tb, int pgp, int64_t out) {
+   key.push_back(k);
+   morton.push_back(code);
+   t_base.push_back(tb);
+   pg.push_back(pgp);
+   out_off.push_back(out);
+   ptr.push_back(ptr.back());
+}
+
+void TileProblem::add_pair(int64_t in, int s) {
+   in_off.push_back(in);
+   slot.push_back(s);
+   ptr.back()++;
+}
+
+// Greedy tiling: outputs of one key in Morton order, while the destinations, halo inputs and
+// padded interactions fit the kernel limits; tiles grouped by frequency count.
+static void build_tiles(const TileProblem& P, TileSet& S) {
+   std::map<int, std::vector<int>> by_key;
+   for (int i = 0; i < (int)P.key.size(); i++)
+      if (P.ptr[i + 1] > P.ptr[i]) by_key[P.key[i]].push_back(i);
+   for (auto& kv : by_key) {
+      std::vector<int>& ids = kv.second;
+      std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return P.morton[a] < P.morton[b]; });
+      size_t pos = 0;
+      while (pos < ids.size()) {
+         TileDesc tile;
+         tile.ndst = tile.nsrc = tile.npairs = 0;
+         tile.pg = P.pg[ids[pos]];
+         tile.t_off = P.t_base[ids[pos]];
+         tile.dst_off = (int64_t)S.tile_dst.size();
+         tile.src_off = (int64_t)S.tile_src.size();
+         tile.pair_off = (int64_t)S.tile_pairs.size();
+         std::map<int64_t, int> halo;
+         while (pos < ids.size()) {
+            const int o = ids[pos];
+            const int cnt = (int)(P.ptr[o + 1] - P.ptr[o]);
+            int fresh = 0;
+            for (int64_t q = P.ptr[o]; q < P.ptr[o + 1]; q++)
+               if (!halo.count(P.in_off[q])) fresh++;
+            // each destination's list is padded to whole groups of four with the zero slot
+            const int padded = (cnt + 3) & ~3;
+            if (tile.ndst > 0 && (tile.ndst + 1 > kTileMaxDst || tile.nsrc + fresh > kTileMaxSrc ||
+                                  tile.npairs + padded > kTileMaxPairs))
+               break;
+            FFTSVD_REQUIRE(padded <= kTileMaxPairs && fresh <= kTileMaxSrc, "interaction list too long");
+            S.tile_dst.push_back(P.out_off[o]);
+            S.tile_dst_pairs.push_back(make_int2(tile.npairs, padded));
+            for (int64_t q = P.ptr[o]; q < P.ptr[o + 1]; q++) {
+               auto it = halo.find(P.in_off[q]);
+               int h;
+               if (it == halo.end()) {
+                  h = tile.nsrc++;
+                  halo[P.in_off[q]] = h;
+                  S.tile_src.push_back(P.in_off[q]);
+               } else {
+                  h = it->second;
+               }
+               S.tile_pairs.push_back(((uint32_t)h << 16) | (uint32_t)P.slot[q]);
+            }
+            for (int q = cnt; q < padded; q++) S.tile_pairs.push_back((uint32_t)kTileZeroSlot);
+            tile.npairs += padded;
+            tile.ndst++;
+            pos++;
+         }
+         S.tiles.push_back(tile);
+      }
+   }
+   std::stable_sort(S.tiles.begin(), S.tiles.end(), [](const TileDesc& a, const TileDesc& b) { return a.pg > b.pg; });
+   for (int i = 0; i < (int)S.tiles.size(); i++) {
+      const TileDesc& t = S.tiles[i];
+      if (S.tile_groups.empty() || S.tile_groups.back().pg != t.pg) {
+         TileGroup g;
+         g.pg = t.pg;
+         g.begin = i;
+         S.tile_groups.push_back(g);
+      }
+      TileGroup& g = S.tile_groups.back();
+      g.count++;
+      g.max_src = std::max(g.max_src, t.nsrc);
+      g.max_pairs = std::max(g.max_pairs, t.npairs);
+      g.max_dst = std::max(g.max_dst, t.ndst);
+   }
+}
+
+// Every index the translation kernel forms stays inside its buffers: table rows, the
+// in_elems input spectra and the out_elems output spectra.
+static void check_tiles(const TileSet& S, int64_t nt, int64_t in_elems, int64_t out_elems) {
+   for (const TileDesc& t : S.tiles) {
+      FFTSVD_REQUIRE(t.ndst > 0 && t.ndst <= kTileMaxDst && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
+                         t.npairs > 0 && t.npairs <= kTileMaxPairs && t.pg > 0,
+                     "tile descriptor");
+      FFTSVD_REQUIRE(t.dst_off + t.ndst <= (int64_t)S.tile_dst.size(), "tile destinations out of range");
+      FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)S.tile_src.size(), "tile sources out of range");
+      FFTSVD_REQUIRE(t.pair_off + t.npairs <= (int64_t)S.tile_pairs.size(), "tile pairs out of range");
+      FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
+      FFTSVD_REQUIRE(t.pair_off % 4 == 0, "tile pairs not aligned");
+      for (int i = 0; i < t.ndst; i++) {
+         const int2 dp = S.tile_dst_pairs[t.dst_off + i];
+         FFTSVD_REQUIRE(dp.x >= 0 && dp.y >= 0 && dp.x + dp.y <= t.npairs && dp.x % 4 == 0 && dp.y % 4 == 0,
+                        "tile destination pairs out of range");
+         const int64_t so = S.tile_dst[t.dst_off + i];
+         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= out_elems, "tile destination spectrum out of range");
+      }
+      for (int i = 0; i < t.nsrc; i++) {
+         const int64_t so = S.tile_src[t.src_off + i];
+         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= in_elems, "tile source spectrum out of range");
+      }
+      for (int i = 0; i < t.npairs; i++) {
+         const uint32_t pr = S.tile_pairs[t.pair_off + i];
+         FFTSVD_REQUIRE((int)(pr >> 16) < t.nsrc && (pr & 0xffffu) <= (uint32_t)kTileZeroSlot, "tile pair out of range");
+      }
+   }
+}
+
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
                             const fftsvd_region_map* maps) {
    OperatorLayout L;
@@ -69,6 +184,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       int pg;
    };
    std::vector<DstExtra> dst_extra;  // parallel to L.dst until the tiles are built
+   std::vector<DstExtra> src_extra;  // parallel to L.src
 
    for (int t = 0; t < num_trees; t++) {
       const fftsvd_tree_flat& T = trees[t];
@@ -198,7 +314,16 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          const int H = n;
          int need = 2 * ch + 2 * r + n3 + 2 * Np + 2 * (n * n * H) + 2 * (n * Np * H) + 16;
          L.max_src_smem_elems = std::max(L.max_src_smem_elems, need);
+         s.level = lvl;
+         s.pad = 0;
          L.src.push_back(s);
+         {
+            const int32_t* ci = &T.cube_index[3 * c];
+            uint64_t code = 0;  // Morton order of the cube coordinates
+            for (int b = 0; b < 21; b++)
+               for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> b) & 1) << (3 * b + k);
+            src_extra.push_back({t * 64 + lvl, code, tlev[lvl], pad16(pg)});
+         }
       }
       for (int c = 0; c < T.num_cubes; c++) {
          const int lvl = T.cube_level[c];
@@ -281,75 +406,37 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       if (!row_written[o]) L.full_cover = false;
 
    // ---- translation tiles: destinations of one tree and level in Morton order, greedily
-   // grouped while the tile's destinations, halo sources and interactions fit the limits
+   // grouped while the tile's destinations, halo sources and interactions fit the limits.
+   // The transposed operator translates the other way: every source cube gathers from the
+   // destinations whose lists hold it, through the table slot of the opposite offset
+   // (the grid-to-grid kernel of a symmetric Green's function satisfies G_DS^T = G_SD).
    {
-      std::map<int, std::vector<int>> by_key;
-      for (int i = 0; i < (int)L.dst.size(); i++) by_key[dst_extra[i].key].push_back(i);
-      for (auto& kv : by_key) {
-         std::vector<int>& ids = kv.second;
-         std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return dst_extra[a].morton < dst_extra[b].morton; });
-         size_t pos = 0;
-         while (pos < ids.size()) {
-            TileDesc tile;
-            tile.ndst = tile.nsrc = tile.npairs = 0;
-            tile.pg = dst_extra[ids[pos]].pg;
-            tile.t_off = dst_extra[ids[pos]].t_base;
-            tile.dst_off = (int64_t)L.tile_dst.size();
-            tile.src_off = (int64_t)L.tile_src.size();
-            tile.pair_off = (int64_t)L.tile_pairs.size();
-            std::map<int64_t, int> halo;
-            while (pos < ids.size()) {
-               const DstDesc& d = L.dst[ids[pos]];
-               int fresh = 0;
-               for (int q = 0; q < d.inter_cnt; q++)
-                  if (!halo.count(L.inter_pairs[2 * (d.inter_off + q)])) fresh++;
-               // each destination's list is padded to whole groups of four with the zero slot
-               const int padded = (d.inter_cnt + 3) & ~3;
-               if (tile.ndst > 0 && (tile.ndst + 1 > kTileMaxDst || tile.nsrc + fresh > kTileMaxSrc ||
-                                     tile.npairs + padded > kTileMaxPairs))
-                  break;
-               FFTSVD_REQUIRE(padded <= kTileMaxPairs && fresh <= kTileMaxSrc, "interaction list too long");
-               L.tile_dst.push_back(d.s_off);
-               L.tile_dst_pairs.push_back(make_int2(tile.npairs, padded));
-               for (int q = 0; q < d.inter_cnt; q++) {
-                  const int64_t so = L.inter_pairs[2 * (d.inter_off + q)];
-                  const int64_t to = L.inter_pairs[2 * (d.inter_off + q) + 1];
-                  auto it = halo.find(so);
-                  int h;
-                  if (it == halo.end()) {
-                     h = tile.nsrc++;
-                     halo[so] = h;
-                     L.tile_src.push_back(so);
-                  } else {
-                     h = it->second;
-                  }
-                  const int64_t slot = (to - tile.t_off) / tile.pg;
-                  FFTSVD_REQUIRE(slot >= 0 && slot < 343 && (to - tile.t_off) % tile.pg == 0, "translation slot");
-                  L.tile_pairs.push_back(((uint32_t)h << 16) | (uint32_t)slot);
-               }
-               for (int q = d.inter_cnt; q < padded; q++) L.tile_pairs.push_back((uint32_t)kTileZeroSlot);
-               tile.npairs += padded;
-               tile.ndst++;
-               pos++;
-            }
-            L.tiles.push_back(tile);
+      TileProblem fwd, adj;
+      std::map<int64_t, int> src_of_spec;
+      for (int i = 0; i < (int)L.src.size(); i++) src_of_spec[L.src[i].spec_off] = i;
+      std::vector<std::vector<std::pair<int64_t, int>>> adj_lists(L.src.size());
+      for (int i = 0; i < (int)L.dst.size(); i++) {
+         const DstDesc& d = L.dst[i];
+         const DstExtra& e = dst_extra[i];
+         fwd.add_output(e.key, e.morton, e.t_base, e.pg, d.s_off);
+         for (int q = 0; q < d.inter_cnt; q++) {
+            const int64_t so = L.inter_pairs[2 * (d.inter_off + q)];
+            const int64_t to = L.inter_pairs[2 * (d.inter_off + q) + 1];
+            const int64_t slot = (to - e.t_base) / e.pg;
+            FFTSVD_REQUIRE(slot >= 0 && slot < 343 && (to - e.t_base) % e.pg == 0, "translation slot");
+            fwd.add_pair(so, (int)slot);
+            auto it = src_of_spec.find(so);
+            FFTSVD_REQUIRE(it != src_of_spec.end(), "interaction with an unknown source spectrum");
+            adj_lists[it->second].push_back({d.s_off, 342 - (int)slot});
          }
       }
-      std::stable_sort(L.tiles.begin(), L.tiles.end(), [](const TileDesc& a, const TileDesc& b) { return a.pg > b.pg; });
-      for (int i = 0; i < (int)L.tiles.size(); i++) {
-         const TileDesc& t = L.tiles[i];
-         if (L.tile_groups.empty() || L.tile_groups.back().pg != t.pg) {
-            TileGroup g;
-            g.pg = t.pg;
-            g.begin = i;
-            L.tile_groups.push_back(g);
-         }
-         TileGroup& g = L.tile_groups.back();
-         g.count++;
-         g.max_src = std::max(g.max_src, t.nsrc);
-         g.max_pairs = std::max(g.max_pairs, t.npairs);
-         g.max_dst = std::max(g.max_dst, t.ndst);
+      for (int i = 0; i < (int)L.src.size(); i++) {
+         const DstExtra& e = src_extra[i];
+         adj.add_output(e.key, e.morton, e.t_base, e.pg, L.src[i].spec_off);
+         for (const auto& pr : adj_lists[i]) adj.add_pair(pr.first, pr.second);
       }
+      build_tiles(fwd, L.fwd);
+      build_tiles(adj, L.adj);
    }
 
    // every index a kernel will form stays inside its buffer
@@ -389,31 +476,8 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       const int64_t pg = (int64_t)(2 * d.n - 1) * (2 * d.n - 1) * d.n;
       FFTSVD_REQUIRE(d.s_off >= 0 && d.s_off + pg <= L.translated_elems, "translated spectrum out of range");
    }
-   for (const TileDesc& t : L.tiles) {
-      FFTSVD_REQUIRE(t.ndst > 0 && t.ndst <= kTileMaxDst && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
-                         t.npairs > 0 && t.npairs <= kTileMaxPairs && t.pg > 0,
-                     "tile descriptor");
-      FFTSVD_REQUIRE(t.dst_off + t.ndst <= (int64_t)L.tile_dst.size(), "tile destinations out of range");
-      FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)L.tile_src.size(), "tile sources out of range");
-      FFTSVD_REQUIRE(t.pair_off + t.npairs <= (int64_t)L.tile_pairs.size(), "tile pairs out of range");
-      FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
-      FFTSVD_REQUIRE(t.pair_off % 4 == 0, "tile pairs not aligned");
-      for (int i = 0; i < t.ndst; i++) {
-         const int2 dp = L.tile_dst_pairs[t.dst_off + i];
-         FFTSVD_REQUIRE(dp.x >= 0 && dp.y >= 0 && dp.x + dp.y <= t.npairs && dp.x % 4 == 0 && dp.y % 4 == 0,
-                        "tile destination pairs out of range");
-         const int64_t so = L.tile_dst[t.dst_off + i];
-         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= L.translated_elems, "tile destination spectrum out of range");
-      }
-      for (int i = 0; i < t.nsrc; i++) {
-         const int64_t so = L.tile_src[t.src_off + i];
-         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= L.spectra_elems, "tile source spectrum out of range");
-      }
-      for (int i = 0; i < t.npairs; i++) {
-         const uint32_t pr = L.tile_pairs[t.pair_off + i];
-         FFTSVD_REQUIRE((int)(pr >> 16) < t.nsrc && (pr & 0xffffu) <= (uint32_t)kTileZeroSlot, "tile pair out of range");
-      }
-   }
+   check_tiles(L.fwd, nt, L.spectra_elems, L.translated_elems);  // spectra -> translated
+   check_tiles(L.adj, nt, L.translated_elems, L.spectra_elems);  // transposed: translated -> spectra
    for (int64_t k = 0; k < (int64_t)L.point_out.size(); k++) {
       FFTSVD_REQUIRE(L.point_out[k] >= 0 && L.point_out[k] < num_unknowns, "point without an output row");
       FFTSVD_REQUIRE(L.point_panel[k] >= -1 && L.point_panel[k] < L.total_panels - 1, "jump panel index");
@@ -443,7 +507,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       kb.fixed[1] = 4.0 * (double)L.src_panels.size();
       const double sbuf = 2.0 * (double)L.translated_elems;
       kb.elems[2] = spec + (double)L.t_elems + sbuf;                      // spectra, T, translated writes
-      kb.fixed[2] = 4.0 * (double)L.tile_pairs.size() + 8.0 * (double)(L.tile_src.size() + L.tile_dst.size());
+      kb.fixed[2] = 4.0 * (double)L.fwd.tile_pairs.size() + 8.0 * (double)(L.fwd.tile_src.size() + L.fwd.tile_dst.size());
       kb.elems[3] = sbuf + uti + u + nq;                                  // translated, UTI, U, staging writes
       kb.fixed[3] = 4.0 * (double)L.dst_points.size();
       kb.elems[4] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
@@ -901,6 +965,239 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
    }
 }
 
+constexpr int kWarpCubes = 4;  // cubes (warps) per block
+constexpr int kWarpThreads = 32 * kWarpCubes;
+
+// ---- transposed operator (y = A^T x), for the adjoint solve
+//
+// A = sum over trees of Out^T (S Gs + D Gd + J Gd), with Gs/Gd the scaled gathers of the
+// join, S/D the single/double-layer operators (near blocks plus far field) and J the
+// jump.  A^T x: gather z = x[out(p)] per tree point, form S^T z and D^T z per tree panel,
+// then scatter-add them scaled to the rows the join read.  The far field runs the
+// forward pipeline backwards: per destination cube U^T, UTI^T and the forward DFT; the
+// translation with the opposite-offset slots (transposed tiles); per source cube the
+// inverse DFT, PV_s^T / PV_d^T and VT^T into one staging row per level.  Blocks of one
+// cube per block; the DFTs are those of the forward kernels.
+
+// zt[p] = x[out(p)] for every tree point
+template <typename T>
+__global__ void gather_points_kernel(int64_t total, const int32_t* __restrict__ point_out, const double* __restrict__ x,
+                                     T* __restrict__ zt) {
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x)
+      zt[k] = (T)x[point_out[k]];
+}
+
+// per destination cube: a = U^T z (U is p x r), g = UTI^T a on the n^3 grid, F = r2c DFT of
+// g at offset n/2, written to the cube's translated-spectrum slot
+template <typename T>
+__global__ void __launch_bounds__(kFarThreads) far_backward_t_kernel(
+    const DstDesc* __restrict__ cubes, const int32_t* __restrict__ dst_points, const T* __restrict__ zt,
+    const T* __restrict__ uti, const T* __restrict__ ucm, typename Vec2<T>::type* __restrict__ out_spectra) {
+   using T2 = typename Vec2<T>::type;
+   extern __shared__ __align__(16) char smem_raw[];
+   const DstDesc c = cubes[blockIdx.x];
+   const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n;
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+   char* p = smem_raw;
+   T* a = carve<T>(p, c.r);
+   T* g = carve<T>(p, n3);
+   T2* tw = carve<T2>(p, Np);
+   T2* A = carve<T2>(p, n * n * H);
+   T2* B = carve<T2>(p, n * Np * H);
+   for (int k = tid; k < Np; k += blockDim.x) {  // exp(-2 pi i k / Np)
+      T cs, sn;
+      Cx<T>::cis(k, Np, &cs, &sn);
+      tw[k] = Cx<T>::make(cs, -sn);
+   }
+   // a_j = sum_q U[q][j] z[q]; U stored r x p (row j contiguous over the points)
+   for (int j = warp; j < c.r; j += nwarps) {
+      const T* row = ucm + c.u_off + (int64_t)j * c.p;
+      T s = T(0);
+      for (int q = lane; q < c.p; q += 32) s += row[q] * zt[dst_points[c.point_off + q]];
+      s = warp_sum(s);
+      if (lane == 0) a[j] = s;
+   }
+   __syncthreads();
+   for (int x = tid; x < n3; x += blockDim.x) {
+      T s = T(0);
+      for (int j = 0; j < c.r; j++) s += uti[c.uti_off + (int64_t)j * n3 + x] * a[j];
+      g[x] = s;
+   }
+   __syncthreads();
+   for (int idx = tid; idx < n * n * H; idx += blockDim.x) {
+      const int kf = idx % H, ij = idx / H;
+      const T* line = g + ij * n;
+      T2 acc = Cx<T>::make(T(0), T(0));
+      for (int k = 0; k < n; k++) {
+         T2 w = tw[((k + off) * kf) % Np];
+         acc.x += line[k] * w.x;
+         acc.y += line[k] * w.y;
+      }
+      A[idx] = acc;
+   }
+   __syncthreads();
+   for (int idx = tid; idx < n * Np * H; idx += blockDim.x) {
+      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+      T2 acc = Cx<T>::make(T(0), T(0));
+      for (int j = 0; j < n; j++) acc = Cx<T>::fma(A[(i * n + j) * H + kf], tw[((j + off) * jf) % Np], acc);
+      B[idx] = acc;
+   }
+   __syncthreads();
+   T2* out = out_spectra + c.s_off;
+   for (int idx = tid; idx < Np * Np * H; idx += blockDim.x) {
+      const int kf = idx % H, jf = (idx / H) % Np, fi = idx / (H * Np);
+      T2 acc = Cx<T>::make(T(0), T(0));
+      for (int i = 0; i < n; i++) acc = Cx<T>::fma(B[(i * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
+      out[idx] = acc;
+   }
+}
+
+// per source cube: g = c2r DFT of the translated spectrum (cropped at n/2, scaled),
+// a_s = PV_s^T g, a_d = PV_d^T g, and per panel {VT^T a_s, VT^T a_d} into the level's
+// staging row (each panel belongs to one source cube per level)
+template <typename T>
+__global__ void __launch_bounds__(kFarThreads) far_forward_t_kernel(
+    const SrcDesc* __restrict__ cubes, const int32_t* __restrict__ src_panels,
+    const typename Vec2<T>::type* __restrict__ in_spectra, const T* __restrict__ vt,
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ staging,
+    int64_t total_panels) {
+   using T2 = typename Vec2<T>::type;
+   extern __shared__ __align__(16) char smem_raw[];
+   const SrcDesc c = cubes[blockIdx.x];
+   const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n, pg = Np * Np * H;
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+   char* p = smem_raw;
+   T2* S = carve<T2>(p, pg);
+   T2* P1 = carve<T2>(p, n * Np * H);
+   T2* P2 = carve<T2>(p, n * n * H);
+   T* g = carve<T>(p, n3);
+   T2* a = carve<T2>(p, c.r);
+   T2* tw = carve<T2>(p, Np);
+   for (int k = tid; k < Np; k += blockDim.x) {  // exp(+2 pi i k / Np)
+      T cs, sn;
+      Cx<T>::cis(k, Np, &cs, &sn);
+      tw[k] = Cx<T>::make(cs, sn);
+   }
+   for (int f = tid; f < pg; f += blockDim.x) S[f] = in_spectra[c.spec_off + f];
+   __syncthreads();
+   for (int idx = tid; idx < n * Np * H; idx += blockDim.x) {
+      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+      T2 acc = Cx<T>::make(T(0), T(0));
+      for (int fi = 0; fi < Np; fi++) acc = Cx<T>::fma(S[(fi * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
+      P1[idx] = acc;
+   }
+   __syncthreads();
+   for (int idx = tid; idx < n * n * H; idx += blockDim.x) {
+      const int kf = idx % H, j = (idx / H) % n, i = idx / (H * n);
+      T2 acc = Cx<T>::make(T(0), T(0));
+      for (int jf = 0; jf < Np; jf++) acc = Cx<T>::fma(P1[(i * Np + jf) * H + kf], tw[((j + off) * jf) % Np], acc);
+      P2[idx] = acc;
+   }
+   __syncthreads();
+   const T scale = T(1) / (T)(Np * Np * Np);
+   for (int q = tid; q < n3; q += blockDim.x) {
+      const int k = q % n, ij = q / n;
+      const T2* line = P2 + ij * H;
+      T acc = line[0].x;
+      for (int kf = 1; kf < H; kf++) {
+         T2 w = tw[((k + off) * kf) % Np];
+         acc += T(2) * (line[kf].x * w.x - line[kf].y * w.y);
+      }
+      g[q] = acc * scale;
+   }
+   __syncthreads();
+   // a_j = {sum_x PV_s[j][x] g[x], sum_x PV_d[j][x] g[x]}; pv stored r x n^3 of pairs
+   for (int j = warp; j < c.r; j += nwarps) {
+      const T2* row = pv + c.pv_off + (int64_t)j * n3;
+      T s = T(0), d = T(0);
+      for (int x = lane; x < n3; x += 32) {
+         const T2 w = row[x];
+         s += w.x * g[x];
+         d += w.y * g[x];
+      }
+      s = warp_sum(s);
+      d = warp_sum(d);
+      if (lane == 0) a[j] = Cx<T>::make(s, d);
+   }
+   __syncthreads();
+   T2* stage = staging + (int64_t)c.level * total_panels;
+   for (int i = tid; i < c.m; i += blockDim.x) {
+      T s = T(0), d = T(0);
+      for (int j = 0; j < c.r; j++) {
+         const T v = vt[c.vt_off + (int64_t)j * c.m + i];
+         s += v * a[j].x;
+         d += v * a[j].y;
+      }
+      stage[src_panels[c.panel_off + i]] = Cx<T>::make(s, d);
+   }
+}
+
+// dynamic shared memory of the transposed far-field kernels (their carve order, 16-byte aligned)
+template <typename T>
+static int far_backward_t_smem(int n, int r) {
+   const int Np = 2 * n - 1, H = n, T2s = 2 * (int)sizeof(T);
+   return 16 * 6 + r * (int)sizeof(T) + n * n * n * (int)sizeof(T) + Np * T2s + n * n * H * T2s + n * Np * H * T2s;
+}
+template <typename T>
+static int far_forward_t_smem(int n, int r) {
+   const int Np = 2 * n - 1, H = n, T2s = 2 * (int)sizeof(T);
+   return 16 * 7 + Np * Np * H * T2s + n * Np * H * T2s + n * n * H * T2s + n * n * n * (int)sizeof(T) + r * T2s +
+          Np * T2s;
+}
+
+// per leaf (one warp): column sums of the near-field blocks against the leaf's gathered
+// rows, {sum_r Ds[r][c] z[r], sum_r Dd[r][c] z[r]}, added to the column's panel
+template <typename T>
+__global__ void __launch_bounds__(kWarpThreads) near_t_kernel(const LeafDesc* __restrict__ leaves, int n_leaf,
+                                                              const int32_t* __restrict__ rows,
+                                                              const int32_t* __restrict__ cols,
+                                                              const typename Vec2<T>::type* __restrict__ d,
+                                                              const T* __restrict__ zt, double2* __restrict__ ut,
+                                                              int32_t zero_slot) {
+   using T2 = typename Vec2<T>::type;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int leaf = blockIdx.x * kWarpCubes + warp;
+   if (leaf >= n_leaf) return;
+   const LeafDesc L = leaves[leaf];
+   for (int c = lane; c < L.ncols; c += 32) {
+      const int k = cols[L.col_off + c];
+      if (k == zero_slot) continue;  // padding column
+      double s = 0.0, dd = 0.0;
+      for (int r = 0; r < L.nrows; r++) {
+         const T2 v = d[L.d_off + (int64_t)r * L.ncols + c];
+         const double z = (double)zt[rows[L.row_off + r]];
+         s += (double)v.x * z;
+         dd += (double)v.y * z;
+      }
+      atomicAdd(&ut[k].x, s);
+      atomicAdd(&ut[k].y, dd);
+   }
+}
+
+// per tree panel k: single-layer and double-layer sums (near, far levels, jump), added
+// scaled to the rows its join read: y[dphi(k)] += dphi_scale s, y[phi(k)] += phi_scale d
+template <typename T>
+__global__ void scatter_panels_kernel(int64_t np, const double2* __restrict__ ut,
+                                      const typename Vec2<T>::type* __restrict__ staging, int levels,
+                                      int64_t total_panels, const double* __restrict__ panel_jump,
+                                      const int32_t* __restrict__ panel_point, const T* __restrict__ zt,
+                                      const int32_t* __restrict__ phi_idx, const double* __restrict__ phi_scale,
+                                      const int32_t* __restrict__ dphi_idx, const double* __restrict__ dphi_scale,
+                                      double* __restrict__ y) {
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < np; k += (int64_t)gridDim.x * blockDim.x) {
+      double s = ut[k].x, d = ut[k].y;
+      for (int l = 0; l < levels; l++) {
+         const auto v = staging[(int64_t)l * total_panels + k];
+         s += (double)v.x;
+         d += (double)v.y;
+      }
+      const int q = panel_point[k];
+      if (q >= 0) d += panel_jump[k] * (double)zt[q];
+      atomicAdd(&y[dphi_idx[k]], dphi_scale[k] * s);
+      atomicAdd(&y[phi_idx[k]], phi_scale[k] * d);
+   }
+}
+
 // ---- one warp per cube for the small grids of the fine levels
 //
 // Most cubes sit on the finest levels, where the grid is 4^3 and a cube holds a
@@ -909,8 +1206,6 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
 // replace barriers by __syncwarp, and fix the grid edge at compile time.  The
 // arithmetic is the block kernels' (same DFT factorisation and twiddles).
 
-constexpr int kWarpCubes = 4;  // cubes (warps) per block
-constexpr int kWarpThreads = 32 * kWarpCubes;
 
 template <int N>
 struct SmallGrid {
@@ -1489,12 +1784,26 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    upload_cast<T>(uti_, L.uti);
    upload_cast<T>(u_, L.u_cm);
    upload_pairs<T>(t_, L.t_pairs);
-   tiles_.upload(L.tiles);
-   tile_src_.upload(L.tile_src);
-   tile_dst_.upload(L.tile_dst);
-   tile_dst_pairs_.upload(L.tile_dst_pairs);
-   tile_pairs_.upload(L.tile_pairs);
-   tile_groups_ = L.tile_groups;
+   fwd_.upload(L.fwd);
+   adj_.upload(L.adj);
+   // transposed operator: gathered points, per-panel sums, per-level far-field rows, and
+   // for each panel the point whose jump term it takes (a point and its panel share an index)
+   zt_.alloc(std::max<int64_t>(L.total_points, 1));
+   ut_.alloc(L.total_panels);
+   staget_.alloc(std::max<int64_t>((int64_t)L.stage_levels * L.total_panels, 1));
+   staget_.zero();  // rows no source cube of a level writes stay zero
+   {
+      std::vector<double> pj(L.total_panels, 0.0);
+      std::vector<int32_t> pp(L.total_panels, -1);
+      for (int64_t q = 0; q < L.total_points; q++)
+         if (L.point_panel[q] >= 0) {
+            FFTSVD_REQUIRE(pp[L.point_panel[q]] < 0, "two jump points on one panel");
+            pp[L.point_panel[q]] = (int32_t)q;
+            pj[L.point_panel[q]] = L.point_jump[q];
+         }
+      panel_jump_.upload(pj);
+      panel_point_.upload(pp);
+   }
    translated_.alloc(std::max<int64_t>(L.translated_elems, 1));
    spectra_.alloc(std::max<int64_t>(L.spectra_elems, 1));
    spectra_.zero();      // row padding is read by the translation and must stay zero
@@ -1508,6 +1817,9 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    dst_smem_ = 0;
    for (const LaunchGroup& g : src_groups_) src_smem_ = std::max(src_smem_, (int)(g.smem_elems * sizeof(T) + 128));
    for (const LaunchGroup& g : dst_groups_) dst_smem_ = std::max(dst_smem_, (int)(g.smem_elems * sizeof(T) + 128));
+   src_smem_t_ = dst_smem_t_ = 0;
+   for (const SrcDesc& c : L.src) src_smem_t_ = std::max(src_smem_t_, far_forward_t_smem<T>(c.n, c.r));
+   for (const DstDesc& c : L.dst) dst_smem_t_ = std::max(dst_smem_t_, far_backward_t_smem<T>(c.n, c.r));
    int maxcols = 2;
    for (const auto& l : L.leaves) maxcols = std::max(maxcols, l.ncols);
    int dev = 0, optin = 0;
@@ -1518,11 +1830,13 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    near_warps_ = (int)std::max<size_t>(1, std::min<size_t>(kNearThreads / 32, (size_t)optin / (maxcols * sizeof(T2))));
    leaf_smem_max_ = (int)(near_warps_ * maxcols * sizeof(T2));
    int tile_smem = 0, tile_smem_b = 0;
-   for (const TileGroup& g : tile_groups_) {
+   for (const TileGroup& g : fwd_.groups) {
       tile_smem = std::max(tile_smem, translate_smem(g, false));
       tile_smem_b = std::max(tile_smem_b, translate_smem(g, true));
    }
-   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || tile_smem > optin)
+   for (const TileGroup& g : adj_.groups) tile_smem = std::max(tile_smem, translate_smem(g, false));
+   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || tile_smem > optin ||
+       src_smem_t_ > optin || dst_smem_t_ > optin)
       throw Error(FFTSVD_ERR_UNSUPPORTED, "operator block needs more shared memory than the device offers");
    if (tile_smem > 0) {
       FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
@@ -1538,6 +1852,10 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, src_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dst_smem_));
    FFTSVD_CUDA(cudaFuncSetAttribute(near_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, leaf_smem_max_));
+   FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_t_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    std::max(src_smem_t_, 1)));
+   FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_t_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    std::max(dst_smem_t_, 1)));
    build_chains();
    FFTSVD_CUDA(cudaDeviceSynchronize());
 }
@@ -1596,24 +1914,80 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
 }
 
 template <typename T>
-void DeviceOperator<T>::launch_translate(const TileGroup& g, const Bufs& b, cudaStream_t stream) {
+void DeviceOperator<T>::DevTiles::upload(const TileSet& S) {
+   tiles.upload(S.tiles);
+   src.upload(S.tile_src);
+   dst.upload(S.tile_dst);
+   dst_pairs.upload(S.tile_dst_pairs);
+   pairs.upload(S.tile_pairs);
+   groups = S.tile_groups;
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_translate_tiles(const DevTiles& tl, const TileGroup& g, const T2* in, T2* out,
+                                               int nrhs, const BatchStrides& bs, cudaStream_t stream) {
    // split each tile's frequency chunks over several blocks so that even the few
    // tiles of the coarse levels fill the device (about eight blocks per SM in total)
-   const bool batch = b.nrhs > 1;
-   const int groups = batch ? b.nrhs / kBatchGroup : 1;
+   const bool batch = nrhs > 1;
+   const int groups = batch ? nrhs / kBatchGroup : 1;
    const int nchunks = g.pg / (batch ? 16 / (int)sizeof(T2) : kTileRowBytes / (int)sizeof(T2));
    const int64_t total = (int64_t)g.count * nchunks * groups;
    const int cpb = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, total / (8 * 148)));
    const dim3 grid(g.count, (nchunks + cpb - 1) / cpb, groups);
    if (batch)
       translate_kernel<T, true><<<grid, kTranslateThreads, translate_smem(g, true), stream>>>(
-          tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(),
-          t_.get(), b.spectra, b.translated, cpb, b.bs);
+          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.dst_pairs.get(), tl.pairs.get(), t_.get(), in, out,
+          cpb, bs);
    else
       translate_kernel<T, false><<<grid, kTranslateThreads, translate_smem(g, false), stream>>>(
-          tiles_.get() + g.begin, tile_src_.get(), tile_dst_.get(), tile_dst_pairs_.get(), tile_pairs_.get(),
-          t_.get(), b.spectra, b.translated, cpb, b.bs);
+          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.dst_pairs.get(), tl.pairs.get(), t_.get(), in, out,
+          cpb, bs);
    FFTSVD_CHECK_LAUNCH();
+}
+
+template <typename T>
+void DeviceOperator<T>::launch_translate(const TileGroup& g, const Bufs& b, cudaStream_t stream) {
+   launch_translate_tiles(fwd_, g, b.spectra, b.translated, b.nrhs, b.bs, stream);
+}
+
+template <typename T>
+void DeviceOperator<T>::apply_transpose(const double* x, double* y, cudaStream_t stream) {
+   const int64_t np = total_panels_ - 1;  // the zero slot is no panel
+   FFTSVD_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * num_unknowns_, stream));
+   FFTSVD_CUDA(cudaMemsetAsync(ut_.get(), 0, sizeof(double2) * total_panels_, stream));
+   const int ew = (int)std::max<int64_t>(1, std::min<int64_t>((std::max(total_points_, np) + 255) / 256, 148 * 16));
+   if (total_points_ > 0) {
+      gather_points_kernel<T><<<ew, 256, 0, stream>>>(total_points_, point_out_.get(), x, zt_.get());
+      FFTSVD_CHECK_LAUNCH();
+   }
+   // far field, backwards: destinations -> translated slots -> (transposed tiles) -> source spectra
+   for (const LaunchGroup& g : dst_groups_) {
+      far_backward_t_kernel<T><<<g.count, far_threads(g.n), dst_smem_t_, stream>>>(
+          dst_.get() + g.begin, dst_points_.get(), zt_.get(), uti_.get(), u_.get(), translated_.get());
+      FFTSVD_CHECK_LAUNCH();
+   }
+   // sources that no destination reaches must read zero
+   FFTSVD_CUDA(cudaMemsetAsync(spectra_.get(), 0, sizeof(T2) * spectra_elems_, stream));
+   for (const TileGroup& g : adj_.groups)
+      launch_translate_tiles(adj_, g, translated_.get(), spectra_.get(), 1, BatchStrides(), stream);
+   for (const LaunchGroup& g : src_groups_) {
+      far_forward_t_kernel<T><<<g.count, far_threads(g.n), src_smem_t_, stream>>>(
+          src_.get() + g.begin, src_panels_.get(), spectra_.get(), vt_.get(), pv_.get(), staget_.get(),
+          total_panels_);
+      FFTSVD_CHECK_LAUNCH();
+   }
+   if (n_leaf_ > 0) {
+      near_t_kernel<T><<<(n_leaf_ + kWarpCubes - 1) / kWarpCubes, kWarpThreads, 0, stream>>>(
+          leaves_.get(), n_leaf_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), zt_.get(), ut_.get(), (int32_t)np);
+      FFTSVD_CHECK_LAUNCH();
+   }
+   if (np > 0) {
+      scatter_panels_kernel<T><<<ew, 256, 0, stream>>>(np, ut_.get(), staget_.get(), stage_levels_, total_panels_,
+                                                       panel_jump_.get(), panel_point_.get(), zt_.get(),
+                                                       join_phi_idx_.get(), join_phi_scale_.get(),
+                                                       join_dphi_idx_.get(), join_dphi_scale_.get(), y);
+      FFTSVD_CHECK_LAUNCH();
+   }
 }
 
 template <typename T>
@@ -1641,7 +2015,7 @@ void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cud
 template <typename T>
 void DeviceOperator<T>::launch_chain(const Chain& ch, const Bufs& b, cudaStream_t stream) {
    for (int i : ch.src) launch_forward(src_groups_[i], b, stream);
-   for (int i : ch.tile) launch_translate(tile_groups_[i], b, stream);
+   for (int i : ch.tile) launch_translate(fwd_.groups[i], b, stream);
    for (int i : ch.dst) launch_backward(dst_groups_[i], b, stream);
 }
 
@@ -1712,7 +2086,7 @@ void DeviceOperator<T>::apply_bufs(const double* x, double* y, const Bufs& b, cu
       FFTSVD_CUDA(cudaEventRecord(ev_[1], stream));
       for (const LaunchGroup& g : src_groups_) launch_forward(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[2], stream));
-      for (const TileGroup& g : tile_groups_) launch_translate(g, b, stream);
+      for (const TileGroup& g : fwd_.groups) launch_translate(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[3], stream));
       for (const LaunchGroup& g : dst_groups_) launch_backward(g, b, stream);
       FFTSVD_CUDA(cudaEventRecord(ev_[4], stream));
@@ -1762,8 +2136,8 @@ void DeviceOperator<T>::build_chains() {
    for (auto& kv : by_n) {
       const int n = kv.first, pgp = ((2 * n - 1) * (2 * n - 1) * n + 15) & ~15;
       kv.second.n = n;
-      for (int i = 0; i < (int)tile_groups_.size(); i++)
-         if (tile_groups_[i].pg == pgp) kv.second.tile.push_back(i);
+      for (int i = 0; i < (int)fwd_.groups.size(); i++)
+         if (fwd_.groups[i].pg == pgp) kv.second.tile.push_back(i);
       // destinations and their interactions: a measure of the chain's length
       for (int i : kv.second.dst) kv.second.work += (double)dst_groups_[i].count * pgp;
    }
@@ -1808,8 +2182,10 @@ size_t DeviceOperator<T>::device_bytes() const {
           xsd_.bytes() + point_out_.bytes() + point_panel_.bytes() + point_jump_.bytes() + leaves_.bytes() +
           leaf_rows_.bytes() + leaf_cols_.bytes() + d_.bytes() + src_.bytes() + src_panels_.bytes() +
           vt_.bytes() + pv_.bytes() + dst_.bytes() + dst_points_.bytes() + uti_.bytes() + u_.bytes() +
-          t_.bytes() + spectra_.bytes() + staging_.bytes() + tiles_.bytes() + tile_src_.bytes() +
-          tile_dst_.bytes() + tile_dst_pairs_.bytes() + tile_pairs_.bytes() + translated_.bytes();
+          t_.bytes() + spectra_.bytes() + staging_.bytes() + fwd_.tiles.bytes() + fwd_.src.bytes() +
+          fwd_.dst.bytes() + fwd_.dst_pairs.bytes() + fwd_.pairs.bytes() + translated_.bytes() + adj_.tiles.bytes() +
+          adj_.src.bytes() + adj_.dst.bytes() + adj_.dst_pairs.bytes() + adj_.pairs.bytes() + zt_.bytes() +
+          ut_.bytes() + staget_.bytes();
 }
 
 template class DeviceOperator<float>;

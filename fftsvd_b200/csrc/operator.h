@@ -28,6 +28,8 @@ struct SrcDesc {        // one far-field source cube (panels > 0, row rank > 0)
    int64_t vt_off;      // into vt, r x m row-major
    int64_t pv_off;      // into pv, r x n^3 of {PV_single, PV_double}
    int64_t spec_off;    // into spectra, (2n-1)^2 n complex
+   int32_t level;       // staging slot of the transposed operator
+   int32_t pad;
 };
 
 struct DstDesc {        // one far-field destination cube (points > 0, column rank > 0)
@@ -63,6 +65,31 @@ struct TileGroup {      // tiles with the same frequency count, one launch
    int pg = 0;
    int begin = 0, count = 0;
    int max_src = 0, max_pairs = 0, max_dst = 0;
+};
+
+// Tiles of one translation direction, as uploaded.
+struct TileSet {
+   std::vector<TileDesc> tiles;
+   std::vector<int64_t> tile_src, tile_dst;
+   std::vector<int2> tile_dst_pairs;   // {begin, count} relative to the tile's pair_off
+   std::vector<uint32_t> tile_pairs;
+   std::vector<TileGroup> tile_groups;
+};
+
+// One translation problem before tiling: each output (destination spectrum) with its tree
+// and level key, Morton code, slot-0 table offset, padded frequency count, and its
+// interactions (input spectrum offset, table slot) in in_off/slot[ptr[o] .. ptr[o+1]).
+struct TileProblem {
+   std::vector<int> key;
+   std::vector<uint64_t> morton;
+   std::vector<int64_t> t_base;
+   std::vector<int> pg;
+   std::vector<int64_t> out_off;
+   std::vector<int64_t> ptr{0};
+   std::vector<int64_t> in_off;
+   std::vector<int> slot;
+   void add_output(int key, uint64_t morton, int64_t t_base, int pg, int64_t out);
+   void add_pair(int64_t in, int slot);
 };
 
 constexpr int kTileMaxDst = 64;
@@ -155,12 +182,9 @@ struct OperatorLayout {
    int64_t translated_elems = 0;       // S buffer, complex elements
    int max_src_smem_elems = 0, max_dst_smem_elems = 0;
    std::vector<LaunchGroup> src_groups, dst_groups;
-   // translation tiles, grouped by frequency count (one launch per group)
-   std::vector<TileDesc> tiles;
-   std::vector<int64_t> tile_src, tile_dst;
-   std::vector<int2> tile_dst_pairs;   // {begin, count} relative to the tile's pair_off
-   std::vector<uint32_t> tile_pairs;
-   std::vector<TileGroup> tile_groups;
+   // translation tiles, grouped by frequency count (one launch per group): the operator's
+   // (spectra -> translated) and the transposed operator's (translated -> spectra)
+   TileSet fwd, adj;
    // algorithmic bytes per matvec at 4-byte or 8-byte element size (excluding vectors)
    int64_t operator_elems = 0;          // D pairs*2 + VT + PV*2 + UTI + U
    int64_t t_elems = 0;                 // unique translation operator reals
@@ -187,6 +211,9 @@ class DeviceOperator {
    void apply_batch(const double* x, double* y, int nrhs, cudaStream_t stream);
    // device bytes of the batch buffers per right-hand side
    size_t batch_bytes_per_rhs() const;
+   // y = A^T x (the transposed operator), x and y device vectors of num_unknowns doubles.
+   // Column sums are accumulated with FP64 atomics: not bitwise reproducible run to run.
+   void apply_transpose(const double* x, double* y, cudaStream_t stream);
    // per-stage events for timing (recorded when enabled)
    void enable_timing(bool on);
    // milliseconds of [join, far_forward, translate, far_backward, near] of the last timed apply
@@ -240,11 +267,25 @@ class DeviceOperator {
    int src_smem_ = 0, dst_smem_ = 0, leaf_smem_max_ = 0;
    int near_warps_ = 1, near_stride_ = 2;
    std::vector<LaunchGroup> src_groups_, dst_groups_;
-   std::vector<TileGroup> tile_groups_;
-   DevBuf<TileDesc> tiles_;
-   DevBuf<int64_t> tile_src_, tile_dst_;
-   DevBuf<int2> tile_dst_pairs_;
-   DevBuf<uint32_t> tile_pairs_;
+   // device copy of one direction's tiles
+   struct DevTiles {
+      DevBuf<TileDesc> tiles;
+      DevBuf<int64_t> src, dst;
+      DevBuf<int2> dst_pairs;
+      DevBuf<uint32_t> pairs;
+      std::vector<TileGroup> groups;
+      void upload(const TileSet& S);
+   };
+   DevTiles fwd_, adj_;
+   void launch_translate_tiles(const DevTiles& tl, const TileGroup& g, const T2* in, T2* out, int nrhs,
+                               const BatchStrides& bs, cudaStream_t stream);
+   // transposed operator: gathered input, per-panel near-field sums, per-level far-field rows
+   DevBuf<T> zt_;
+   DevBuf<double2> ut_;
+   DevBuf<typename Vec2<T>::type> staget_;
+   DevBuf<double> panel_jump_;
+   DevBuf<int32_t> panel_point_;
+   int src_smem_t_ = 0, dst_smem_t_ = 0;
    DevBuf<typename Vec2<T>::type> translated_;
    DevBuf<int32_t> join_phi_idx_, join_dphi_idx_;
    DevBuf<double> join_phi_scale_, join_dphi_scale_;

@@ -104,12 +104,21 @@ void Preconditioner::build(const fftsvd_precond_csc& P, int n) {
    blk_idx.upload(idx);
    inv_off.upload(off);
    this->inv.upload(inv);
+   // inverse of the transposed block = transpose of the inverse (adjoint solves)
+   std::vector<double> invt(inv.size());
+   for (int b = 0; b < nblocks; b++) {
+      const int k = ptr[b + 1] - ptr[b];
+      for (int i = 0; i < k; i++)
+         for (int j = 0; j < k; j++) invt[off[b] + (size_t)i * k + j] = inv[off[b] + (size_t)j * k + i];
+   }
+   this->inv_t.upload(invt);
 }
 
-void Preconditioner::apply(const double* r, double* z, cudaStream_t s) const {
+void Preconditioner::apply(const double* r, double* z, cudaStream_t s, bool transpose) const {
    const int threads = 256;
    const int blocks = std::max(1, std::min((nblocks + threads - 1) / threads, 148 * 8));
-   precond_kernel<<<blocks, threads, 0, s>>>(nblocks, blk_ptr.get(), blk_idx.get(), inv_off.get(), inv.get(), r, z, 0);
+   precond_kernel<<<blocks, threads, 0, s>>>(nblocks, blk_ptr.get(), blk_idx.get(), inv_off.get(),
+                                             transpose ? inv_t.get() : inv.get(), r, z, 0);
    FFTSVD_CHECK_LAUNCH();
 }
 
@@ -136,11 +145,19 @@ void Surface::ensure_capacity(int nvec) {
 }
 
 void Surface::apply(int precision, const double* x, double* yv) {
-   if (precision == FFTSVD_PREC_FP64)
+   if (transposed) {
+      if (precision == FFTSVD_PREC_FP64)
+         op64.apply_transpose(x, yv, stream);
+      else
+         op32.apply_transpose(x, yv, stream);
+   } else if (precision == FFTSVD_PREC_FP64) {
       op64.apply(x, yv, stream);
-   else
+   } else {
       op32.apply(x, yv, stream);
+   }
 }
+
+void Surface::pinv(const double* r_in, double* z) { precond.apply(r_in, z, stream, transposed); }
 
 double Surface::pnorm(const double* v) {
    const int nb = vec_blocks(n);
@@ -162,7 +179,7 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
    *status = FFTSVD_OK;
    FFTSVD_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
    // r = P^-1 rhs (GMRES.c:457-465)
-   precond.apply(rhs, r.get(), stream);
+   pinv(rhs, r.get());
    const double normr = pnorm(r.get());
    if (!std::isfinite(normr)) {
       *status = FFTSVD_ERR_NONFINITE;
@@ -191,7 +208,7 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       const double* vi = Vp + (int64_t)i * ldv;
       double* vnext = Vp + (int64_t)(i + 1) * ldv;
       apply(precision, vi, w.get());
-      precond.apply(w.get(), w.get(), stream);
+      pinv(w.get(), w.get());
       dots_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
       reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h1.get(), 0, 0, 0);
@@ -252,7 +269,7 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
    } else if (precision == FFTSVD_PREC_MIXED) {
       // FP64 iterative refinement around FP32-operator GMRES: x += A32^-1 (b - A64 x)
       const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
-      precond.apply(rhs, t0.get(), stream);
+      pinv(rhs, t0.get());
       const double bn = pnorm(t0.get());
       FFTSVD_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
       FFTSVD_CUDA(cudaMemcpyAsync(t1.get(), rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
@@ -271,10 +288,10 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
          if (st2 == FFTSVD_ERR_NONFINITE) { status = st2; break; }
          add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x, 0);
          FFTSVD_CHECK_LAUNCH();
-         op64.apply(x, t2.get(), stream);
+         apply(FFTSVD_PREC_FP64, x, t2.get());
          sub_kernel<<<ew_blocks, 256, 0, stream>>>(n, rhs, t2.get(), t1.get(), 0);
          FFTSVD_CHECK_LAUNCH();
-         precond.apply(t1.get(), t0.get(), stream);
+         pinv(t1.get(), t0.get());
          res = pnorm(t0.get()) / bn;
          if (!std::isfinite(res)) status = FFTSVD_ERR_NONFINITE;
       }

@@ -22,9 +22,10 @@ struct Preconditioner {
    int nblocks = 0;
    DevBuf<int32_t> blk_ptr, blk_idx;
    DevBuf<int64_t> inv_off;
-   DevBuf<double> inv;
+   DevBuf<double> inv, inv_t;  // block inverses and their transposes
    void build(const fftsvd_precond_csc& P, int n);  // host factorisation into dense block inverses
-   void apply(const double* r, double* z, cudaStream_t s) const;
+   // z = P^-1 r, or P^-T r for the transposed system
+   void apply(const double* r, double* z, cudaStream_t s, bool transpose = false) const;
 };
 
 struct Surface {
@@ -56,13 +57,21 @@ struct Surface {
 
    ~Surface();
    void ensure_capacity(int nvec);
+   // While `transposed` is set, apply, pinv, gmres and solve work on A^T and P^T (adjoint solves).
+   bool transposed = false;
    void apply(int precision, const double* x, double* y);
+   void pinv(const double* r, double* z);
    double pnorm(const double* v);  // ||v|| on device, synchronous
    // Left-preconditioned un-restarted GMRES (GMRES.c:446-539) with operator `precision`;
    // x overwritten.  Returns iterations; residual via *res.
    int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
              bool absolute_zero_check = true);
    int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
+   // Solvation energy and its derivatives with respect to the charges and their positions
+   // (adjoint.cu); dG_dq holds num_charges entries, dG_dx 3 * num_charges; info[0] is the
+   // forward solve, info[1] the adjoint (transposed) solve.
+   int adjoint(int precision, double tol, int maxit, double* energy, double* dG_dq, double* dG_dx,
+               fftsvd_solve_info* info);
 
    // ---- many right-hand sides (batch.cu); blocks of ncols vectors, column c at base + c * n
    std::unique_ptr<BatchWorkspace> bw;

@@ -238,6 +238,29 @@ class Surface:
     def reaction_potentials_device(self, sol_ptr: int, phi_ptr: int):
         check(load().fftsvd_b200_reaction_potentials_device(self._h, C.c_void_p(sol_ptr), C.c_void_p(phi_ptr)))
 
+    # ---- adjoint
+    def set_charges(self, charge_pos, charge):
+        qp, qv = f64(charge_pos), f64(charge)
+        check(load().fftsvd_b200_set_charges(self._h, len(qv), ptr(qp), ptr(qv)))
+        self.num_charges = len(qv)
+
+    def matvec_transpose(self, x, precision="fp64"):
+        x = f64(x)
+        y = np.empty(self.n)
+        check(load().fftsvd_b200_matvec_transpose(self._h, _prec(precision), ptr(x), ptr(y)))
+        return y
+
+    def adjoint(self, precision="fp64", tol=1e-6, max_iterations=1000):
+        """Solvation energy and its derivatives: (dG, dG/dq [nq], dG/dx [nq, 3], (forward, adjoint) SolveInfo)."""
+        nq = self.num_charges
+        e = C.c_double()
+        dq = np.empty(max(nq, 1))
+        dx = np.empty(max(3 * nq, 1))
+        info = (SolveInfo * 2)()
+        check(load().fftsvd_b200_adjoint(self._h, _prec(precision), float(tol), int(max_iterations), C.byref(e),
+                                         ptr(dq), ptr(dx), info))
+        return e.value, dq[:nq].copy(), dx[:3 * nq].reshape(nq, 3).copy(), (info[0], info[1])
+
     # ---- many right-hand sides (blocks of k vectors, one after the other)
     def matvec_batch_device(self, x_ptr: int, y_ptr: int, nrhs: int, precision="fp32"):
         check(load().fftsvd_b200_matvec_batch_device(self._h, _prec(precision), int(nrhs), C.c_void_p(x_ptr),

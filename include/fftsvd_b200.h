@@ -255,6 +255,25 @@ int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const doubl
 /* The CUDA stream all work of this surface is issued on (cudaStream_t). */
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s);
 
+/* ---- adjoint: derivatives of the solvation energy (no counterpart in the
+   reference; its FFTSVDforce computes conductor forces, FFTSVDforce.c:111-156) ---- */
+
+/* Replace the surface's point charges (positions [3*num_charges] in A, values in e). */
+int fftsvd_b200_set_charges(fftsvd_surface* s, int32_t num_charges, const double* charge_pos, const double* charge);
+/* y = A^T x, the transposed surface operator (near blocks and the far field run
+   backwards, the translation with the opposite-offset tables).  Column sums use
+   FP64 atomics, so results are not bitwise reproducible run to run. */
+int fftsvd_b200_matvec_transpose(fftsvd_surface* s, int32_t precision, const double* x, double* y);
+int fftsvd_b200_matvec_transpose_device(fftsvd_surface* s, int32_t precision, const double* x, double* y);
+/* Solvation energy dG = 1/2 k q^T L A^-1 B q (k = 332.112 / eps_in, B the right-hand
+   side of the charges, L the reaction-potential collection) and its exact derivatives
+   with respect to every charge (dG_dq, num_charges entries, kcal/mol/e) and every
+   charge position (dG_dx, 3 * num_charges entries, kcal/mol/A), from one forward and
+   one transposed solve (lambda = A^-T L^T q) at `precision` and `tol`.  dG_dq and
+   dG_dx may be NULL; info is NULL or two entries (forward, adjoint solve). */
+int fftsvd_b200_adjoint(fftsvd_surface* s, int32_t precision, double tol, int32_t max_iterations, double* energy,
+                        double* dG_dq, double* dG_dx, fftsvd_solve_info* info);
+
 /* ---- many right-hand sides of one surface (no counterpart in the reference;
    the batched solve named by the port's plan, fftsvd_b200_solve_batch) ----
    Blocks of k vectors of fftsvd_b200_num_unknowns doubles are stored one vector
