@@ -42,6 +42,9 @@ CONFIGS = {
                   level=5, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1),
     "large": dict(name="large blob L7 (327680 panels, R 60 A, 30000 charges, eps 4/80, kappa 0.125)", kind="blob",
                   level=7, radius=60.0, nq=30000, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=3),
+    # adjoint forces on the blob system, checked by central differences on seeded atoms
+    "adjoint": dict(name="blob L6 (81920 panels, 2500 charges): adjoint dG/dx and dG/dq", kind="blob",
+                    level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, fd_atoms=50),
     # many right-hand sides: the blob surface with its charges in 256 seeded disjoint groups
     "batch": dict(name="blob L6 (81920 panels), 256 right-hand sides of ~10 charges each", kind="blob",
                   level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, groups=256),
@@ -471,6 +474,90 @@ def run_batch(args, cfg, ws, rank, local):
     s.close()
 
 
+def run_adjoint(args, cfg, ws, rank, local):
+    """Energy derivatives by one forward and one transposed solve (mixed precision), timed
+    on the device; central differences (FP64 solves, h = 1e-4 A / 1e-4 e) on seeded atoms."""
+    import torch
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface
+
+    torch.cuda.set_device(local)
+    lib = load()
+    tri, qpos, q = make_workload(cfg)
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    stream = torch.cuda.ExternalStream(lib.fftsvd_b200_surface_stream(s._h))
+    for _ in range(max(1, args.warmup - 2)):
+        s.adjoint(precision="mixed", tol=GMRES_TOL)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total = 0.0
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e, dq, dx, info = s.adjoint(precision="mixed", tol=GMRES_TOL)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+    ms = barrier_max(total / args.steps, ws)
+    # FP64 adjoint to the finite differences' tolerance, and the differences themselves
+    tol_fd = 1e-12  # energy noise ~1e-12 |dG|: far below the differences over 2h = 2e-4 A
+    e64, dq64, dx64, _ = s.adjoint(precision="fp64", tol=tol_fd)
+
+    def energy(pos, chg):
+        s.set_charges(pos, chg)
+        sol = s.solve(s.rhs(), precision="fp64", tol=tol_fd).solution
+        return s.energy(s.reaction_potentials(sol))
+
+    rng = np.random.default_rng(cfg["seed"] + 2000)
+    atoms = rng.choice(len(q), size=min(cfg["fd_atoms"], len(q)), replace=False)
+    h = 1e-4
+    fscale = np.abs(dx64).max()
+    errx, errq = [], []
+    for j in atoms:
+        for a in range(3):
+            p, m = qpos.copy(), qpos.copy()
+            p[j, a] += h
+            m[j, a] -= h
+            fd = (energy(p, q) - energy(m, q)) / (2 * h)
+            errx.append(abs(dx64[j, a] - fd) / max(abs(fd), 1e-2 * fscale))
+        qp, qm = q.copy(), q.copy()
+        qp[j] += h
+        qm[j] -= h
+        fdq = (energy(qpos, qp) - energy(qpos, qm)) / (2 * h)
+        errq.append(abs(dq64[j] - fdq) / abs(fdq))
+    # the worst component again at half and twice the step: an error growing like 1/h is a
+    # jump of the discrete energy (a collection integral changing formula between x-h and x+h)
+    worst = int(np.argmax(errx))
+    wj, wa = atoms[worst // 3], worst % 3
+    step_err = {}
+    for hh in (h / 2, h, 2 * h):
+        p, m = qpos.copy(), qpos.copy()
+        p[wj, wa] += hh
+        m[wj, wa] -= hh
+        fd = (energy(p, q) - energy(m, q)) / (2 * hh)
+        step_err[f"{hh:g}"] = abs(dx64[wj, wa] - fd)
+    s.set_charges(qpos, q)
+    if rank == 0:
+        line = {
+            "metric": "adjoint dG/dx and dG/dq ms (forward and transposed mixed-precision solves + derivative kernels)",
+            "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 operator, f64 Krylov vectors, refinement and derivative kernels", "data": "synthetic",
+            "config": {"workload": cfg["name"], "charges": len(q), "gmres_tol": GMRES_TOL, "svd_tol": SVD_TOL,
+                       "fd_atoms": len(atoms), "fd_step": h, "fd_solver_tol": tol_fd},
+            "iterations_forward": info[0].iterations, "iterations_adjoint": info[1].iterations,
+            "dG_kcal": e, "dG_rel_err_mixed_vs_fp64": abs(e - e64) / abs(e64),
+            "force_rel_err_mixed_vs_fp64": float(np.abs(dx - dx64).max() / fscale),
+            "fd_max_rel_err_dG_dx": max(errx), "fd_median_rel_err_dG_dx": float(np.median(errx)),
+            "fd_max_rel_err_dG_dq": max(errq),
+            "fd_worst_component": {"atom": int(wj), "axis": int(wa), "force": float(dx64[wj, wa]),
+                                   "abs_err_by_step": step_err},
+            "max_force_kcal_per_A": float(fscale), "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    s.close()
+
+
 def run_matvec_only(args, cfg, local):
     """Build the surface and run `--reps` FP32 and FP64 matvecs (for profiler captures)."""
     import torch
@@ -515,6 +602,8 @@ def main():
             run_reference(args, cfg, ws, rank)
         elif "groups" in cfg:
             run_batch(args, cfg, ws, rank, local)
+        elif "fd_atoms" in cfg:
+            run_adjoint(args, cfg, ws, rank, local)
         else:
             run_ours(args, cfg, ws, rank, local)
     finally:
