@@ -45,6 +45,9 @@ CONFIGS = {
     # adjoint forces on the blob system, checked by central differences on seeded atoms
     "adjoint": dict(name="blob L6 (81920 panels, 2500 charges): adjoint dG/dx and dG/dq", kind="blob",
                     level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, fd_atoms=50),
+    # many surfaces: 64 seeded blobs of level 3 to 6 solved concurrently
+    "many": dict(name="64 seeded blobs, level 3-6 icospheres (1280-81920 panels), 50-2500 charges", kind="many",
+                 surfaces=64, seed=5, eps_in=4.0, eps_out=80.0, kappa=0.125),
     # many right-hand sides: the blob surface with its charges in 256 seeded disjoint groups
     "batch": dict(name="blob L6 (81920 panels), 256 right-hand sides of ~10 charges each", kind="blob",
                   level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, groups=256),
@@ -558,6 +561,87 @@ def run_adjoint(args, cfg, ws, rank, local):
     s.close()
 
 
+MANY_LEVELS = {3: (8.0, 50), 4: (12.0, 200), 5: (16.0, 800), 6: (22.0, 2500)}  # level -> (radius A, charges)
+
+
+def run_many(args, cfg, ws, rank, local):
+    """Independent surfaces: the same set solved one after another and through one
+    fftsvd_b200_solve_many call (host threads, per-surface streams); surfaces sharded
+    over ranks."""
+    import torch
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface, solve_many
+
+    torch.cuda.set_device(local)
+    lib = load()
+    rng = np.random.default_rng(cfg["seed"])
+    levels = rng.choice([3, 4, 5, 6], size=cfg["surfaces"], p=[0.4, 0.3, 0.2, 0.1])
+    mine = replica_shares(cfg["surfaces"], ws)[rank]
+    surfs, rhs, sols, panels = [], [], [], 0
+    t0 = time.time()
+    for i in mine:
+        lv = int(levels[i])
+        radius, nq = MANY_LEVELS[lv]
+        sub = dict(kind="blob", level=lv, radius=radius, nq=nq, seed=cfg["seed"] * 1000 + i)
+        tri, qpos, q = make_workload(sub)
+        s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+        surfs.append(s)
+        r = torch.empty(s.n, dtype=torch.float64, device="cuda")
+        s.rhs_device(r.data_ptr())
+        rhs.append(r)
+        sols.append(torch.empty_like(r))
+        panels += len(tri)
+    setup_s = time.time() - t0
+    torch.cuda.synchronize()
+
+    def sequential(precision):
+        total = 0.0
+        for s, r, x in zip(surfs, rhs, sols):
+            st = torch.cuda.ExternalStream(lib.fftsvd_b200_surface_stream(s._h))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            s.solve_device(r.data_ptr(), x.data_ptr(), precision, GMRES_TOL)
+            e1.record(st)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total
+
+    def concurrent(precision):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        info = solve_many(surfs, [r.data_ptr() for r in rhs], [x.data_ptr() for x in sols], precision, GMRES_TOL)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3, info
+
+    for _ in range(max(1, args.warmup - 2)):
+        concurrent("mixed")
+    seq_ms = sequential("mixed")
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        runs = [concurrent("mixed")[0] for _ in range(args.steps)]
+    conc_ms = barrier_max(sum(runs) / len(runs), ws)
+    e_mixed = [s.energy(s.reaction_potentials(x.cpu().numpy())) for s, x in zip(surfs, sols)]
+    conc64, _ = concurrent("fp64")
+    e64 = [s.energy(s.reaction_potentials(x.cpu().numpy())) for s, x in zip(surfs, sols)]
+    errs = [abs(a - b) / abs(b) for a, b in zip(e_mixed, e64) if b != 0.0]
+    if rank == 0:
+        line = {
+            "metric": f"many-surface PBE solve ms ({cfg['surfaces']} surfaces, mixed precision)",
+            "value": conc_ms, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": conc_ms, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 operator, f64 Krylov vectors and refinement", "data": "synthetic",
+            "config": {"workload": cfg["name"], "surfaces_per_rank": len(surfs), "panels_per_rank": panels,
+                       "levels": [int(levels[i]) for i in mine], "gmres_tol": GMRES_TOL, "svd_tol": SVD_TOL,
+                       "timing": "host clock around one fftsvd_b200_solve_many call (it returns after every solve)"},
+            "sequential_ms": seq_ms, "concurrency_speedup": seq_ms / conc_ms, "fp64_ms": conc64,
+            "speedup_mixed_vs_fp64": conc64 / conc_ms, "dG_rel_err_mixed_vs_fp64_max": max(errs) if errs else None,
+            "setup_s": setup_s, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    for s in surfs:
+        s.close()
+
+
 def run_matvec_only(args, cfg, local):
     """Build the surface and run `--reps` FP32 and FP64 matvecs (for profiler captures)."""
     import torch
@@ -600,6 +684,8 @@ def main():
             run_matvec_only(args, cfg, local)
         elif args.impl == "reference":
             run_reference(args, cfg, ws, rank)
+        elif cfg.get("kind") == "many":
+            run_many(args, cfg, ws, rank, local)
         elif "groups" in cfg:
             run_batch(args, cfg, ws, rank, local)
         elif "fd_atoms" in cfg:

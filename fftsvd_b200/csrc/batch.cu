@@ -15,8 +15,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
@@ -386,3 +389,52 @@ int fftsvd_b200_matvec_batch_device(fftsvd_surface* s, int32_t precision, int32_
 }
 
 }  // extern "C"
+
+// ---- many surfaces at once
+//
+// Every surface owns its buffers, streams and events, so solves of different surfaces
+// are independent: a pool of host threads runs them concurrently (largest surface
+// first), each on its surface's device and streams, and the GPU overlaps their kernels.
+extern "C" int fftsvd_b200_solve_many(int32_t count, fftsvd_surface* const* surfaces, const double* const* rhs,
+                                      double* const* sol, int32_t precision, double tol, int32_t max_iterations,
+                                      fftsvd_solve_info* info) {
+   if (count <= 0 || !surfaces || !rhs || !sol) return FFTSVD_ERR_ARGUMENT;
+   for (int i = 0; i < count; i++)
+      if (!surfaces[i] || !rhs[i] || !sol[i]) return FFTSVD_ERR_ARGUMENT;
+   std::vector<int> order(count);
+   for (int i = 0; i < count; i++) order[i] = i;
+   std::stable_sort(order.begin(), order.end(),
+                    [&](int a, int b) { return surfaces[a]->s.n > surfaces[b]->s.n; });
+   std::vector<int> status(count, FFTSVD_OK);
+   std::vector<std::string> message(count);
+   std::atomic<int> next{0};
+   const int workers = std::max(1, std::min<int>(count, std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+   auto work = [&]() {
+      for (;;) {
+         const int k = next.fetch_add(1);
+         if (k >= count) return;
+         const int i = order[k];
+         fftsvd::Surface& S = surfaces[i]->s;
+         fftsvd_solve_info one{};
+         int st = FFTSVD_OK;
+         const int rc = guarded([&] {
+            FFTSVD_CUDA(cudaSetDevice(S.device));
+            st = S.solve(precision, rhs[i], sol[i], tol, max_iterations, &one);
+         });
+         status[i] = rc != FFTSVD_OK ? rc : st;
+         if (rc != FFTSVD_OK) message[i] = fftsvd_b200_last_error();
+         if (info) info[i] = one;
+      }
+   };
+   std::vector<std::thread> pool;
+   for (int w = 1; w < workers; w++) pool.emplace_back(work);
+   work();
+   for (auto& t : pool) t.join();
+   for (int i = 0; i < count; i++)
+      if (status[i] != FFTSVD_OK) {
+         fftsvd::set_last_error(message[i].empty() ? "surface " + std::to_string(i) + " did not solve"
+                                                   : "surface " + std::to_string(i) + ": " + message[i]);
+         return status[i];
+      }
+   return FFTSVD_OK;
+}

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 
@@ -1751,6 +1752,19 @@ static void upload_pairs(DevBuf<typename Vec2<T>::type>& dst, const std::vector<
    dst.upload(tmp);
 }
 
+// The dynamic shared-memory limit of a kernel is one device-wide setting shared by
+// every surface: raise it to what this surface needs, never lower it (a smaller
+// surface set up later must not break the launches of a larger one).
+static std::mutex g_smem_limit_mutex;
+template <typename K>
+static void raise_smem_limit(K* kernel, int bytes) {
+   std::lock_guard<std::mutex> lock(g_smem_limit_mutex);
+   cudaFuncAttributes a;
+   FFTSVD_CUDA(cudaFuncGetAttributes(&a, kernel));
+   if (a.maxDynamicSharedSizeBytes < bytes)
+      FFTSVD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
 template <typename T>
 void DeviceOperator<T>::upload(const OperatorLayout& L) {
    num_unknowns_ = L.num_unknowns;
@@ -1839,8 +1853,8 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
        src_smem_t_ > optin || dst_smem_t_ > optin)
       throw Error(FFTSVD_ERR_UNSUPPORTED, "operator block needs more shared memory than the device offers");
    if (tile_smem > 0) {
-      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
-      FFTSVD_CUDA(cudaFuncSetAttribute(translate_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem_b));
+      raise_smem_limit(translate_kernel<T, false>, tile_smem);
+      raise_smem_limit(translate_kernel<T, true>, tile_smem_b);
    }
    // FFTSVD_B200_WARP_MIN_CUBES overrides the cube count from which small grids run
    // one cube per warp (tests set 0 to cover those kernels on small surfaces)
@@ -1849,13 +1863,11 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    spectra_elems_ = std::max<int64_t>(L.spectra_elems, 1);
    translated_elems_ = std::max<int64_t>(L.translated_elems, 1);
    batch_capacity_ = 0;
-   FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, src_smem_));
-   FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dst_smem_));
-   FFTSVD_CUDA(cudaFuncSetAttribute(near_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, leaf_smem_max_));
-   FFTSVD_CUDA(cudaFuncSetAttribute(far_forward_t_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    std::max(src_smem_t_, 1)));
-   FFTSVD_CUDA(cudaFuncSetAttribute(far_backward_t_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    std::max(dst_smem_t_, 1)));
+   raise_smem_limit(far_forward_kernel<T>, src_smem_);
+   raise_smem_limit(far_backward_kernel<T>, dst_smem_);
+   raise_smem_limit(near_kernel<T>, leaf_smem_max_);
+   raise_smem_limit(far_forward_t_kernel<T>, std::max(src_smem_t_, 1));
+   raise_smem_limit(far_backward_t_kernel<T>, std::max(dst_smem_t_, 1));
    build_chains();
    FFTSVD_CUDA(cudaDeviceSynchronize());
 }

@@ -300,6 +300,19 @@ class Surface:
         return e
 
 
+def solve_many(surfaces, rhs_ptrs, sol_ptrs, precision="mixed", tol=1e-6, max_iterations=1000, raise_on_error=True):
+    """Solve several surfaces concurrently (device vectors per surface).  Returns the SolveInfo array."""
+    k = len(surfaces)
+    hs = (C.c_void_p * k)(*[s._h for s in surfaces])
+    rp = (C.c_void_p * k)(*[C.c_void_p(int(p)) for p in rhs_ptrs])
+    xp = (C.c_void_p * k)(*[C.c_void_p(int(p)) for p in sol_ptrs])
+    info = (SolveInfo * k)()
+    rc = load().fftsvd_b200_solve_many(k, hs, rp, xp, _prec(precision), float(tol), int(max_iterations), info)
+    if raise_on_error:
+        check(rc)
+    return info
+
+
 def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4,
                   num_threads=0):
     """Run only the host setup (no GPU): returns ([exterior tree, interior tree], preconditioner) as numpy."""

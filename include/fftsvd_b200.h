@@ -299,6 +299,14 @@ int fftsvd_b200_solve_batch_device(fftsvd_surface* s, int32_t nrhs, int32_t prec
 /* Same with host pointers. */
 int fftsvd_b200_solve_batch(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
                             double tol, int32_t max_iterations, fftsvd_solve_info* info);
+/* Solves `count` surfaces concurrently: rhs[i] and sol[i] are device vectors of
+   surface i (fftsvd_b200_solve_device semantics per surface), info is NULL or count
+   entries.  A pool of host threads drives the solves, each on its surface's device and
+   streams, largest surface first, so the surfaces' kernels overlap on the GPU.  Returns
+   the first non-OK status (by surface index), else FFTSVD_OK. */
+int fftsvd_b200_solve_many(int32_t count, fftsvd_surface* const* surfaces, const double* const* rhs,
+                           double* const* sol, int32_t precision, double tol, int32_t max_iterations,
+                           fftsvd_solve_info* info);
 /* Right-hand sides of charge groups: group g is the surface's charges
    [group_ptr[g], group_ptr[g+1]) (host array of ngroups + 1 non-decreasing
    offsets); rhs (device) receives ngroups vectors (SurfaceOperator.c:291-321

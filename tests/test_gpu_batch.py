@@ -100,3 +100,21 @@ def test_solve_batch_fault_isolated_to_its_column(blob3):
     one = s.solve(base, precision="fp64", tol=1e-6)
     assert rel(sol[0], one.solution) < 1e-9
     assert rel(sol[2], 3.0 * one.solution) < 1e-6
+
+
+def test_solve_many_matches_individual_solves(gpu):
+    import torch
+    from fftsvd_b200.surface import solve_many
+    surfs, rhs, sols = [], [], []
+    for name in ("born3", "blob3", "blob4"):
+        tri, qpos, q, c = make_case(name)
+        s = Surface.from_problem(tri, qpos, q, c["eps_in"], c["eps_out"], c["kappa"], svd_tol=1e-4)
+        surfs.append(s)
+        rhs.append(_dev(s.rhs()))
+        sols.append(torch.empty_like(rhs[-1]))
+    info = solve_many(surfs, [r.data_ptr() for r in rhs], [x.data_ptr() for x in sols], "mixed", tol=1e-6)
+    torch.cuda.synchronize()
+    for i, s in enumerate(surfs):
+        one = s.solve(rhs[i].cpu().numpy(), precision="mixed", tol=1e-6)
+        assert info[i].status == 0 and info[i].iterations == one.iterations
+        assert rel(sols[i].cpu().numpy(), one.solution) < 1e-12, i
