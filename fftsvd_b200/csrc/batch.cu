@@ -80,7 +80,7 @@ void Surface::apply_batch(int precision, const double* X, double* Y, int ncols) 
 void Surface::precond_batch(const double* r_in, double* z, int ncols) {
    const int threads = 256;
    const int blocks = std::max(1, std::min((precond.nblocks + threads - 1) / threads, 148 * 8));
-   precond_kernel<<<dim3(blocks, ncols), threads, 0, stream>>>(precond.nblocks, precond.blk_ptr.get(),
+   precond_kernel<<<dim3(blocks, 1, ncols), threads, 0, stream>>>(precond.nblocks, precond.blk_ptr.get(),
                                                                precond.blk_idx.get(), precond.inv_off.get(),
                                                                precond.inv.get(), r_in, z, n);
    FFTSVD_CHECK_LAUNCH();
@@ -89,9 +89,9 @@ void Surface::precond_batch(const double* r_in, double* z, int ncols) {
 void Surface::pnorm_batch(const double* v, int ncols, std::vector<double>& out) {
    BatchWorkspace& B = *bw;
    const int nb = vec_blocks(n);
-   norm_partial_kernel<<<dim3(nb, ncols), kVecThreads, 0, stream>>>(n, v, B.normpart.get(), n, nb);
+   norm_partial_kernel<<<dim3(nb, 1, ncols), kVecThreads, 0, stream>>>(n, v, B.normpart.get(), n, nb);
    FFTSVD_CHECK_LAUNCH();
-   reduce_partial_kernel<<<dim3(1, ncols), 256, 0, stream>>>(1, nb, B.normpart.get(), B.scal.get(), 0, nb, 1);
+   reduce_partial_kernel<<<dim3(1, 1, ncols), 256, 0, stream>>>(1, nb, B.normpart.get(), B.scal.get(), 0, nb, 1);
    FFTSVD_CHECK_LAUNCH();
    out.resize(ncols);
    FFTSVD_CUDA(cudaMemcpyAsync(out.data(), B.scal.get(), sizeof(double) * ncols, cudaMemcpyDeviceToHost, stream));
@@ -106,7 +106,7 @@ int Surface::gmres_batch(int precision, int ncols, const double* rhs, double* x,
    FFTSVD_REQUIRE(ncols <= B.ncols && ncols % kBatchGroup == 0, "batch workspace too small");
    maxit = std::min(maxit, B.capacity - 1);
    const int cap = B.capacity;
-   const int nb = vec_blocks(n);
+   const int nb = vec_blocks(n), nd = dot_blocks(n);
    const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
    const int64_t ldv = (int64_t)ncols * n;
    res.assign(ncols, 0.0);
@@ -141,7 +141,7 @@ int Surface::gmres_batch(int precision, int ncols, const double* rhs, double* x,
    if (running > 0) {
       double* Vp = B.V.get();
       FFTSVD_CUDA(cudaMemcpyAsync(B.factor.get(), inv.data(), sizeof(double) * ncols, cudaMemcpyHostToDevice, stream));
-      scale_kernel<<<dim3(ew_blocks, ncols), 256, 0, stream>>>(n, B.r.get(), B.factor.get(), 0.0, Vp, n, 1);
+      scale_kernel<<<dim3(ew_blocks, 1, ncols), 256, 0, stream>>>(n, B.r.get(), B.factor.get(), 0.0, Vp, n, 1);
       FFTSVD_CHECK_LAUNCH();
       FFTSVD_CUDA(cudaMemcpyAsync(B.g.get(), g0.data(), sizeof(double) * g0.size(), cudaMemcpyHostToDevice, stream));
       FFTSVD_CUDA(cudaMemcpyAsync(B.st.get(), sth.data(), sizeof(GivensState) * ncols, cudaMemcpyHostToDevice, stream));
@@ -155,27 +155,31 @@ int Surface::gmres_batch(int precision, int ncols, const double* rhs, double* x,
          double* vnext = Vp + (int64_t)(i + 1) * ldv;
          apply_batch(precision, vi, B.w.get(), ncols);
          precond_batch(B.w.get(), B.w.get(), ncols);
-         dots_partial_kernel<<<dim3(nb, ncols), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, B.w.get(),
-                                                                           B.partial.get(), n, pcol);
+         // CGS2 per column (see Surface::gmres)
+         const size_t sh = sizeof(double) * nvec;
+         dots_partial_kernel<<<dim3(nd, nvec, ncols), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, B.w.get(),
+                                                                                 B.partial.get(), n, pcol);
          FFTSVD_CHECK_LAUNCH();
-         reduce_partial_kernel<<<dim3(nvec, ncols), 256, 0, stream>>>(nvec, nb, B.partial.get(), B.h1.get(), 0, pcol,
-                                                                      cap);
+         reduce_partial_kernel<<<dim3(nvec, 1, ncols), 256, 0, stream>>>(nvec, nd, B.partial.get(), B.h1.get(), 0,
+                                                                         pcol, cap);
          FFTSVD_CHECK_LAUNCH();
-         const size_t sh = sizeof(double) * (((nvec + 1) & ~1) + kVecThreads / 32 * 8 + 8);
-         update_dots_kernel<<<dim3(nb, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h1.get(), B.w.get(),
-                                                                          B.partial.get(), n, pcol, cap);
+         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h1.get(), B.w.get(),
+                                                                        B.w.get(), nullptr, n, 0, cap);
          FFTSVD_CHECK_LAUNCH();
-         reduce_partial_kernel<<<dim3(nvec, ncols), 256, 0, stream>>>(nvec, nb, B.partial.get(), B.h2.get(), 0, pcol,
-                                                                      cap);
+         dots_partial_kernel<<<dim3(nd, nvec, ncols), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, B.w.get(),
+                                                                                 B.partial.get(), n, pcol);
          FFTSVD_CHECK_LAUNCH();
-         update_norm_kernel<<<dim3(nb, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h2.get(), B.w.get(),
-                                                                          vnext, B.normpart.get(), n, nb, cap);
+         reduce_partial_kernel<<<dim3(nvec, 1, ncols), 256, 0, stream>>>(nvec, nd, B.partial.get(), B.h2.get(), 0,
+                                                                         pcol, cap);
+         FFTSVD_CHECK_LAUNCH();
+         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h2.get(), B.w.get(),
+                                                                        vnext, B.normpart.get(), n, nb, cap);
          FFTSVD_CHECK_LAUNCH();
          givens_kernel<<<ncols, 256, 0, stream>>>(i, cap, B.H.get(), B.h1.get(), B.h2.get(), B.normpart.get(), nb,
                                                   B.cs.get(), B.sn.get(), B.g.get(), B.st.get(), cap, nb,
                                                   B.active.get());
          FFTSVD_CHECK_LAUNCH();
-         scale_kernel<<<dim3(ew_blocks, ncols), 256, 0, stream>>>(n, vnext, &B.st.get()->inv_beta, 0.0, vnext, n,
+         scale_kernel<<<dim3(ew_blocks, 1, ncols), 256, 0, stream>>>(n, vnext, &B.st.get()->inv_beta, 0.0, vnext, n,
                                                                   fcol);
          FFTSVD_CHECK_LAUNCH();
          FFTSVD_CUDA(cudaMemcpyAsync(sth.data(), B.st.get(), sizeof(GivensState) * ncols, cudaMemcpyDeviceToHost,
@@ -228,7 +232,7 @@ int Surface::gmres_batch(int precision, int ncols, const double* rhs, double* x,
             }
          }
          FFTSVD_CUDA(cudaMemcpyAsync(B.y.get(), yh.data(), sizeof(double) * yh.size(), cudaMemcpyHostToDevice, stream));
-         combine_kernel<<<dim3(ew_blocks, ncols), 256, sizeof(double) * kmax, stream>>>(n, kmax, Vp, ldv, B.y.get(), x,
+         combine_kernel<<<dim3(ew_blocks, 1, ncols), 256, sizeof(double) * kmax, stream>>>(n, kmax, Vp, ldv, B.y.get(), x,
                                                                                         n, kmax);
          FFTSVD_CHECK_LAUNCH();
       }
@@ -301,10 +305,10 @@ int Surface::solve_batch(int precision, int k, const double* rhs, double* x, dou
                iters[c] += iit[c];
                if (ist[c] == FFTSVD_ERR_NONFINITE) status[c] = FFTSVD_ERR_NONFINITE;
             }
-         add_kernel<<<dim3(ew_blocks, ncols), 256, 0, stream>>>(n, B.xout.get(), B.x0.get(), n);
+         add_kernel<<<dim3(ew_blocks, 1, ncols), 256, 0, stream>>>(n, B.xout.get(), B.x0.get(), n);
          FFTSVD_CHECK_LAUNCH();
          apply_batch(FFTSVD_PREC_FP64, B.x0.get(), B.t2.get(), ncols);
-         sub_kernel<<<dim3(ew_blocks, ncols), 256, 0, stream>>>(n, B.b0.get(), B.t2.get(), B.t1.get(), n);
+         sub_kernel<<<dim3(ew_blocks, 1, ncols), 256, 0, stream>>>(n, B.b0.get(), B.t2.get(), B.t1.get(), n);
          FFTSVD_CHECK_LAUNCH();
          precond_batch(B.t1.get(), B.t0.get(), ncols);
          std::vector<double> rn;

@@ -2,8 +2,10 @@
 // Gram-Schmidt, one dot and one axpy per basis vector (GMRES.c:485-488); here
 // each Arnoldi step uses classical Gram-Schmidt applied twice (two passes of
 // one multi-dot and one multi-axpy over the whole basis), which is as stable as
-// MGS and turns 2(i+1) dependent vector sweeps into four.  All reductions are
-// two-stage with a fixed order, so results are bitwise reproducible run to run.
+// MGS and turns 2(i+1) dependent vector sweeps into four.  The multi-dot runs one
+// block per (4096-row chunk, basis vector); updates one row per thread.  All
+// reductions are two-stage with a fixed order, so results are bitwise
+// reproducible run to run.
 #include <cmath>
 
 #include "gmres.cuh"
@@ -19,8 +21,8 @@ __device__ inline double warp_sum_d(double v) {
 __global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
                                const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
                                const double* __restrict__ r, double* __restrict__ z, int64_t col) {
-   r += blockIdx.y * col;
-   z += blockIdx.y * col;
+   r += blockIdx.z * col;
+   z += blockIdx.z * col;
    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += gridDim.x * blockDim.x) {
       const int p0 = blk_ptr[b], k = blk_ptr[b + 1] - p0;
       double in[8], out[8];
@@ -35,62 +37,44 @@ __global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr,
    }
 }
 
-// Block-wide reduction of 8 values per thread into red[0..7] (fixed order).
-__device__ inline void block_reduce8(double (&acc)[8], double* red /* [nwarps*8] */, int tid) {
-   const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-   for (int q = 0; q < 8; q++) acc[q] = warp_sum_d(acc[q]);
-   if (lane == 0)
-#pragma unroll
-      for (int q = 0; q < 8; q++) red[warp * 8 + q] = acc[q];
+// Sum of v over the block's threads, in a fixed order; valid in thread 0.
+__device__ inline double block_sum(double v, double* red /* [kVecThreads / 32] */) {
+   v = warp_sum_d(v);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (lane == 0) red[warp] = v;
    __syncthreads();
-   if (tid < 8) {
-      double s = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w * 8 + tid];
-      red[kVecThreads / 32 * 8 + tid] = s;
-   }
-   __syncthreads();
-}
-
-__device__ inline void dots_of(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv, int64_t k0, int64_t k1,
-                               double w0, double w1, double* __restrict__ partial, double* red) {
-   const int tid = threadIdx.x;
-   for (int j = 0; j < nvec; j += 8) {
-      double acc[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-         double s = 0.0;
-         if (j + q < nvec) {
-            const double* v = V + (int64_t)(j + q) * ldv;
-            if (k0 < n) s += v[k0] * w0;
-            if (k1 < n) s += v[k1] * w1;
-         }
-         acc[q] = s;
-      }
-      block_reduce8(acc, red, tid);
-      if (tid < 8 && j + tid < nvec) partial[(int64_t)(j + tid) * gridDim.x + blockIdx.x] = red[kVecThreads / 32 * 8 + tid];
-      __syncthreads();
-   }
+   double s = 0.0;
+   if (threadIdx.x == 0)
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+   return s;
 }
 
 __global__ void __launch_bounds__(kVecThreads) dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V,
                                                                    int64_t ldv, const double* __restrict__ w,
                                                                    double* __restrict__ partial, int64_t col,
                                                                    int64_t pcol) {
-   __shared__ double red[kVecThreads / 32 * 8 + 8];
-   V += blockIdx.y * col;
-   w += blockIdx.y * col;
-   partial += blockIdx.y * pcol;
-   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
-   const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
-   dots_of(n, nvec, V, ldv, k0, k1, w0, w1, partial, red);
+   __shared__ double red[kVecThreads / 32];
+   const int j = blockIdx.y;
+   V += blockIdx.z * col + (int64_t)j * ldv;
+   w += blockIdx.z * col;
+   partial += blockIdx.z * pcol;
+   const int64_t k0 = (int64_t)blockIdx.x * kDotChunk, k1 = min(n, k0 + kDotChunk);
+   double s0 = 0.0, s1 = 0.0;
+   int64_t k = k0 + threadIdx.x;
+   for (; k + blockDim.x < k1; k += 2 * blockDim.x) {
+      s0 += V[k] * w[k];
+      s1 += V[k + blockDim.x] * w[k + blockDim.x];
+   }
+   if (k < k1) s0 += V[k] * w[k];
+   const double s = block_sum(s0 + s1, red);
+   if (threadIdx.x == 0) partial[(int64_t)j * gridDim.x + blockIdx.x] = s;
 }
 
 __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
                                       int accumulate, int64_t pcol, int64_t hcol) {
    __shared__ double red[32];
-   partial += blockIdx.y * pcol;
-   out += blockIdx.y * hcol;
+   partial += blockIdx.z * pcol;
+   out += blockIdx.z * hcol;
    const int j = blockIdx.x;
    if (j >= nvec) return;
    double s = 0.0;
@@ -105,72 +89,52 @@ __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restri
    }
 }
 
-__global__ void __launch_bounds__(kVecThreads) update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V,
-                                                                  int64_t ldv, const double* __restrict__ h,
-                                                                  double* __restrict__ w, double* __restrict__ partial,
-                                                                  int64_t col, int64_t pcol, int64_t hcol) {
-   extern __shared__ double sh[];  // [nvec] h, then reduction scratch
-   V += blockIdx.y * col;
-   w += blockIdx.y * col;
-   partial += blockIdx.y * pcol;
-   h += blockIdx.y * hcol;
-   double* hs = sh;
-   double* red = sh + ((nvec + 1) & ~1);
+__global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec, const double* __restrict__ V,
+                                                             int64_t ldv, const double* __restrict__ h,
+                                                             const double* __restrict__ w, double* __restrict__ out,
+                                                             double* __restrict__ norm_partial, int64_t col,
+                                                             int64_t pcol, int64_t hcol) {
+   extern __shared__ double hs[];  // [nvec]
+   __shared__ double red[kVecThreads / 32];
+   V += blockIdx.z * col;
+   w += blockIdx.z * col;
+   out += blockIdx.z * col;
+   h += blockIdx.z * hcol;
    for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
    __syncthreads();
-   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
-   double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
-   for (int j = 0; j < nvec; j++) {
-      const double* v = V + (int64_t)j * ldv;
-      if (k0 < n) w0 -= v[k0] * hs[j];
-      if (k1 < n) w1 -= v[k1] * hs[j];
+   const int64_t k = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+   double x = 0.0;
+   if (k < n) {
+      x = w[k];
+      const double* v = V + k;
+      int j = 0;
+      for (; j + 3 < nvec; j += 4) {
+         const double a0 = v[(int64_t)j * ldv], a1 = v[(int64_t)(j + 1) * ldv];
+         const double a2 = v[(int64_t)(j + 2) * ldv], a3 = v[(int64_t)(j + 3) * ldv];
+         x -= a0 * hs[j];
+         x -= a1 * hs[j + 1];
+         x -= a2 * hs[j + 2];
+         x -= a3 * hs[j + 3];
+      }
+      for (; j < nvec; j++) x -= v[(int64_t)j * ldv] * hs[j];
+      out[k] = x;
    }
-   if (k0 < n) w[k0] = w0;
-   if (k1 < n) w[k1] = w1;
-   dots_of(n, nvec, V, ldv, k0, k1, w0, w1, partial, red);
-}
-
-__global__ void __launch_bounds__(kVecThreads) update_norm_kernel(int64_t n, int nvec, const double* __restrict__ V,
-                                                                  int64_t ldv, const double* __restrict__ h,
-                                                                  const double* __restrict__ w,
-                                                                  double* __restrict__ out,
-                                                                  double* __restrict__ partial, int64_t col,
-                                                                  int64_t pcol, int64_t hcol) {
-   extern __shared__ double sh[];
-   V += blockIdx.y * col;
-   w += blockIdx.y * col;
-   out += blockIdx.y * col;
-   partial += blockIdx.y * pcol;
-   h += blockIdx.y * hcol;
-   double* hs = sh;
-   double* red = sh + ((nvec + 1) & ~1);
-   for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
-   __syncthreads();
-   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
-   double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
-   for (int j = 0; j < nvec; j++) {
-      const double* v = V + (int64_t)j * ldv;
-      if (k0 < n) w0 -= v[k0] * hs[j];
-      if (k1 < n) w1 -= v[k1] * hs[j];
+   if (norm_partial) {
+      const double s = block_sum(x * x, red);
+      if (threadIdx.x == 0) norm_partial[blockIdx.z * pcol + blockIdx.x] = s;
    }
-   if (k0 < n) out[k0] = w0;
-   if (k1 < n) out[k1] = w1;
-   double acc[8] = {w0 * w0 + w1 * w1, 0, 0, 0, 0, 0, 0, 0};
-   block_reduce8(acc, red, threadIdx.x);
-   if (threadIdx.x == 0) partial[blockIdx.x] = red[kVecThreads / 32 * 8];
 }
 
 __global__ void __launch_bounds__(kVecThreads) norm_partial_kernel(int64_t n, const double* __restrict__ w,
                                                                    double* __restrict__ partial, int64_t col,
                                                                    int64_t pcol) {
-   __shared__ double red[kVecThreads / 32 * 8 + 8];
-   w += blockIdx.y * col;
-   partial += blockIdx.y * pcol;
-   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x, k1 = k0 + kVecThreads;
-   const double w0 = k0 < n ? w[k0] : 0.0, w1 = k1 < n ? w[k1] : 0.0;
-   double acc[8] = {w0 * w0 + w1 * w1, 0, 0, 0, 0, 0, 0, 0};
-   block_reduce8(acc, red, threadIdx.x);
-   if (threadIdx.x == 0) partial[blockIdx.x] = red[kVecThreads / 32 * 8];
+   __shared__ double red[kVecThreads / 32];
+   w += blockIdx.z * col;
+   partial += blockIdx.z * pcol;
+   const int64_t k = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+   const double x = k < n ? w[k] : 0.0;
+   const double s = block_sum(x * x, red);
+   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
 __device__ inline void rotate(double c, double s, double* a, double* b) {  // GMRES.c:17-22
@@ -240,9 +204,9 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
 
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
                              double factor, double* __restrict__ dst, int64_t col, int64_t fcol) {
-   src += blockIdx.y * col;
-   dst += blockIdx.y * col;
-   const double f = factor_ptr ? factor_ptr[blockIdx.y * fcol] : factor;
+   src += blockIdx.z * col;
+   dst += blockIdx.z * col;
+   const double f = factor_ptr ? factor_ptr[blockIdx.z * fcol] : factor;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] = src[k] * f;
 }
@@ -250,9 +214,9 @@ __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const do
 __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
                                const double* __restrict__ y, double* __restrict__ x, int64_t col, int64_t ycol) {
    extern __shared__ double ys[];
-   V += blockIdx.y * col;
-   x += blockIdx.y * col;
-   y += blockIdx.y * ycol;
+   V += blockIdx.z * col;
+   x += blockIdx.z * col;
+   y += blockIdx.z * ycol;
    for (int j = threadIdx.x; j < nvec; j += blockDim.x) ys[j] = y[j];
    __syncthreads();
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -264,16 +228,16 @@ __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V
 
 __global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                            double* __restrict__ dst, int64_t col) {
-   a += blockIdx.y * col;
-   b += blockIdx.y * col;
-   dst += blockIdx.y * col;
+   a += blockIdx.z * col;
+   b += blockIdx.z * col;
+   dst += blockIdx.z * col;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] = a[k] - b[k];
 }
 
 __global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst, int64_t col) {
-   a += blockIdx.y * col;
-   dst += blockIdx.y * col;
+   a += blockIdx.z * col;
+   dst += blockIdx.z * col;
    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
       dst[k] += a[k];
 }

@@ -1,7 +1,7 @@
 // Device kernels of the GMRES solve (GMRES.c:446-539) and the block-diagonal
 // preconditioner (Preconditioner.c:272-294).  FP64 throughout.
 //
-// Every kernel also runs a batch of independent columns: column c = blockIdx.y
+// Every kernel also runs a batch of independent columns: column c = blockIdx.z
 // (blockIdx.x for givens_kernel) shifts each vector argument by c times its
 // column stride (col for vectors and basis columns, pcol for partial sums, hcol
 // for Gram-Schmidt coefficients, fcol for scale factors, ycol for combination
@@ -15,29 +15,26 @@
 namespace fftsvd {
 
 constexpr int kVecThreads = 256;
-constexpr int kRowsPerThread = 2;
-constexpr int kRowsPerBlock = kVecThreads * kRowsPerThread;
+constexpr int kRowsPerBlock = kVecThreads;  // one row per thread in row-wise kernels
+constexpr int kDotChunk = 4096;             // rows per block of the multi-dot
 
 // z[idx] = inv * r[idx] for every preconditioner block (blocks of size <= 8).
 __global__ void precond_kernel(int nblocks, const int32_t* __restrict__ blk_ptr, const int32_t* __restrict__ blk_idx,
                                const int64_t* __restrict__ inv_off, const double* __restrict__ inv,
                                const double* __restrict__ r, double* __restrict__ z, int64_t col);
 
-// partial[j * nblk + b] = sum over rows of block b of V[j][k] * w[k], j < nvec
+// grid (dot_blocks(n), nvec): partial[j * dot_blocks + b] = sum over rows of chunk b of V[j][k] * w[k]
 __global__ void dots_partial_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
                                     const double* __restrict__ w, double* __restrict__ partial, int64_t col,
                                     int64_t pcol);
 // out[j] = (accumulate ? out[j] : 0) + sum_b partial[j * nblk + b]; one block per j
 __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
                                       int accumulate, int64_t pcol, int64_t hcol);
-// w -= V h; then partial dots of the updated w against V (second Gram-Schmidt pass)
-__global__ void update_dots_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                                   const double* __restrict__ h, double* __restrict__ w, double* __restrict__ partial,
-                                   int64_t col, int64_t pcol, int64_t hcol);
-// out = w - V h (written to out, may alias w); partial[b] = sum of squares of out over block b
-__global__ void update_norm_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                                   const double* __restrict__ h, const double* __restrict__ w, double* __restrict__ out,
-                                   double* __restrict__ partial, int64_t col, int64_t pcol, int64_t hcol);
+// grid (vec_blocks(n)): out = w - V h (out may alias w), with nvec doubles of dynamic shared
+// memory; if norm_partial is given, norm_partial[b] = sum of squares of out over block b
+__global__ void update_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
+                              const double* __restrict__ h, const double* __restrict__ w, double* __restrict__ out,
+                              double* __restrict__ norm_partial, int64_t col, int64_t pcol, int64_t hcol);
 // partial[b] = sum of squares of w over block b
 __global__ void norm_partial_kernel(int64_t n, const double* __restrict__ w, double* __restrict__ partial, int64_t col,
                                     int64_t pcol);
@@ -74,5 +71,6 @@ __global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double
 __global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst, int64_t col);
 
 inline int vec_blocks(int64_t n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
+inline int dot_blocks(int64_t n) { return (int)((n + kDotChunk - 1) / kDotChunk); }
 
 }  // namespace fftsvd

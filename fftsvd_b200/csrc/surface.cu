@@ -173,7 +173,7 @@ double Surface::pnorm(const double* v) {
 
 int Surface::gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
                    bool absolute_zero_check) {
-   const int nb = vec_blocks(n);
+   const int nb = vec_blocks(n), nd = dot_blocks(n);
    const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
    ensure_capacity(maxit + 1);
    *status = FFTSVD_OK;
@@ -209,17 +209,20 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       double* vnext = Vp + (int64_t)(i + 1) * ldv;
       apply(precision, vi, w.get());
       pinv(w.get(), w.get());
-      dots_partial_kernel<<<nb, kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
+      // CGS2: h1 = V^T w, w -= V h1, h2 = V^T w, vnext = w - V h2 with its norm partials
+      const size_t sh = sizeof(double) * nvec;
+      dots_partial_kernel<<<dim3(nd, nvec), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h1.get(), 0, 0, 0);
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nd, partial.get(), h1.get(), 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      const size_t sh = sizeof(double) * (((nvec + 1) & ~1) + kVecThreads / 32 * 8 + 8);
-      update_dots_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), partial.get(), 0, 0, 0);
+      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), w.get(), nullptr, 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nb, partial.get(), h2.get(), 0, 0, 0);
+      dots_partial_kernel<<<dim3(nd, nvec), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      update_norm_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get(), 0,
-                                                           0, 0);
+      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nd, partial.get(), h2.get(), 0, 0, 0);
+      FFTSVD_CHECK_LAUNCH();
+      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get(), 0, 0,
+                                                     0);
       FFTSVD_CHECK_LAUNCH();
       givens_kernel<<<1, 256, 0, stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb, cs.get(),
                                            sn.get(), g.get(), st.get(), 0, 0, nullptr);
