@@ -333,17 +333,15 @@ def run_ours(args, cfg, ws, rank, local):
     peak, peak_kind = hbm_peak()
     dom = max(kernels, key=lambda k: prof["fp32"][k]["ms"])
     ach = prof["fp32"][dom]["gbs"]
+    # DRAM traffic of that stage per matvec, from the ncu capture summarised in profiles/
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "translate_dram_blob_l6.md")
+    key = cfg["kind"] + str(cfg.get("level", ""))
     if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                tj = json.load(f)
-            ent = tj.get(cfg["kind"] + str(cfg["level"]), {}).get(dom)
-            if ent:
-                traffic = float(ent)
-        except Exception:
-            traffic = None
+        for line in open(tpath):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) == 3 and cells[0] == key and cells[1] == dom and cells[2].isdigit():
+                traffic = float(cells[2])
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
