@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -46,8 +47,85 @@ void TileProblem::add_pair(int64_t in, int s) {
    ptr.back()++;
 }
 
-// Greedy tiling: outputs of one key in Morton order, while the destinations, halo inputs and
-// padded interactions fit the kernel limits; tiles grouped by frequency count.
+// Cube coordinates from a Morton code (bit 3b + k of the code is bit b of coordinate k).
+static void morton_decode(uint64_t code, int c[3]) {
+   c[0] = c[1] = c[2] = 0;
+   for (int b = 0; b < 21; b++)
+      for (int k = 0; k < 3; k++) c[k] |= (int)((code >> (3 * b + k)) & 1) << b;
+}
+
+namespace {
+// Sibling outputs sharing one list of sources: per source its base slot (the slot of
+// member 0) and the mask of the members that interact with it.
+struct MemberGroup {
+   std::vector<int> members;   // output ids
+   std::vector<int> delta;     // slot of member j = base + delta[j]
+   std::vector<int64_t> src;   // input offsets, first-seen order
+   std::vector<uint32_t> mask;
+   std::vector<int> base;
+};
+
+constexpr int kCenterSlot = 171;  // offset (0, 0, 0)
+
+int slot_of(const int v[3]) { return ((v[0] + 3) * 7 + (v[1] + 3)) * 7 + (v[2] + 3); }
+
+// Members [first, last) of ids (siblings in Morton order) as one group.  Returns false
+// when the shared source list would not be exact for every member: each member's
+// offset to each source of the union must lie in [-3, 3]^3, and a member that does not
+// interact with a source must be its neighbour (its slot is then one of the zeroed
+// local-offset rows).
+bool make_group(const TileProblem& P, const std::vector<int>& ids, size_t first, size_t last, MemberGroup& G) {
+   G = MemberGroup();
+   std::vector<std::array<int, 3>> pos;
+   for (size_t i = first; i < last; i++) {
+      int c[3];
+      morton_decode(P.morton[ids[i]], c);
+      pos.push_back({c[0], c[1], c[2]});
+   }
+   std::map<int64_t, int> where;
+   std::vector<std::array<int, 3>> v0;  // offset of member 0 to each source
+   for (size_t m = 0; m < pos.size(); m++) {
+      const int o = ids[first + m];
+      const int dp[3] = {pos[m][0] - pos[0][0], pos[m][1] - pos[0][1], pos[m][2] - pos[0][2]};
+      G.members.push_back(o);
+      G.delta.push_back(dp[0] * 49 + dp[1] * 7 + dp[2]);
+      for (int64_t q = P.ptr[o]; q < P.ptr[o + 1]; q++) {
+         const int s = P.slot[q];
+         FFTSVD_REQUIRE(s >= 0 && s < 343, "translation slot");
+         const std::array<int, 3> v = {s / 49 - 3 - dp[0], (s / 7) % 7 - 3 - dp[1], s % 7 - 3 - dp[2]};
+         auto it = where.find(P.in_off[q]);
+         if (it == where.end()) {
+            it = where.emplace(P.in_off[q], (int)G.src.size()).first;
+            G.src.push_back(P.in_off[q]);
+            G.mask.push_back(0);
+            v0.push_back(v);
+         }
+         const int e = it->second;
+         if (v0[e] != v) return false;
+         FFTSVD_REQUIRE(!((G.mask[e] >> m) & 1u), "repeated interaction");
+         G.mask[e] |= 1u << m;
+      }
+   }
+   for (size_t e = 0; e < G.src.size(); e++) {
+      for (size_t m = 0; m < pos.size(); m++) {
+         int v[3], far = 0;
+         for (int k = 0; k < 3; k++) {
+            v[k] = v0[e][k] + pos[m][k] - pos[0][k];
+            if (v[k] < -3 || v[k] > 3) return false;
+            far |= (v[k] < -1 || v[k] > 1);
+         }
+         if (!((G.mask[e] >> m) & 1u) && far) return false;
+      }
+      G.base.push_back(slot_of(v0[e].data()));
+   }
+   return true;
+}
+}  // namespace
+
+// Tiling: outputs of one key in Morton order form member groups (runs of at most
+// kGroupMax siblings, or single outputs where a shared list would not be exact);
+// consecutive groups form a tile while its groups, halo inputs and padded entries fit
+// the kernel limits; tiles grouped by frequency count.
 static void build_tiles(const TileProblem& P, TileSet& S) {
    std::map<int, std::vector<int>> by_key;
    for (int i = 0; i < (int)P.key.size(); i++)
@@ -55,46 +133,76 @@ static void build_tiles(const TileProblem& P, TileSet& S) {
    for (auto& kv : by_key) {
       std::vector<int>& ids = kv.second;
       std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return P.morton[a] < P.morton[b]; });
-      size_t pos = 0;
-      while (pos < ids.size()) {
-         TileDesc tile;
-         tile.ndst = tile.nsrc = tile.npairs = 0;
-         tile.pg = P.pg[ids[pos]];
-         tile.t_off = P.t_base[ids[pos]];
-         tile.dst_off = (int64_t)S.tile_dst.size();
-         tile.src_off = (int64_t)S.tile_src.size();
-         tile.pair_off = (int64_t)S.tile_pairs.size();
-         std::map<int64_t, int> halo;
-         while (pos < ids.size()) {
-            const int o = ids[pos];
-            const int cnt = (int)(P.ptr[o + 1] - P.ptr[o]);
-            int fresh = 0;
-            for (int64_t q = P.ptr[o]; q < P.ptr[o + 1]; q++)
-               if (!halo.count(P.in_off[q])) fresh++;
-            // each destination's list is padded to whole groups of four with the zero slot
-            const int padded = (cnt + 3) & ~3;
-            if (tile.ndst > 0 && (tile.ndst + 1 > kTileMaxDst || tile.nsrc + fresh > kTileMaxSrc ||
-                                  tile.npairs + padded > kTileMaxPairs))
-               break;
-            FFTSVD_REQUIRE(padded <= kTileMaxPairs && fresh <= kTileMaxSrc, "interaction list too long");
-            S.tile_dst.push_back(P.out_off[o]);
-            S.tile_dst_pairs.push_back(make_int2(tile.npairs, padded));
-            for (int64_t q = P.ptr[o]; q < P.ptr[o + 1]; q++) {
-               auto it = halo.find(P.in_off[q]);
-               int h;
-               if (it == halo.end()) {
-                  h = tile.nsrc++;
-                  halo[P.in_off[q]] = h;
-                  S.tile_src.push_back(P.in_off[q]);
-               } else {
-                  h = it->second;
-               }
-               S.tile_pairs.push_back(((uint32_t)h << 16) | (uint32_t)P.slot[q]);
+      std::vector<MemberGroup> groups;
+      for (size_t i = 0; i < ids.size();) {
+         size_t last = i + 1;
+         while (last < ids.size() && (int)(last - i) < kGroupMax && (P.morton[ids[last]] >> 3) == (P.morton[ids[i]] >> 3))
+            last++;
+         MemberGroup G;
+         if (make_group(P, ids, i, last, G)) {
+            groups.push_back(std::move(G));
+         } else {
+            for (size_t k = i; k < last; k++) {
+               FFTSVD_REQUIRE(make_group(P, ids, k, k + 1, G), "interaction outside the 7x7x7 offset range");
+               groups.push_back(std::move(G));
             }
-            for (int q = cnt; q < padded; q++) S.tile_pairs.push_back((uint32_t)kTileZeroSlot);
-            tile.npairs += padded;
-            tile.ndst++;
+         }
+         i = last;
+      }
+      size_t pos = 0;
+      while (pos < groups.size()) {
+         TileDesc tile;
+         tile.ngroups = tile.nsrc = tile.nentries = tile.nmembers = 0;
+         tile.pad = 0;
+         tile.pg = P.pg[groups[pos].members[0]];
+         tile.t_off = P.t_base[groups[pos].members[0]];
+         tile.grp_off = (int64_t)S.tile_grp.size();
+         tile.mem_off = (int64_t)S.tile_dst.size();
+         tile.src_off = (int64_t)S.tile_src.size();
+         tile.ent_off = (int64_t)S.tile_entries.size();
+         std::map<int64_t, int> halo;
+         std::vector<int> tg;
+         while (pos < groups.size()) {
+            const MemberGroup& G = groups[pos];
+            int fresh = 0;
+            for (int64_t in : G.src)
+               if (!halo.count(in)) fresh++;
+            const int padded = ((int)G.src.size() + 3) & ~3;
+            if (!tg.empty() && ((int)tg.size() + 1 > kTileMaxGroups || tile.nsrc + fresh > kTileMaxSrc ||
+                                tile.nentries + padded > kTileMaxEntries))
+               break;
+            FFTSVD_REQUIRE(fresh <= kTileMaxSrc && padded <= kTileMaxEntries, "interaction list too long");
+            for (int64_t in : G.src)
+               if (!halo.count(in)) {
+                  halo[in] = tile.nsrc++;
+                  S.tile_src.push_back(in);
+               }
+            tile.nentries += padded;
+            tg.push_back((int)pos);
             pos++;
+         }
+         // one warp per group: groups by decreasing cost (entries times members plus the
+         // entry overhead), which the kernel deals to its warps in a snake order
+         auto cost = [&](int gi) { return (groups[gi].src.size() + 3) / 4 * (2 + groups[gi].members.size()); };
+         std::stable_sort(tg.begin(), tg.end(), [&](int a, int b) { return cost(a) > cost(b); });
+         int ent = 0;
+         for (int gi : tg) {
+            const MemberGroup& G = groups[gi];
+            const int nm = (int)G.members.size(), ne = ((int)G.src.size() + 3) & ~3;
+            S.tile_grp.push_back(make_int4(ent, ne, tile.nmembers, nm));
+            for (int j = 0; j < nm; j++) {
+               S.tile_dst.push_back(P.out_off[G.members[j]]);
+               S.tile_delta.push_back(G.delta[j] - kEntryBaseBias);
+            }
+            for (size_t e = 0; e < G.src.size(); e++)
+               S.tile_entries.push_back(((uint32_t)halo.at(G.src[e]) << 17) | (G.mask[e] << 9) |
+                                        (uint32_t)(G.base[e] + kEntryBaseBias));
+            // padding: halo row 0 through each member's own (zeroed) offset
+            for (int e = (int)G.src.size(); e < ne; e++)
+               S.tile_entries.push_back((uint32_t)(kCenterSlot + kEntryBaseBias));
+            ent += ne;
+            tile.nmembers += nm;
+            tile.ngroups++;
          }
          S.tiles.push_back(tile);
       }
@@ -111,37 +219,55 @@ static void build_tiles(const TileProblem& P, TileSet& S) {
       TileGroup& g = S.tile_groups.back();
       g.count++;
       g.max_src = std::max(g.max_src, t.nsrc);
-      g.max_pairs = std::max(g.max_pairs, t.npairs);
-      g.max_dst = std::max(g.max_dst, t.ndst);
+      g.max_entries = std::max(g.max_entries, t.nentries);
+      g.max_groups = std::max(g.max_groups, t.ngroups);
+      g.max_members = std::max(g.max_members, t.nmembers);
    }
 }
 
 // Every index the translation kernel forms stays inside its buffers: table rows, the
-// in_elems input spectra and the out_elems output spectra.
+// in_elems input spectra and the out_elems output spectra, and the shared-memory rows.
 static void check_tiles(const TileSet& S, int64_t nt, int64_t in_elems, int64_t out_elems) {
    for (const TileDesc& t : S.tiles) {
-      FFTSVD_REQUIRE(t.ndst > 0 && t.ndst <= kTileMaxDst && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
-                         t.npairs > 0 && t.npairs <= kTileMaxPairs && t.pg > 0,
+      FFTSVD_REQUIRE(t.ngroups > 0 && t.ngroups <= kTileMaxGroups && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
+                         t.nentries > 0 && t.nentries <= kTileMaxEntries && t.nentries % 4 == 0 &&
+                         t.nmembers > 0 && t.nmembers <= kTileMaxGroups * kGroupMax && t.pg > 0 && t.pg % 16 == 0,
                      "tile descriptor");
-      FFTSVD_REQUIRE(t.dst_off + t.ndst <= (int64_t)S.tile_dst.size(), "tile destinations out of range");
+      FFTSVD_REQUIRE(t.grp_off + t.ngroups <= (int64_t)S.tile_grp.size(), "tile groups out of range");
+      FFTSVD_REQUIRE(t.mem_off + t.nmembers <= (int64_t)S.tile_dst.size() &&
+                         t.mem_off + t.nmembers <= (int64_t)S.tile_delta.size(),
+                     "tile members out of range");
       FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)S.tile_src.size(), "tile sources out of range");
-      FFTSVD_REQUIRE(t.pair_off + t.npairs <= (int64_t)S.tile_pairs.size(), "tile pairs out of range");
+      FFTSVD_REQUIRE(t.ent_off + t.nentries <= (int64_t)S.tile_entries.size(), "tile entries out of range");
       FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
-      FFTSVD_REQUIRE(t.pair_off % 4 == 0, "tile pairs not aligned");
-      for (int i = 0; i < t.ndst; i++) {
-         const int2 dp = S.tile_dst_pairs[t.dst_off + i];
-         FFTSVD_REQUIRE(dp.x >= 0 && dp.y >= 0 && dp.x + dp.y <= t.npairs && dp.x % 4 == 0 && dp.y % 4 == 0,
-                        "tile destination pairs out of range");
-         const int64_t so = S.tile_dst[t.dst_off + i];
+      for (int i = 0; i < t.nmembers; i++) {
+         const int64_t so = S.tile_dst[t.mem_off + i];
          FFTSVD_REQUIRE(so >= 0 && so + t.pg <= out_elems, "tile destination spectrum out of range");
       }
       for (int i = 0; i < t.nsrc; i++) {
          const int64_t so = S.tile_src[t.src_off + i];
          FFTSVD_REQUIRE(so >= 0 && so + t.pg <= in_elems, "tile source spectrum out of range");
       }
-      for (int i = 0; i < t.npairs; i++) {
-         const uint32_t pr = S.tile_pairs[t.pair_off + i];
-         FFTSVD_REQUIRE((int)(pr >> 16) < t.nsrc && (pr & 0xffffu) <= (uint32_t)kTileZeroSlot, "tile pair out of range");
+      for (int g = 0; g < t.ngroups; g++) {
+         const int4 gi = S.tile_grp[t.grp_off + g];
+         FFTSVD_REQUIRE(gi.x >= 0 && gi.x % 4 == 0 && gi.y > 0 && gi.y % 4 == 0 && gi.x + gi.y <= t.nentries &&
+                            gi.z >= 0 && gi.w >= 1 && gi.w <= kGroupMax && gi.z + gi.w <= t.nmembers,
+                        "tile group out of range");
+         for (int e = gi.x; e < gi.x + gi.y; e++) {
+            const uint32_t w = S.tile_entries[t.ent_off + e];
+            const int halo = (int)(w >> 17), base = (int)(w & 0x1ffu) - kEntryBaseBias;
+            const uint32_t mask = (w >> 9) & 0xffu;
+            // the kernel reads slot base + delta_j for every member j of the warp's largest
+            // group (delta 0 beyond this group's members): all of them must be table rows
+            FFTSVD_REQUIRE(halo < t.nsrc && (mask >> gi.w) == 0 && base >= 0 && base < 343, "tile entry out of range");
+            for (int j = 0; j < gi.w; j++) {
+               const int slot = base + S.tile_delta[t.mem_off + gi.z + j] + kEntryBaseBias;
+               FFTSVD_REQUIRE(slot >= 0 && slot < 343, "tile entry slot out of range");
+               const int dx = slot / 49 - 3, dy = (slot / 7) % 7 - 3, dz = slot % 7 - 3;
+               const bool local = std::abs(dx) <= 1 && std::abs(dy) <= 1 && std::abs(dz) <= 1;
+               FFTSVD_REQUIRE(local != (((mask >> j) & 1u) != 0), "tile entry reaches a non-interacting member");
+            }
+         }
       }
    }
 }
@@ -395,6 +521,13 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          const int n = T.grid[lvl], Np = 2 * n - 1, pg = Np * Np * n, pgp = pad16(pg);
          FFTSVD_REQUIRE(T.t_level_ptr[lvl + 1] - T.t_level_ptr[lvl] == 343LL * pg, "translation table size mismatch");
          for (int slot = 0; slot < 343; slot++) {
+            // the 27 local offsets (|d| <= 1 on every axis) never interact: zero rows, which the
+            // translation reads for sibling members that do not interact with a shared source
+            const int dx = slot / 49 - 3, dy = (slot / 7) % 7 - 3, dz = slot % 7 - 3;
+            if (std::abs(dx) <= 1 && std::abs(dy) <= 1 && std::abs(dz) <= 1) {
+               L.t_pairs.insert(L.t_pairs.end(), 2 * (size_t)pgp, 0.0);
+               continue;
+            }
             const double* src = T.t_ops + 2 * (T.t_level_ptr[lvl] + (int64_t)slot * pg);
             L.t_pairs.insert(L.t_pairs.end(), src, src + 2 * pg);
             L.t_pairs.insert(L.t_pairs.end(), 2 * (size_t)(pgp - pg), 0.0);
@@ -508,7 +641,8 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       kb.fixed[1] = 4.0 * (double)L.src_panels.size();
       const double sbuf = 2.0 * (double)L.translated_elems;
       kb.elems[2] = spec + (double)L.t_elems + sbuf;                      // spectra, T, translated writes
-      kb.fixed[2] = 4.0 * (double)L.fwd.tile_pairs.size() + 8.0 * (double)(L.fwd.tile_src.size() + L.fwd.tile_dst.size());
+      kb.fixed[2] = 4.0 * (double)(L.fwd.tile_entries.size() + L.fwd.tile_delta.size()) + 16.0 * (double)L.fwd.tile_grp.size() +
+                 8.0 * (double)(L.fwd.tile_src.size() + L.fwd.tile_dst.size());
       kb.elems[3] = sbuf + uti + u + nq;                                  // translated, UTI, U, staging writes
       kb.fixed[3] = 4.0 * (double)L.dst_points.size();
       kb.elems[4] = dpairs + 2.0 * lcols + (double)L.stage_levels * nq;   // D, gathered x, staged far field
@@ -718,8 +852,9 @@ __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
    }
 }
 
-constexpr int kTileRowBytes = 128;                               // shared-memory row per slot/source and chunk
-constexpr int kTranslateThreads = kTileMaxDst * kTileRowBytes / 16;  // one thread per destination unit
+constexpr int kTileRowBytes = 128;                         // shared-memory row per slot/source and chunk
+constexpr int kTileUnits = kTileRowBytes / 16;             // 16-byte units per row: threads per member group
+constexpr int kTranslateThreads = kTileMaxGroups * kTileUnits;
 
 __device__ inline void cp_async16(void* smem, const void* gmem) {
    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -742,6 +877,10 @@ template <> struct Pack16<float> {
       a.z += b.z;
       a.w += b.w;
    }
+   __device__ static inline V shfl_xor(const V& a, int m) {
+      return make_float4(__shfl_xor_sync(0xffffffffu, a.x, m), __shfl_xor_sync(0xffffffffu, a.y, m),
+                         __shfl_xor_sync(0xffffffffu, a.z, m), __shfl_xor_sync(0xffffffffu, a.w, m));
+   }
    __device__ static inline void fma(V& acc, const V& a, const V& b) {  // acc += a * b, two complex
       acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
       acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
@@ -756,21 +895,62 @@ template <> struct Pack16<double> {
       a.x += b.x;
       a.y += b.y;
    }
+   __device__ static inline V shfl_xor(const V& a, int m) {
+      return make_double2(__shfl_xor_sync(0xffffffffu, a.x, m), __shfl_xor_sync(0xffffffffu, a.y, m));
+   }
    __device__ static inline void fma(V& acc, const V& a, const V& b) {
       acc.x = ::fma(a.x, b.x, ::fma(-a.y, b.y, acc.x));
       acc.y = ::fma(a.x, b.y, ::fma(a.y, b.x, acc.y));
    }
 };
 
+// One member group's part of one frequency chunk, one warp per group: lane = (entry
+// phase p = lane / 8, 16-byte unit u = lane % 8).  Phase p takes the entry pairs
+// p, p + 4, p + 8, ... of the group's list; for each entry it reads the source unit
+// from shared memory once and applies it to all NM members of the group.  Members are
+// siblings, so every source of the group lies within three cubes of each member and
+// base + delta_j is always a table row; for a member that does not interact with the
+// source it is one of the 27 local-offset rows, which hold zeros.  Padding entries
+// point at the zero row of each member's own offset.  The loop therefore has no
+// branches.  Shared entry word: bits 20-31 halo row in 16-byte units, bits 0-11
+// (base slot + bias) in 16-byte units; dj[j] is member j's (delta - bias) in bytes.
+// The four phase partials are summed with shuffles in a fixed order.
+template <typename T, int NM>
+__device__ __forceinline__ void translate_group(uint32_t tsu, uint32_t fsu, uint32_t es, int npairs, int phase,
+                                                const int (&dj)[kGroupMax], typename Pack16<T>::V (&acc)[kGroupMax]) {
+   using V = typename Pack16<T>::V;
+   extern __shared__ __align__(16) char smem_raw[];
+   for (int q = phase; q < npairs; q += 4) {
+      const uint2 w2 = *reinterpret_cast<const uint2*>(smem_raw + es + (uint32_t)q * 8u);
+      const uint32_t ws[2] = {w2.x, w2.y};
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+         const uint32_t w = ws[e];
+         const V f = *reinterpret_cast<const V*>(smem_raw + fsu + ((w >> 16) & 0xfff0u));
+         const uint32_t tb = tsu + ((w << 4) & 0xfff0u);
+#pragma unroll
+         for (int j = 0; j < NM; j++)
+            Pack16<T>::fma(acc[j], *reinterpret_cast<const V*>(smem_raw + (tb + (uint32_t)dj[j])), f);
+      }
+   }
+#pragma unroll
+   for (int j = 0; j < NM; j++) {
+      Pack16<T>::add(acc[j], Pack16<T>::shfl_xor(acc[j], 8));
+      Pack16<T>::add(acc[j], Pack16<T>::shfl_xor(acc[j], 16));
+   }
+}
+
 // One block per (tile, range of frequency chunks): S[d][f] = sum over the
 // interactions of destination d of T[slot][f] * F[source][f] (Cube_multiply_T,
-// Cube.c:2062-2111).  The chunk of all 343 translation slots of the tile's tree
-// and level and the chunk of every halo source spectrum are copied to shared
-// memory with cp.async, one chunk ahead of the computation (double buffer), so
-// each table entry and spectrum crosses L2 once per tile instead of once per
-// interaction.  Rows are padded to a multiple of 16 complex values, so every
-// copy is a full aligned 16 bytes.  Each thread owns one 16-byte unit of one
-// destination's kTileRowBytes row.
+// Cube.c:2062-2111).  The chunk of all 343 translation slots of the tile's tree and
+// level and the chunk of every halo source spectrum are copied to shared memory with
+// cp.async, so each table entry and spectrum crosses L2 once per tile instead of
+// once per interaction; two blocks per SM overlap one's copies with the other's
+// arithmetic.  Rows are padded to a multiple of 16 complex values, so every copy is
+// a full aligned 16 bytes.  Each warp takes member groups of the tile in turn: the
+// groups are ordered by cost and dealt to the warps in a snake order, so the warps of
+// a block finish together.  A warp keeps one accumulator per member, so each source
+// unit read from shared memory serves every sibling of the group.
 //
 // Single right-hand side: a row is kTileRowBytes of consecutive frequencies of
 // one spectrum (8 units); the slot rows are as wide.
@@ -779,14 +959,15 @@ template <> struct Pack16<double> {
 // right-hand sides, and a slot row is the single unit of those frequencies, read
 // once and applied to all 8.
 template <typename T, bool BATCH>
-__global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
+__global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
     const TileDesc* __restrict__ tiles, const int64_t* __restrict__ tile_src, const int64_t* __restrict__ tile_dst,
-    const int2* __restrict__ tile_dst_pairs, const uint32_t* __restrict__ tile_pairs,
-    const typename Vec2<T>::type* __restrict__ tops, const typename Vec2<T>::type* __restrict__ spectra,
-    typename Vec2<T>::type* __restrict__ S, int chunks_per_block, BatchStrides bs) {
+    const int32_t* __restrict__ tile_delta, const int4* __restrict__ tile_grp,
+    const uint32_t* __restrict__ tile_entries, const typename Vec2<T>::type* __restrict__ tops,
+    const typename Vec2<T>::type* __restrict__ spectra, typename Vec2<T>::type* __restrict__ S,
+    int chunks_per_block, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
    using V = typename Pack16<T>::V;
-   constexpr int U = kTileRowBytes / 16;                          // 16-byte units per row
+   constexpr int U = kTileUnits;                                  // 16-byte units per row
    constexpr int PER16 = 16 / (int)sizeof(T2);                    // complex values per unit
    constexpr int CH = BATCH ? PER16 : kTileRowBytes / (int)sizeof(T2);  // frequencies per chunk
    constexpr int TU = BATCH ? 1 : U;                              // units per slot row
@@ -801,88 +982,83 @@ __global__ void __launch_bounds__(kTranslateThreads, 1) translate_kernel(
    if (kbeg >= nchunks) return;
    const int kend = min(nchunks, kbeg + chunks_per_block);
    char* p = smem_raw;
-   V* Tb0 = carve<V>(p, (kTileZeroSlot + 1) * TU);  // 343 slots and the zero row
-   V* Tb1 = carve<V>(p, (kTileZeroSlot + 1) * TU);
-   V* Fb0 = carve<V>(p, t.nsrc * U);
-   V* Fb1 = carve<V>(p, t.nsrc * U);
-   uint32_t* pairs = carve<uint32_t>(p, t.npairs);
-   int2* dinfo = carve<int2>(p, t.ndst);
+   V* Tb = carve<V>(p, 343 * TU);
+   V* Fb = carve<V>(p, t.nsrc * U);
+   uint32_t* ent = carve<uint32_t>(p, t.nentries);
+   int4* grp = carve<int4>(p, t.ngroups);
+   int64_t* dstoff = carve<int64_t>(p, t.nmembers);
+   int* delta = carve<int>(p, t.nmembers);
    int64_t* srcoff = carve<int64_t>(p, t.nsrc);
-   int64_t* dstoff = carve<int64_t>(p, t.ndst);
-   // pairs pre-scaled to byte offsets in the row buffers: (source row << 16) | slot row
-   // (at most 255 * U * 16 and 343 * TU * 16, both below 65536)
-   for (int i = threadIdx.x; i < t.npairs; i += blockDim.x) {
-      const uint32_t pr = tile_pairs[t.pair_off + i];
-      pairs[i] = ((pr >> 16) * (uint32_t)(U * 16)) << 16 | ((pr & 0xffffu) * (uint32_t)(TU * 16));
+   // entries re-encoded with row offsets in 16-byte units (halo <= 319 rows of U units,
+   // base + bias <= 511 rows of TU units: both below 4096)
+   for (int i = threadIdx.x; i < t.nentries; i += blockDim.x) {
+      const uint32_t w = tile_entries[t.ent_off + i];
+      ent[i] = (((w >> 17) * (uint32_t)U) << 20) | ((w & 0x1ffu) * (uint32_t)TU);
    }
-   for (int i = threadIdx.x; i < t.ndst; i += blockDim.x) {
-      dinfo[i] = tile_dst_pairs[t.dst_off + i];
-      dstoff[i] = tile_dst[t.dst_off + i];
+   for (int i = threadIdx.x; i < t.ngroups; i += blockDim.x) grp[i] = tile_grp[t.grp_off + i];
+   for (int i = threadIdx.x; i < t.nmembers; i += blockDim.x) {
+      dstoff[i] = tile_dst[t.mem_off + i];
+      delta[i] = tile_delta[t.mem_off + i] * TU * 16;
    }
    for (int i = threadIdx.x; i < t.nsrc; i += blockDim.x) srcoff[i] = tile_src[t.src_off + i];
-   for (int i = threadIdx.x; i < TU; i += blockDim.x) {
-      Tb0[kTileZeroSlot * TU + i] = Pack16<T>::zero();
-      Tb1[kTileZeroSlot * TU + i] = Pack16<T>::zero();
-   }
-   __syncthreads();
-   auto stage = [&](int k, V* Tb, V* Fb) {
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+   const int u = lane & (U - 1), phase = lane / U;
+   // all shared accesses below are smem_raw plus a byte offset, so they compile to
+   // shared-window loads
+   const uint32_t tsu = (uint32_t)((const char*)Tb - smem_raw) + (BATCH ? 0u : (uint32_t)u * 16u);
+   const uint32_t fsu = (uint32_t)((const char*)Fb - smem_raw) + (uint32_t)u * 16u;
+   const uint32_t es0 = (uint32_t)((const char*)ent - smem_raw);
+   for (int k = kbeg; k < kend; k++) {
       const int f0 = k * CH;
-      for (int i = threadIdx.x; i < kTileZeroSlot * TU; i += blockDim.x) {
-         const int s = i / TU, u = i % TU;
-         cp_async16(&Tb[i], &tops[t.t_off + (int64_t)s * t.pg + f0 + u * PER16]);
+      __syncthreads();  // metadata written / the previous chunk's rows consumed
+      for (int i = threadIdx.x; i < 343 * TU; i += blockDim.x) {
+         const int s = i / TU, uu = i % TU;
+         cp_async16(&Tb[i], &tops[t.t_off + (int64_t)s * t.pg + f0 + uu * PER16]);
       }
       for (int i = threadIdx.x; i < t.nsrc * U; i += blockDim.x) {
-         const int s = i / U, u = i % U;
+         const int s = i / U, uu = i % U;
          if (BATCH)
-            cp_async16(&Fb[i], &spectra[u * bs.spectra + srcoff[s] + f0]);
+            cp_async16(&Fb[i], &spectra[uu * bs.spectra + srcoff[s] + f0]);
          else
-            cp_async16(&Fb[i], &spectra[srcoff[s] + f0 + u * PER16]);
+            cp_async16(&Fb[i], &spectra[srcoff[s] + f0 + uu * PER16]);
       }
       cp_async_commit();
-   };
-   stage(kbeg, Tb0, Fb0);
-   for (int k = kbeg; k < kend; k++) {
-      const bool odd = (k - kbeg) & 1;
-      if (k + 1 < kend) {
-         stage(k + 1, odd ? Tb0 : Tb1, odd ? Fb0 : Fb1);
-         cp_async_wait<1>();
-      } else {
-         cp_async_wait<0>();
-      }
+      cp_async_wait<0>();
       __syncthreads();
-      // all shared accesses below are smem_raw plus a byte offset, so they compile to
-      // shared-window loads
-      const uint32_t ts = (uint32_t)((const char*)(odd ? Tb1 : Tb0) - smem_raw);
-      const uint32_t fs = (uint32_t)((const char*)(odd ? Fb1 : Fb0) - smem_raw);
-      const uint32_t ps = (uint32_t)((const char*)pairs - smem_raw);
-      const int f0 = k * CH;
-      // thread -> (destination, unit)
-      for (int item = threadIdx.x; item < t.ndst * U; item += blockDim.x) {
-         const int d = item / U, u = item % U;
-         const char* tsu = smem_raw + ts + (BATCH ? 0u : (uint32_t)u * 16u);
-         const char* fsu = smem_raw + fs + (uint32_t)u * 16u;
-         const int2 di = dinfo[d];
-         V acc = Pack16<T>::zero(), acc1 = Pack16<T>::zero();  // two chains of dependent FMAs
-         // four pairs per 16-byte load; lists are padded to groups of four with the zero row
-         const uint4* pp = reinterpret_cast<const uint4*>(smem_raw + ps + (uint32_t)di.x * 4u);
-         for (int q = 0; q < (di.y >> 2); q++) {
-            const uint4 pr = pp[q];
-            Pack16<T>::fma(acc, *reinterpret_cast<const V*>(tsu + (pr.x & 0xffffu)),
-                           *reinterpret_cast<const V*>(fsu + (pr.x >> 16)));
-            Pack16<T>::fma(acc1, *reinterpret_cast<const V*>(tsu + (pr.y & 0xffffu)),
-                           *reinterpret_cast<const V*>(fsu + (pr.y >> 16)));
-            Pack16<T>::fma(acc, *reinterpret_cast<const V*>(tsu + (pr.z & 0xffffu)),
-                           *reinterpret_cast<const V*>(fsu + (pr.z >> 16)));
-            Pack16<T>::fma(acc1, *reinterpret_cast<const V*>(tsu + (pr.w & 0xffffu)),
-                           *reinterpret_cast<const V*>(fsu + (pr.w >> 16)));
+      // groups in cost order, dealt to the warps in a snake order
+      for (int r = 0;; r++) {
+         const int gidx = r * nwarps + ((r & 1) ? nwarps - 1 - warp : warp);
+         if (gidx >= t.ngroups) break;
+         const int4 gi = grp[gidx];
+         int dj[kGroupMax];
+#pragma unroll
+         for (int j = 0; j < kGroupMax; j++) dj[j] = j < gi.w ? delta[gi.z + j] : 0;
+         V acc[kGroupMax];
+#pragma unroll
+         for (int j = 0; j < kGroupMax; j++) acc[j] = Pack16<T>::zero();
+         const uint32_t es = es0 + (uint32_t)gi.x * 4u;
+         const int np = gi.y >> 1;
+         switch (gi.w) {
+            case 1: translate_group<T, 1>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 2: translate_group<T, 2>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 3: translate_group<T, 3>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 4: translate_group<T, 4>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 5: translate_group<T, 5>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 6: translate_group<T, 6>(tsu, fsu, es, np, phase, dj, acc); break;
+            case 7: translate_group<T, 7>(tsu, fsu, es, np, phase, dj, acc); break;
+            default: translate_group<T, 8>(tsu, fsu, es, np, phase, dj, acc); break;
          }
-         Pack16<T>::add(acc, acc1);
-         if (BATCH)
-            *reinterpret_cast<V*>(&S[u * bs.translated + dstoff[d] + f0]) = acc;
-         else
-            *reinterpret_cast<V*>(&S[dstoff[d] + f0 + u * PER16]) = acc;
+         // phase p writes the members j = p, p + 4 (every lane holds the sums)
+#pragma unroll
+         for (int j = 0; j < kGroupMax; j++)
+            if (j < gi.w && (j & 3) == phase) {
+               const int64_t o = dstoff[gi.z + j];
+               if (BATCH)
+                  *reinterpret_cast<V*>(&S[u * bs.translated + o + f0]) = acc[j];
+               else
+                  *reinterpret_cast<V*>(&S[o + f0 + u * PER16]) = acc[j];
+            }
       }
-      __syncthreads();  // this buffer is refilled by the stage issued in the next iteration
    }
 }
 
@@ -1839,6 +2015,8 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    int dev = 0, optin = 0;
    FFTSVD_CUDA(cudaGetDevice(&dev));
    FFTSVD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+   FFTSVD_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+   sm_count_ = std::max(sm_count_, 1);
    // one warp per leaf; as many leaves per block (up to four) as the gathered columns allow
    near_stride_ = maxcols;
    near_warps_ = (int)std::max<size_t>(1, std::min<size_t>(kNearThreads / 32, (size_t)optin / (maxcols * sizeof(T2))));
@@ -1881,11 +2059,11 @@ void DeviceOperator<T>::enable_timing(bool on) {
 
 template <typename T>
 int DeviceOperator<T>::translate_smem(const TileGroup& g, bool batch) const {
-   // two chunk rows per slot (and the zero row) and per halo source, pairs, per-destination
-   // {begin, count} and offsets, halo offsets; each carve aligned to 16 bytes
+   // one chunk row per slot and per halo source, entries, groups, member offsets and
+   // deltas, halo offsets; each carve aligned to 16 bytes
    const size_t slot_row = batch ? 16 : kTileRowBytes;
-   return (int)(2 * (kTileZeroSlot + 1) * slot_row + (size_t)2 * g.max_src * kTileRowBytes +
-                (size_t)g.max_pairs * sizeof(uint32_t) + (size_t)g.max_dst * (sizeof(int2) + sizeof(int64_t)) +
+   return (int)(343 * slot_row + (size_t)g.max_src * kTileRowBytes + (size_t)g.max_entries * sizeof(uint32_t) +
+                (size_t)g.max_groups * sizeof(int4) + (size_t)g.max_members * (sizeof(int64_t) + sizeof(int)) +
                 (size_t)g.max_src * sizeof(int64_t) + 128);
 }
 
@@ -1930,30 +2108,39 @@ void DeviceOperator<T>::DevTiles::upload(const TileSet& S) {
    tiles.upload(S.tiles);
    src.upload(S.tile_src);
    dst.upload(S.tile_dst);
-   dst_pairs.upload(S.tile_dst_pairs);
-   pairs.upload(S.tile_pairs);
+   delta.upload(S.tile_delta);
+   grp.upload(S.tile_grp);
+   entries.upload(S.tile_entries);
    groups = S.tile_groups;
 }
 
 template <typename T>
 void DeviceOperator<T>::launch_translate_tiles(const DevTiles& tl, const TileGroup& g, const T2* in, T2* out,
                                                int nrhs, const BatchStrides& bs, cudaStream_t stream) {
-   // split each tile's frequency chunks over several blocks so that even the few
-   // tiles of the coarse levels fill the device (about eight blocks per SM in total)
+   // split each tile's frequency chunks over blocks of cpb chunks each: the split with
+   // the fewest chunk times over all waves of resident blocks (two per SM), the
+   // smallest such cpb (more blocks fill the device better at the coarse levels)
    const bool batch = nrhs > 1;
    const int groups = batch ? nrhs / kBatchGroup : 1;
    const int nchunks = g.pg / (batch ? 16 / (int)sizeof(T2) : kTileRowBytes / (int)sizeof(T2));
-   const int64_t total = (int64_t)g.count * nchunks * groups;
-   const int cpb = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, total / (8 * 148)));
+   const int64_t slots = 2LL * sm_count_;
+   int cpb = 1;
+   int64_t best = -1;
+   for (int c = 1; c <= nchunks; c++) {
+      const int64_t blocks = (int64_t)g.count * ((nchunks + c - 1) / c) * groups;
+      const int64_t cost = (blocks + slots - 1) / slots * c;
+      if (best < 0 || cost < best) best = cost, cpb = c;
+   }
    const dim3 grid(g.count, (nchunks + cpb - 1) / cpb, groups);
+   const int threads = std::min(kTranslateThreads, 32 * g.max_groups);  // up to one warp per member group
    if (batch)
-      translate_kernel<T, true><<<grid, kTranslateThreads, translate_smem(g, true), stream>>>(
-          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.dst_pairs.get(), tl.pairs.get(), t_.get(), in, out,
-          cpb, bs);
+      translate_kernel<T, true><<<grid, threads, translate_smem(g, true), stream>>>(
+          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.delta.get(), tl.grp.get(), tl.entries.get(),
+          t_.get(), in, out, cpb, bs);
    else
-      translate_kernel<T, false><<<grid, kTranslateThreads, translate_smem(g, false), stream>>>(
-          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.dst_pairs.get(), tl.pairs.get(), t_.get(), in, out,
-          cpb, bs);
+      translate_kernel<T, false><<<grid, threads, translate_smem(g, false), stream>>>(
+          tl.tiles.get() + g.begin, tl.src.get(), tl.dst.get(), tl.delta.get(), tl.grp.get(), tl.entries.get(),
+          t_.get(), in, out, cpb, bs);
    FFTSVD_CHECK_LAUNCH();
 }
 
@@ -2195,8 +2382,8 @@ size_t DeviceOperator<T>::device_bytes() const {
           leaf_rows_.bytes() + leaf_cols_.bytes() + d_.bytes() + src_.bytes() + src_panels_.bytes() +
           vt_.bytes() + pv_.bytes() + dst_.bytes() + dst_points_.bytes() + uti_.bytes() + u_.bytes() +
           t_.bytes() + spectra_.bytes() + staging_.bytes() + fwd_.tiles.bytes() + fwd_.src.bytes() +
-          fwd_.dst.bytes() + fwd_.dst_pairs.bytes() + fwd_.pairs.bytes() + translated_.bytes() + adj_.tiles.bytes() +
-          adj_.src.bytes() + adj_.dst.bytes() + adj_.dst_pairs.bytes() + adj_.pairs.bytes() + zt_.bytes() +
+          fwd_.dst.bytes() + fwd_.delta.bytes() + fwd_.grp.bytes() + fwd_.entries.bytes() + translated_.bytes() + adj_.tiles.bytes() +
+          adj_.src.bytes() + adj_.dst.bytes() + adj_.delta.bytes() + adj_.grp.bytes() + adj_.entries.bytes() + zt_.bytes() +
           ut_.bytes() + staget_.bytes();
 }
 

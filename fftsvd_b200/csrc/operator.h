@@ -46,33 +46,46 @@ struct DstDesc {        // one far-field destination cube (points > 0, column ra
    int64_t s_off;       // into the translated spectra, (2n-1)^2 n complex
 };
 
-// Translation tile: destination cubes of one tree and level that share a halo
-// of source spectra; all of them, the halo and the level's 343 translation
-// slots are staged through shared memory one frequency chunk at a time.
+// Translation tile: sibling destination cubes (outputs) of one tree and level, in
+// member groups of up to kGroupMax siblings, that share a halo of source spectra.
+// The halo and the level's 343 translation slots are staged through shared memory
+// one frequency chunk at a time.  A group's sources are listed once (the union of
+// its members' interaction lists); one entry carries the halo row, the mask of the
+// members that interact with that source and a base slot.  The slot of member j is
+// base + delta_j, because a slot is a linear function of the offset between the two
+// cubes (slot = ((dx+3)*7 + (dy+3))*7 + dz+3 for output minus input).
 struct TileDesc {
-   int32_t ndst;        // destinations in the tile
+   int32_t ngroups;     // member groups (one thread row each)
    int32_t nsrc;        // halo sources
-   int32_t npairs;      // (destination, source) interactions
-   int32_t pg;          // frequencies per cube, (2n-1)^2 n
-   int64_t dst_off;     // into tile_dst (S offsets) and tile_dst_pairs
+   int32_t nentries;    // (group, source) entries, each group's list padded to a multiple of four
+   int32_t nmembers;    // outputs in the tile
+   int32_t pg;          // frequencies per cube, (2n-1)^2 n padded to 16
+   int32_t pad;
+   int64_t grp_off;     // into tile_grp
+   int64_t mem_off;     // into tile_dst and tile_delta
    int64_t src_off;     // into tile_src (spectrum offsets)
-   int64_t pair_off;    // into tile_pairs: packed (halo index << 16) | slot, grouped per destination,
-                        // each destination's list padded to a multiple of four
+   int64_t ent_off;     // into tile_entries
    int64_t t_off;       // translation table of slot 0 of this tree and level (complex elements)
 };
 
 struct TileGroup {      // tiles with the same frequency count, one launch
    int pg = 0;
    int begin = 0, count = 0;
-   int max_src = 0, max_pairs = 0, max_dst = 0;
+   int max_src = 0, max_entries = 0, max_groups = 0, max_members = 0;
 };
+
+// Entry word: bits 0-8 base slot + kEntryBaseBias, bits 9-16 member mask, bits 17-31 halo row.
+constexpr int kEntryBaseBias = 64;
+constexpr int kGroupMax = 8;
 
 // Tiles of one translation direction, as uploaded.
 struct TileSet {
    std::vector<TileDesc> tiles;
    std::vector<int64_t> tile_src, tile_dst;
-   std::vector<int2> tile_dst_pairs;   // {begin, count} relative to the tile's pair_off
-   std::vector<uint32_t> tile_pairs;
+   std::vector<int32_t> tile_delta;    // per member: slot of the member = entry base + delta
+   std::vector<int4> tile_grp;         // per group: {entry begin, entry count, member begin, member count},
+                                       // relative to the tile's ent_off and mem_off
+   std::vector<uint32_t> tile_entries;
    std::vector<TileGroup> tile_groups;
 };
 
@@ -92,11 +105,9 @@ struct TileProblem {
    void add_pair(int64_t in, int slot);
 };
 
-constexpr int kTileMaxDst = 64;
-constexpr int kTileMaxSrc = 256;
-constexpr int kTileMaxPairs = 4096;
-constexpr int kTileChunk = 16;  // frequencies per shared-memory chunk
-constexpr int kTileZeroSlot = 343;  // all-zero translation row that pads pair lists to groups of four
+constexpr int kTileMaxGroups = 32;   // thread rows per block
+constexpr int kTileMaxSrc = 320;
+constexpr int kTileMaxEntries = 3072;
 
 struct LeafDesc {       // one leaf with points
    int32_t row_off;     // into leaf_rows
@@ -248,6 +259,7 @@ class DeviceOperator {
    void launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream);
    bool warp_path(const LaunchGroup& g) const;
    int warp_min_cubes_ = kWarpMinCubes;
+   int sm_count_ = 148;
    int64_t spectra_elems_ = 1, translated_elems_ = 1;
    int batch_capacity_ = 0;
    DevBuf<T2> xsd_b_, spectra_b_, translated_b_;
@@ -271,8 +283,9 @@ class DeviceOperator {
    struct DevTiles {
       DevBuf<TileDesc> tiles;
       DevBuf<int64_t> src, dst;
-      DevBuf<int2> dst_pairs;
-      DevBuf<uint32_t> pairs;
+      DevBuf<int32_t> delta;
+      DevBuf<int4> grp;
+      DevBuf<uint32_t> entries;
       std::vector<TileGroup> groups;
       void upload(const TileSet& S);
    };
