@@ -1600,7 +1600,7 @@ __device__ inline typename Vec2<T>::type shfl_c(typename Vec2<T>::type v, int sr
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forward_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forward_n4_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
@@ -1633,6 +1633,19 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forw
       for (int j = 0; j < N; j++) w2[sl][j] = tw[((j + OFF) * (jp + 4 * sl)) % Np];
 #pragma unroll
    for (int q = 0; q < Np; q++) W[q] = tw[q];
+   // FP64: the first PF rows of PV (they depend only on the cube) are in flight during
+   // VT x (FP32 keeps its registers for occupancy instead)
+   constexpr int PF = sizeof(T) == 8 ? 4 : 0;
+   const T2* pvc = pv + c.pv_off + lane;
+   T2 pf0[PF > 0 ? PF : 1], pf1[PF > 0 ? PF : 1];
+#pragma unroll
+   for (int j = 0; j < PF; j++) {
+      pf0[j] = pf1[j] = Cx<T>::make(T(0), T(0));
+      if (j < r) {
+         pf0[j] = pvc[(int64_t)j * N3];
+         pf1[j] = pvc[(int64_t)j * N3 + 32];
+      }
+   }
    // a = VT x
    T as = T(0), ad = T(0);
    const T* row = vt + c.vt_off + (int64_t)min(lane, r - 1) * m;
@@ -1652,9 +1665,15 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forw
    }
    // grid charges at q = lane and lane + 32
    T g0 = T(0), g1 = T(0);
-   const T2* pvc = pv + c.pv_off + lane;
+#pragma unroll
+   for (int j = 0; j < PF; j++)
+      if (j < r) {
+         const T s = __shfl_sync(kAll, as, j), d = __shfl_sync(kAll, ad, j);
+         g0 += pf0[j].x * s + pf0[j].y * d;
+         g1 += pf1[j].x * s + pf1[j].y * d;
+      }
 #pragma unroll 4
-   for (int j = 0; j < r; j++) {
+   for (int j = PF; j < r; j++) {
       const T s = __shfl_sync(kAll, as, j), d = __shfl_sync(kAll, ad, j);
       const T2 w0 = pvc[(int64_t)j * N3], w1v = pvc[(int64_t)j * N3 + 32];
       g0 += w0.x * s + w0.y * d;
@@ -1712,7 +1731,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_forw
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 6 : 4) far_backward_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_backward_n4_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
