@@ -160,24 +160,20 @@ int Surface::gmres_batch(int precision, int ncols, const double* rhs, double* x,
          dots_partial_kernel<<<dim3(nd, nvec, ncols), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, B.w.get(),
                                                                                  B.partial.get(), n, pcol);
          FFTSVD_CHECK_LAUNCH();
-         reduce_partial_kernel<<<dim3(nvec, 1, ncols), 256, 0, stream>>>(nvec, nd, B.partial.get(), B.h1.get(), 0,
-                                                                         pcol, cap);
-         FFTSVD_CHECK_LAUNCH();
-         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h1.get(), B.w.get(),
-                                                                        B.w.get(), nullptr, n, 0, cap);
+         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.partial.get(), nd,
+                                                                        B.h1.get(), B.w.get(), B.w.get(), nullptr, n,
+                                                                        pcol, 0, cap);
          FFTSVD_CHECK_LAUNCH();
          dots_partial_kernel<<<dim3(nd, nvec, ncols), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, B.w.get(),
                                                                                  B.partial.get(), n, pcol);
          FFTSVD_CHECK_LAUNCH();
-         reduce_partial_kernel<<<dim3(nvec, 1, ncols), 256, 0, stream>>>(nvec, nd, B.partial.get(), B.h2.get(), 0,
-                                                                         pcol, cap);
+         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.partial.get(), nd,
+                                                                        B.h2.get(), B.w.get(), vnext,
+                                                                        B.normpart.get(), n, pcol, nb, cap);
          FFTSVD_CHECK_LAUNCH();
-         update_kernel<<<dim3(nb, 1, ncols), kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, B.h2.get(), B.w.get(),
-                                                                        vnext, B.normpart.get(), n, nb, cap);
-         FFTSVD_CHECK_LAUNCH();
-         givens_kernel<<<ncols, 256, 0, stream>>>(i, cap, B.H.get(), B.h1.get(), B.h2.get(), B.normpart.get(), nb,
-                                                  B.cs.get(), B.sn.get(), B.g.get(), B.st.get(), cap, nb,
-                                                  B.active.get());
+         givens_kernel<<<ncols, 256, givens_smem(i), stream>>>(i, cap, B.H.get(), B.h1.get(), B.h2.get(),
+                                                               B.normpart.get(), nb, B.cs.get(), B.sn.get(), B.g.get(),
+                                                               B.st.get(), cap, nb, B.active.get());
          FFTSVD_CHECK_LAUNCH();
          scale_kernel<<<dim3(ew_blocks, 1, ncols), 256, 0, stream>>>(n, vnext, &B.st.get()->inv_beta, 0.0, vnext, n,
                                                                   fcol);

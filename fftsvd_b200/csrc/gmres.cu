@@ -90,17 +90,28 @@ __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restri
 }
 
 __global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec, const double* __restrict__ V,
-                                                             int64_t ldv, const double* __restrict__ h,
+                                                             int64_t ldv, const double* __restrict__ partial,
+                                                             int nblk, double* __restrict__ h_out,
                                                              const double* __restrict__ w, double* __restrict__ out,
                                                              double* __restrict__ norm_partial, int64_t col,
-                                                             int64_t pcol, int64_t hcol) {
+                                                             int64_t dcol, int64_t pcol, int64_t hcol) {
    extern __shared__ double hs[];  // [nvec]
    __shared__ double red[kVecThreads / 32];
    V += blockIdx.z * col;
    w += blockIdx.z * col;
    out += blockIdx.z * col;
-   h += blockIdx.z * hcol;
-   for (int j = threadIdx.x; j < nvec; j += blockDim.x) hs[j] = h[j];
+   partial += blockIdx.z * dcol;
+   // coefficients: h[j] = sum of the nblk chunk partials of dot j, one warp per j, fixed order
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+   for (int j = warp; j < nvec; j += nwarps) {
+      double s = 0.0;
+      for (int b = lane; b < nblk; b += 32) s += partial[(int64_t)j * nblk + b];
+      s = warp_sum_d(s);
+      if (lane == 0) {
+         hs[j] = s;
+         if (blockIdx.x == 0) h_out[blockIdx.z * hcol + j] = s;
+      }
+   }
    __syncthreads();
    const int64_t k = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
    double x = 0.0;
@@ -148,6 +159,7 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                               GivensState* __restrict__ st, int64_t hcol, int64_t pcol,
                               const int32_t* __restrict__ active) {
+   extern __shared__ double gsh[];  // the new column (i + 2), then the previous rotations cs[i], sn[i]
    __shared__ double red[256];
    // column blockIdx.x of a batch: its own Hessenberg (ldh x ldh), rotations, g and state
    const int colx = blockIdx.x;
@@ -163,43 +175,55 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
       if (threadIdx.x == 0) st->inv_beta = 0.0;
       return;
    }
+   double* colv = gsh;
+   double* css = gsh + i + 2;
+   double* sns = css + i;
    double s = 0.0;
    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += norm_partial[b];
    red[threadIdx.x] = s;
-   __syncthreads();
+   // the column and the rotations are loaded in parallel; the rotations then run in shared memory
+   bool bad = false;
+   for (int j = threadIdx.x; j <= i; j += blockDim.x) {
+      colv[j] = h1[j] + h2[j];
+      bad = bad || !isfinite(colv[j]);
+   }
+   for (int k = threadIdx.x; k < i; k += blockDim.x) {
+      css[k] = cs[k];
+      sns[k] = sn[k];
+   }
+   const int any_bad = __syncthreads_or(bad);
    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
       if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
       __syncthreads();
    }
-   if (threadIdx.x != 0) return;
-   const double beta = sqrt(red[0]);
-   double* col = H + (int64_t)i * ldh;
-   bool finite = isfinite(beta);
-   for (int j = 0; j <= i; j++) {
-      col[j] = h1[j] + h2[j];
-      finite = finite && isfinite(col[j]);
+   if (threadIdx.x == 0) {
+      const double beta = sqrt(red[0]);
+      const bool finite = isfinite(beta) && !any_bad;
+      colv[i + 1] = beta;
+      for (int k = 0; k < i; k++) rotate(css[k], sns[k], &colv[k], &colv[k + 1]);
+      // GMRES.c:3-15
+      double c, sv;
+      if (colv[i + 1] == 0.0) {
+         c = 1.0;
+         sv = 0.0;
+      } else {
+         const double r1 = fabs(colv[i]), r2 = fabs(colv[i + 1]);
+         const double len = sqrt(r1 * r1 + r2 * r2);
+         c = colv[i] / len;
+         sv = -colv[i + 1] / len;
+      }
+      cs[i] = c;
+      sn[i] = sv;
+      rotate(c, sv, &colv[i], &colv[i + 1]);
+      g[i + 1] = 0.0;
+      rotate(c, sv, &g[i], &g[i + 1]);
+      st->residual = fabs(g[i + 1]) / st->normr;
+      st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
+      st->flag = !finite ? 2 : (beta == 0.0 ? 1 : 0);
    }
-   col[i + 1] = beta;
-   for (int k = 0; k < i; k++) rotate(cs[k], sn[k], &col[k], &col[k + 1]);
-   // GMRES.c:3-15
-   double c, sv;
-   if (col[i + 1] == 0.0) {
-      c = 1.0;
-      sv = 0.0;
-   } else {
-      const double r1 = fabs(col[i]), r2 = fabs(col[i + 1]);
-      const double len = sqrt(r1 * r1 + r2 * r2);
-      c = col[i] / len;
-      sv = -col[i + 1] / len;
-   }
-   cs[i] = c;
-   sn[i] = sv;
-   rotate(c, sv, &col[i], &col[i + 1]);
-   g[i + 1] = 0.0;
-   rotate(c, sv, &g[i], &g[i + 1]);
-   st->residual = fabs(g[i + 1]) / st->normr;
-   st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
-   st->flag = !finite ? 2 : (beta == 0.0 ? 1 : 0);
+   __syncthreads();
+   double* colh = H + (int64_t)i * ldh;
+   for (int j = threadIdx.x; j <= i + 1; j += blockDim.x) colh[j] = colv[j];
 }
 
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,

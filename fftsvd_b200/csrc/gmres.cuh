@@ -30,11 +30,15 @@ __global__ void dots_partial_kernel(int64_t n, int nvec, const double* __restric
 // out[j] = (accumulate ? out[j] : 0) + sum_b partial[j * nblk + b]; one block per j
 __global__ void reduce_partial_kernel(int nvec, int nblk, const double* __restrict__ partial, double* __restrict__ out,
                                       int accumulate, int64_t pcol, int64_t hcol);
-// grid (vec_blocks(n)): out = w - V h (out may alias w), with nvec doubles of dynamic shared
-// memory; if norm_partial is given, norm_partial[b] = sum of squares of out over block b
+// grid (vec_blocks(n)): h[j] = sum over b < nblk of partial[j * nblk + b] (the multi-dot's
+// chunk partials, column stride dcol; block 0 stores h in h_out), then out = w - V h (out
+// may alias w), with nvec doubles of dynamic shared memory; if norm_partial is given,
+// norm_partial[b] = sum of squares of out over block b (column stride pcol)
 __global__ void update_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,
-                              const double* __restrict__ h, const double* __restrict__ w, double* __restrict__ out,
-                              double* __restrict__ norm_partial, int64_t col, int64_t pcol, int64_t hcol);
+                              const double* __restrict__ partial, int nblk, double* __restrict__ h_out,
+                              const double* __restrict__ w, double* __restrict__ out,
+                              double* __restrict__ norm_partial, int64_t col, int64_t dcol, int64_t pcol,
+                              int64_t hcol);
 // partial[b] = sum of squares of w over block b
 __global__ void norm_partial_kernel(int64_t n, const double* __restrict__ w, double* __restrict__ partial, int64_t col,
                                     int64_t pcol);
@@ -49,8 +53,9 @@ struct GivensState {
 
 // Completes Arnoldi step i: H column from the two Gram-Schmidt passes and the
 // norm partials, applies the previous rotations, forms the new one, updates g
-// (GMRES.c:485-503).  One block per column; a column whose active flag is 0
-// (active may be null: all active) only zeroes its inv_beta.
+// (GMRES.c:485-503).  One block per column with givens_smem(i) bytes of dynamic shared
+// memory; a column whose active flag is 0 (active may be null: all active) only zeroes
+// its inv_beta.
 __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
                               const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
@@ -70,6 +75,7 @@ __global__ void sub_kernel(int64_t n, const double* __restrict__ a, const double
 // dst += a
 __global__ void add_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ dst, int64_t col);
 
+inline size_t givens_smem(int i) { return sizeof(double) * (3 * (size_t)i + 2); }
 inline int vec_blocks(int64_t n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
 inline int dot_blocks(int64_t n) { return (int)((n + kDotChunk - 1) / kDotChunk); }
 

@@ -213,19 +213,16 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
       const size_t sh = sizeof(double) * nvec;
       dots_partial_kernel<<<dim3(nd, nvec), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nd, partial.get(), h1.get(), 0, 0, 0);
-      FFTSVD_CHECK_LAUNCH();
-      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h1.get(), w.get(), w.get(), nullptr, 0, 0, 0);
+      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, partial.get(), nd, h1.get(), w.get(), w.get(),
+                                                     nullptr, 0, 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
       dots_partial_kernel<<<dim3(nd, nvec), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      reduce_partial_kernel<<<nvec, 256, 0, stream>>>(nvec, nd, partial.get(), h2.get(), 0, 0, 0);
+      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, partial.get(), nd, h2.get(), w.get(), vnext,
+                                                     normpart.get(), 0, 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
-      update_kernel<<<nb, kVecThreads, sh, stream>>>(n, nvec, Vp, ldv, h2.get(), w.get(), vnext, normpart.get(), 0, 0,
-                                                     0);
-      FFTSVD_CHECK_LAUNCH();
-      givens_kernel<<<1, 256, 0, stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb, cs.get(),
-                                           sn.get(), g.get(), st.get(), 0, 0, nullptr);
+      givens_kernel<<<1, 256, givens_smem(i), stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb,
+                                                        cs.get(), sn.get(), g.get(), st.get(), 0, 0, nullptr);
       FFTSVD_CHECK_LAUNCH();
       scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext, 0, 0);
       FFTSVD_CHECK_LAUNCH();
