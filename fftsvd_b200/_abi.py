@@ -76,6 +76,16 @@ class SurfaceStats(C.Structure):
                 ("matvec_bytes_fp64", C.c_double)]
 
 
+TUNE_MAX_CANDIDATES = 8
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("chosen", C.c_int32 * 2),
+                ("max_groups", C.c_int32 * TUNE_MAX_CANDIDATES), ("max_src", C.c_int32 * TUNE_MAX_CANDIDATES),
+                ("max_entries", C.c_int32 * TUNE_MAX_CANDIDATES),
+                ("matvec_ms", (C.c_double * TUNE_MAX_CANDIDATES) * 2)]
+
+
 # field name -> (count expression, dtype) used to copy a TreeFlat into numpy arrays
 def tree_flat_to_numpy(t: TreeFlat) -> dict:
     """Copy every array of a TreeFlat into owned numpy arrays (dict keyed by field name)."""

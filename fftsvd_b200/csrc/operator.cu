@@ -125,8 +125,10 @@ bool make_group(const TileProblem& P, const std::vector<int>& ids, size_t first,
 // Tiling: outputs of one key in Morton order form member groups (runs of at most
 // kGroupMax siblings, or single outputs where a shared list would not be exact);
 // consecutive groups form a tile while its groups, halo inputs and padded entries fit
-// the kernel limits; tiles grouped by frequency count.
-static void build_tiles(const TileProblem& P, TileSet& S) {
+// the limits; tiles grouped by frequency count.  The groups and the order of every
+// group's entries do not depend on the limits, so neither does any sum the
+// translation forms: the limits change the speed only.
+static void build_tiles(const TileProblem& P, const TileLimits& lim, TileSet& S) {
    std::map<int, std::vector<int>> by_key;
    for (int i = 0; i < (int)P.key.size(); i++)
       if (P.ptr[i + 1] > P.ptr[i]) by_key[P.key[i]].push_back(i);
@@ -168,8 +170,8 @@ static void build_tiles(const TileProblem& P, TileSet& S) {
             for (int64_t in : G.src)
                if (!halo.count(in)) fresh++;
             const int padded = ((int)G.src.size() + 3) & ~3;
-            if (!tg.empty() && ((int)tg.size() + 1 > kTileMaxGroups || tile.nsrc + fresh > kTileMaxSrc ||
-                                tile.nentries + padded > kTileMaxEntries))
+            if (!tg.empty() && ((int)tg.size() + 1 > lim.max_groups || tile.nsrc + fresh > lim.max_src ||
+                                tile.nentries + padded > lim.max_entries))
                break;
             FFTSVD_REQUIRE(fresh <= kTileMaxSrc && padded <= kTileMaxEntries, "interaction list too long");
             for (int64_t in : G.src)
@@ -270,6 +272,18 @@ static void check_tiles(const TileSet& S, int64_t nt, int64_t in_elems, int64_t 
          }
       }
    }
+}
+
+void make_tiles(const TileProblems& P, const TileLimits& lim, TileSet& fwd, TileSet& adj) {
+   FFTSVD_REQUIRE(lim.max_groups >= 1 && lim.max_groups <= kTileMaxGroups && lim.max_src >= 1 &&
+                      lim.max_src <= kTileMaxSrc && lim.max_entries >= 4 && lim.max_entries <= kTileMaxEntries,
+                  "tile limits out of range");
+   fwd = TileSet();
+   adj = TileSet();
+   build_tiles(P.fwd, lim, fwd);
+   build_tiles(P.adj, lim, adj);
+   check_tiles(fwd, P.nt, P.spectra_elems, P.translated_elems);  // spectra -> translated
+   check_tiles(adj, P.nt, P.translated_elems, P.spectra_elems);  // transposed: translated -> spectra
 }
 
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
@@ -544,8 +558,10 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
    // The transposed operator translates the other way: every source cube gathers from the
    // destinations whose lists hold it, through the table slot of the opposite offset
    // (the grid-to-grid kernel of a symmetric Green's function satisfies G_DS^T = G_SD).
+   L.problems = std::make_shared<TileProblems>();
    {
-      TileProblem fwd, adj;
+      TileProblem& fwd = L.problems->fwd;
+      TileProblem& adj = L.problems->adj;
       std::map<int64_t, int> src_of_spec;
       for (int i = 0; i < (int)L.src.size(); i++) src_of_spec[L.src[i].spec_off] = i;
       std::vector<std::vector<std::pair<int64_t, int>>> adj_lists(L.src.size());
@@ -569,8 +585,6 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          adj.add_output(e.key, e.morton, e.t_base, e.pg, L.src[i].spec_off);
          for (const auto& pr : adj_lists[i]) adj.add_pair(pr.first, pr.second);
       }
-      build_tiles(fwd, L.fwd);
-      build_tiles(adj, L.adj);
    }
 
    // every index a kernel will form stays inside its buffer
@@ -610,8 +624,10 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       const int64_t pg = (int64_t)(2 * d.n - 1) * (2 * d.n - 1) * d.n;
       FFTSVD_REQUIRE(d.s_off >= 0 && d.s_off + pg <= L.translated_elems, "translated spectrum out of range");
    }
-   check_tiles(L.fwd, nt, L.spectra_elems, L.translated_elems);  // spectra -> translated
-   check_tiles(L.adj, nt, L.translated_elems, L.spectra_elems);  // transposed: translated -> spectra
+   L.problems->nt = nt;
+   L.problems->spectra_elems = L.spectra_elems;
+   L.problems->translated_elems = L.translated_elems;
+   make_tiles(*L.problems, TileLimits(), L.fwd, L.adj);
    for (int64_t k = 0; k < (int64_t)L.point_out.size(); k++) {
       FFTSVD_REQUIRE(L.point_out[k] >= 0 && L.point_out[k] < num_unknowns, "point without an output row");
       FFTSVD_REQUIRE(L.point_panel[k] >= -1 && L.point_panel[k] < L.total_panels - 1, "jump panel index");
@@ -2040,19 +2056,10 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    near_stride_ = maxcols;
    near_warps_ = (int)std::max<size_t>(1, std::min<size_t>(kNearThreads / 32, (size_t)optin / (maxcols * sizeof(T2))));
    leaf_smem_max_ = (int)(near_warps_ * maxcols * sizeof(T2));
-   int tile_smem = 0, tile_smem_b = 0;
-   for (const TileGroup& g : fwd_.groups) {
-      tile_smem = std::max(tile_smem, translate_smem(g, false));
-      tile_smem_b = std::max(tile_smem_b, translate_smem(g, true));
-   }
-   for (const TileGroup& g : adj_.groups) tile_smem = std::max(tile_smem, translate_smem(g, false));
-   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || tile_smem > optin ||
-       src_smem_t_ > optin || dst_smem_t_ > optin)
+   if (src_smem_ > optin || dst_smem_ > optin || leaf_smem_max_ > optin || src_smem_t_ > optin ||
+       dst_smem_t_ > optin)
       throw Error(FFTSVD_ERR_UNSUPPORTED, "operator block needs more shared memory than the device offers");
-   if (tile_smem > 0) {
-      raise_smem_limit(translate_kernel<T, false>, tile_smem);
-      raise_smem_limit(translate_kernel<T, true>, tile_smem_b);
-   }
+   raise_translate_smem(optin);
    // FFTSVD_B200_WARP_MIN_CUBES overrides the cube count from which small grids run
    // one cube per warp (tests set 0 to cover those kernels on small surfaces)
    warp_min_cubes_ = kWarpMinCubes;
@@ -2074,6 +2081,38 @@ void DeviceOperator<T>::enable_timing(bool on) {
    if (on && !ev_[0])
       for (auto& e : ev_) FFTSVD_CUDA(cudaEventCreate(&e));
    timing_ = on;
+}
+
+// Raise the translation kernels' dynamic shared-memory limits to what the current tiles need.
+template <typename T>
+void DeviceOperator<T>::raise_translate_smem(int optin) {
+   int tile_smem = 0, tile_smem_b = 0;
+   for (const TileGroup& g : fwd_.groups) {
+      tile_smem = std::max(tile_smem, translate_smem(g, false));
+      tile_smem_b = std::max(tile_smem_b, translate_smem(g, true));
+   }
+   for (const TileGroup& g : adj_.groups) tile_smem = std::max(tile_smem, translate_smem(g, false));
+   if (tile_smem > optin || tile_smem_b > optin)
+      throw Error(FFTSVD_ERR_UNSUPPORTED, "translation tile needs more shared memory than the device offers");
+   if (tile_smem > 0) {
+      raise_smem_limit(translate_kernel<T, false>, tile_smem);
+      raise_smem_limit(translate_kernel<T, true>, tile_smem_b);
+   }
+}
+
+template <typename T>
+void DeviceOperator<T>::set_tiles(const TileSet& fwd, const TileSet& adj) {
+   FFTSVD_REQUIRE(fwd.tile_groups.size() == fwd_.groups.size() && adj.tile_groups.size() == adj_.groups.size(),
+                  "tiles of another operator");
+   for (size_t i = 0; i < fwd.tile_groups.size(); i++)
+      FFTSVD_REQUIRE(fwd.tile_groups[i].pg == fwd_.groups[i].pg, "tiles of another operator");
+   int dev = 0, optin = 0;
+   FFTSVD_CUDA(cudaGetDevice(&dev));
+   FFTSVD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+   FFTSVD_CUDA(cudaDeviceSynchronize());  // no launch may still read the old tiles
+   fwd_.upload(fwd);
+   adj_.upload(adj);
+   raise_translate_smem(optin);
 }
 
 template <typename T>

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "common.h"
@@ -109,6 +110,25 @@ constexpr int kTileMaxGroups = 32;   // thread rows per block
 constexpr int kTileMaxSrc = 320;
 constexpr int kTileMaxEntries = 3072;
 
+// Limits of one translation tile (at most the kernel's bounds above).  Smaller tiles
+// give more blocks and less shared memory per block, larger ones stage each table
+// chunk for more destinations.
+struct TileLimits {
+   int max_groups = kTileMaxGroups;
+   int max_src = kTileMaxSrc;
+   int max_entries = kTileMaxEntries;
+};
+
+// Both translation problems of an operator with the buffer sizes their indices are
+// checked against, kept so that the tiles can be rebuilt with other limits.
+struct TileProblems {
+   TileProblem fwd, adj;
+   int64_t nt = 0, spectra_elems = 0, translated_elems = 0;
+};
+
+// Tiles of both directions under the given limits, range-checked.
+void make_tiles(const TileProblems& P, const TileLimits& lim, TileSet& fwd, TileSet& adj);
+
 struct LeafDesc {       // one leaf with points
    int32_t row_off;     // into leaf_rows
    int32_t nrows;
@@ -196,6 +216,7 @@ struct OperatorLayout {
    // translation tiles, grouped by frequency count (one launch per group): the operator's
    // (spectra -> translated) and the transposed operator's (translated -> spectra)
    TileSet fwd, adj;
+   std::shared_ptr<TileProblems> problems;
    // algorithmic bytes per matvec at 4-byte or 8-byte element size (excluding vectors)
    int64_t operator_elems = 0;          // D pairs*2 + VT + PV*2 + UTI + U
    int64_t t_elems = 0;                 // unique translation operator reals
@@ -222,6 +243,9 @@ class DeviceOperator {
    void apply_batch(const double* x, double* y, int nrhs, cudaStream_t stream);
    // device bytes of the batch buffers per right-hand side
    size_t batch_bytes_per_rhs() const;
+   // Replace the translation tiles (the same problems under other limits, make_tiles):
+   // results are unchanged bit for bit, only the launch shapes differ.  Synchronises.
+   void set_tiles(const TileSet& fwd, const TileSet& adj);
    // y = A^T x (the transposed operator), x and y device vectors of num_unknowns doubles.
    // Column sums are accumulated with FP64 atomics: not bitwise reproducible run to run.
    void apply_transpose(const double* x, double* y, cudaStream_t stream);
@@ -251,6 +275,7 @@ class DeviceOperator {
       BatchStrides bs;
    };
    int translate_smem(const TileGroup& g, bool batch) const;
+   void raise_translate_smem(int optin);
    void apply_bufs(const double* x, double* y, const Bufs& b, cudaStream_t stream);
    void launch_forward(const LaunchGroup& g, const Bufs& b, cudaStream_t stream);
    void launch_translate(const TileGroup& g, const Bufs& b, cudaStream_t stream);

@@ -324,6 +324,7 @@ void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree
    S.operator_elems = L.operator_elems;
    S.t_elems = L.t_elems;
    S.kernel_bytes = L.kernel_bytes;
+   S.tile_problems = L.problems;
    S.op64.upload(L);
    S.op32.upload(L);
    S.precond.build(*P, num_unknowns);

@@ -67,6 +67,10 @@ struct Surface {
    int gmres(int precision, const double* rhs, double* x, double tol, int maxit, double* res, int* status,
              bool absolute_zero_check = true);
    int solve(int precision, const double* rhs, double* x, double tol, int maxit, fftsvd_solve_info* info);
+   // Translation tile shapes: each candidate timed on both operators, the fastest kept (tune.cu).
+   std::shared_ptr<TileProblems> tile_problems;
+   void autotune(fftsvd_tune_info* info);
+   void set_tile_limits(int max_groups, int max_src, int max_entries);
    // Solvation energy and its derivatives with respect to the charges and their positions
    // (adjoint.cu); dG_dq holds num_charges entries, dG_dx 3 * num_charges; info[0] is the
    // forward solve, info[1] the adjoint (transposed) solve.

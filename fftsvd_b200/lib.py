@@ -33,7 +33,8 @@ EXPORTED = [
     "fftsvd_b200_matvec_batch_device", "fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch",
     "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
     "fftsvd_b200_set_charges", "fftsvd_b200_matvec_transpose", "fftsvd_b200_matvec_transpose_device",
-    "fftsvd_b200_adjoint", "fftsvd_b200_solve_many",
+    "fftsvd_b200_adjoint", "fftsvd_b200_solve_many", "fftsvd_b200_surface_autotune",
+    "fftsvd_b200_surface_set_tile_limits",
 ]
 
 
@@ -98,6 +99,8 @@ def load():
     lib.fftsvd_b200_solve_many.argtypes = [C.c_int32, C.POINTER(sp), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.c_int32, C.c_double, C.c_int32, C.POINTER(SolveInfo)]
     lib.fftsvd_b200_matvec_transpose.argtypes = [sp, C.c_int32, _f64p, _f64p]
+    lib.fftsvd_b200_surface_autotune.argtypes = [sp, C.POINTER(_abi.TuneInfo)]
+    lib.fftsvd_b200_surface_set_tile_limits.argtypes = [sp, C.c_int32, C.c_int32, C.c_int32]
     lib.fftsvd_b200_matvec_transpose_device.argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_adjoint.argtypes = [sp, C.c_int32, C.c_double, C.c_int32, _f64p, _f64p, _f64p,
                                         C.POINTER(SolveInfo)]

@@ -221,6 +221,25 @@ class Surface:
         check(load().fftsvd_b200_matvec_bytes(self._h, _prec(precision), C.byref(b)))
         return b.value
 
+    def autotune(self) -> dict:
+        """Time the matvec of both operator precisions under each candidate translation tile
+        shape and keep the fastest (results are unchanged bit for bit).  Returns the
+        candidates, their times and the chosen index per precision."""
+        info = _abi.TuneInfo()
+        check(load().fftsvd_b200_surface_autotune(self._h, C.byref(info)))
+        k = info.candidates
+        return {
+            "candidates": [(info.max_groups[c], info.max_src[c], info.max_entries[c]) for c in range(k)],
+            "matvec_ms_fp32": [info.matvec_ms[0][c] for c in range(k)],
+            "matvec_ms_fp64": [info.matvec_ms[1][c] for c in range(k)],
+            "chosen_fp32": info.chosen[0],
+            "chosen_fp64": info.chosen[1],
+        }
+
+    def set_tile_limits(self, max_groups=32, max_src=320, max_entries=3072):
+        """Rebuild the translation tiles under explicit limits (launch shapes only)."""
+        check(load().fftsvd_b200_surface_set_tile_limits(self._h, int(max_groups), int(max_src), int(max_entries)))
+
     # ---- operations on device pointers (torch tensors or raw ints)
     def matvec_device(self, x_ptr: int, y_ptr: int, precision="fp32"):
         check(load().fftsvd_b200_matvec_device(self._h, _prec(precision), C.c_void_p(x_ptr), C.c_void_p(y_ptr)))

@@ -255,6 +255,32 @@ int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const doubl
 /* The CUDA stream all work of this surface is issued on (cudaStream_t). */
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s);
 
+/* ---- tile-shape autotuner (no counterpart in the reference) ---- */
+
+#define FFTSVD_TUNE_MAX_CANDIDATES 8
+typedef struct {
+   int32_t candidates;                        /* candidate tile limits tried */
+   int32_t chosen[2];                         /* index kept for the FP32 and the FP64 operator */
+   int32_t max_groups[FFTSVD_TUNE_MAX_CANDIDATES];   /* per candidate: member groups per tile */
+   int32_t max_src[FFTSVD_TUNE_MAX_CANDIDATES];      /* halo source spectra per tile */
+   int32_t max_entries[FFTSVD_TUNE_MAX_CANDIDATES];  /* (group, source) entries per tile */
+   double matvec_ms[2][FFTSVD_TUNE_MAX_CANDIDATES];  /* concurrent matvec time, FP32 and FP64 */
+} fftsvd_tune_info;
+
+/* Rebuild the surface's translation tiles under each candidate limit set, time 10
+   matvecs of each operator precision with each (after 3 warm-up matvecs) and keep the
+   fastest per precision.  The tiles only change launch shapes: every sum keeps its
+   order, so later results are bit-for-bit those of the untuned surface.  Synchronises
+   the device; do not call it while other work of this surface is in flight.  info may
+   be null. */
+int fftsvd_b200_surface_autotune(fftsvd_surface* s, fftsvd_tune_info* info);
+
+/* Rebuild the translation tiles of both operators under explicit limits: member groups
+   per tile (1..32), halo source spectra per tile (1..320), entries per tile (4..3072).
+   The default surface uses 32, 320, 3072.  Like the autotuner this changes launch
+   shapes only.  Synchronises the device. */
+int fftsvd_b200_surface_set_tile_limits(fftsvd_surface* s, int32_t max_groups, int32_t max_src, int32_t max_entries);
+
 /* ---- adjoint: derivatives of the solvation energy (no counterpart in the
    reference; its FFTSVDforce computes conductor forces, FFTSVDforce.c:111-156) ---- */
 
