@@ -998,8 +998,13 @@ __global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
    if (kbeg >= nchunks) return;
    const int kend = min(nchunks, kbeg + chunks_per_block);
    char* p = smem_raw;
-   V* Tb = carve<V>(p, 343 * TU);
-   V* Fb = carve<V>(p, t.nsrc * U);
+   // batch: two buffers (the table rows are one unit wide, so both fit beside a second block
+   // per SM): the next chunk is copied while this one is multiplied
+   constexpr bool DB = BATCH;
+   V* const Tb0 = carve<V>(p, 343 * TU);
+   V* const Fb0 = carve<V>(p, t.nsrc * U);
+   V* const Tb1 = DB ? carve<V>(p, 343 * TU) : Tb0;
+   V* const Fb1 = DB ? carve<V>(p, t.nsrc * U) : Fb0;
    uint32_t* ent = carve<uint32_t>(p, t.nentries);
    int4* grp = carve<int4>(p, t.ngroups);
    int64_t* dstoff = carve<int64_t>(p, t.nmembers);
@@ -1021,12 +1026,11 @@ __global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
    const int u = lane & (U - 1), phase = lane / U;
    // all shared accesses below are smem_raw plus a byte offset, so they compile to
    // shared-window loads
-   const uint32_t tsu = (uint32_t)((const char*)Tb - smem_raw) + (BATCH ? 0u : (uint32_t)u * 16u);
-   const uint32_t fsu = (uint32_t)((const char*)Fb - smem_raw) + (uint32_t)u * 16u;
    const uint32_t es0 = (uint32_t)((const char*)ent - smem_raw);
-   for (int k = kbeg; k < kend; k++) {
+   auto stage = [&](int k, int b) {
       const int f0 = k * CH;
-      __syncthreads();  // metadata written / the previous chunk's rows consumed
+      V* const Tb = b ? Tb1 : Tb0;
+      V* const Fb = b ? Fb1 : Fb0;
       for (int i = threadIdx.x; i < 343 * TU; i += blockDim.x) {
          const int s = i / TU, uu = i % TU;
          cp_async16(&Tb[i], &tops[t.t_off + (int64_t)s * t.pg + f0 + uu * PER16]);
@@ -1039,8 +1043,29 @@ __global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
             cp_async16(&Fb[i], &spectra[srcoff[s] + f0 + uu * PER16]);
       }
       cp_async_commit();
-      cp_async_wait<0>();
+   };
+   __syncthreads();  // metadata written
+   if (DB) stage(kbeg, 0);
+   for (int k = kbeg; k < kend; k++) {
+      const int f0 = k * CH;
+      const int b = DB ? (k - kbeg) & 1 : 0;
+      if (DB) {
+         if (k + 1 < kend) {
+            stage(k + 1, b ^ 1);
+            cp_async_wait<1>();
+         } else {
+            cp_async_wait<0>();
+         }
+      } else {
+         if (k > kbeg) __syncthreads();  // the previous chunk's rows consumed
+         stage(k, 0);
+         cp_async_wait<0>();
+      }
       __syncthreads();
+      // all shared accesses below are smem_raw plus a byte offset, so they compile to
+      // shared-window loads
+      const uint32_t tsu = (uint32_t)((const char*)(b ? Tb1 : Tb0) - smem_raw) + (BATCH ? 0u : (uint32_t)u * 16u);
+      const uint32_t fsu = (uint32_t)((const char*)(b ? Fb1 : Fb0) - smem_raw) + (uint32_t)u * 16u;
       // groups in cost order, dealt to the warps in a snake order
       for (int r = 0;; r++) {
          const int gidx = r * nwarps + ((r & 1) ? nwarps - 1 - warp : warp);
@@ -1075,6 +1100,7 @@ __global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
                   *reinterpret_cast<V*>(&S[o + f0 + u * PER16]) = acc[j];
             }
       }
+      if (DB) __syncthreads();  // buffer b is refilled by the copies issued in the next iteration
    }
 }
 
@@ -2119,8 +2145,9 @@ template <typename T>
 int DeviceOperator<T>::translate_smem(const TileGroup& g, bool batch) const {
    // one chunk row per slot and per halo source, entries, groups, member offsets and
    // deltas, halo offsets; each carve aligned to 16 bytes
-   const size_t slot_row = batch ? 16 : kTileRowBytes;
-   return (int)(343 * slot_row + (size_t)g.max_src * kTileRowBytes + (size_t)g.max_entries * sizeof(uint32_t) +
+   // batch: two buffers of table and halo rows
+   const size_t slot_row = batch ? 16 : kTileRowBytes, nbuf = batch ? 2 : 1;
+   return (int)(nbuf * (343 * slot_row + (size_t)g.max_src * kTileRowBytes) + (size_t)g.max_entries * sizeof(uint32_t) +
                 (size_t)g.max_groups * sizeof(int4) + (size_t)g.max_members * (sizeof(int64_t) + sizeof(int)) +
                 (size_t)g.max_src * sizeof(int64_t) + 128);
 }
@@ -2182,9 +2209,11 @@ void DeviceOperator<T>::launch_translate_tiles(const DevTiles& tl, const TileGro
    const int groups = batch ? nrhs / kBatchGroup : 1;
    const int nchunks = g.pg / (batch ? 16 / (int)sizeof(T2) : kTileRowBytes / (int)sizeof(T2));
    const int64_t slots = 2LL * sm_count_;
+   // (batch: at least four chunks per block, so that the double buffer overlaps copies with
+   // arithmetic and neighbouring units of a spectrum row share their L2 sectors)
    int cpb = 1;
    int64_t best = -1;
-   for (int c = 1; c <= nchunks; c++) {
+   for (int c = batch ? std::min(nchunks, 4) : 1; c <= nchunks; c++) {
       const int64_t blocks = (int64_t)g.count * ((nchunks + c - 1) / c) * groups;
       const int64_t cost = (blocks + slots - 1) / slots * c;
       if (best < 0 || cost < best) best = cost, cpb = c;
