@@ -662,9 +662,42 @@ def run_matvec_only(args, cfg, local):
     s.close()
 
 
+def run_capture(args, cfg, local):
+    """Build the surface and run one part of the workload for a profiler capture:
+    `gmres` = right-hand side, 12 steps of an FP64 GMRES solve and the reaction potentials;
+    `transpose` = one FP32 transposed matvec (the adjoint's operator)."""
+    import ctypes as C
+
+    import torch
+    from fftsvd_b200 import _abi
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface
+
+    torch.cuda.set_device(local)
+    tri, qpos, q = make_workload(cfg)
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    x = torch.randn(s.n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    if args.capture == "gmres":
+        s.rhs_device(x.data_ptr())
+        info = _abi.SolveInfo()
+        load().fftsvd_b200_solve_device(s._h, _abi.PREC_FP64, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                        GMRES_TOL, 12, C.byref(info))  # stops at the cap: a capture, not a solve
+        phi = torch.empty(len(q), dtype=torch.float64, device="cuda")
+        s.reaction_potentials_device(y.data_ptr(), phi.data_ptr())
+    else:
+        load().fftsvd_b200_matvec_transpose_device(s._h, _abi.PREC_FP32, C.c_void_p(x.data_ptr()),
+                                                   C.c_void_p(y.data_ptr()))
+    torch.cuda.synchronize()
+    print(json.dumps({"capture": args.capture, "workload": cfg["name"], "norm": float(y.norm())}))
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--matvec-only", action="store_true", help="only run --reps matvecs (profiling)")
+    ap.add_argument("--capture", choices=["gmres", "transpose"], default=None,
+                    help="only run one part of the workload (profiling)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -680,6 +713,8 @@ def main():
     try:
         if args.matvec_only:
             run_matvec_only(args, cfg, local)
+        elif args.capture:
+            run_capture(args, cfg, local)
         elif args.impl == "reference":
             run_reference(args, cfg, ws, rank)
         elif cfg.get("kind") == "many":
