@@ -1875,6 +1875,207 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_back
    }
 }
 
+// ---- the transposed 4^3 transforms, one cube per warp with the DFT in registers
+// (lane and register layout of far_forward_n4_kernel / far_backward_n4_kernel: grid
+// point q = lane + 32 h)
+
+// per destination cube: a = U^T z (lane j accumulates row j, the points broadcast 32 at
+// a time), g = UTI^T a at q = lane and lane + 32, F = r2c DFT of g into the cube's
+// translated-spectrum slot
+template <typename T>
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_backward_t_n4_kernel(
+    const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points, const T* __restrict__ zt,
+    const T* __restrict__ uti, const T* __restrict__ ucm, typename Vec2<T>::type* __restrict__ out_spectra) {
+   using T2 = typename Vec2<T>::type;
+   constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(-2 pi i k / 7)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, -sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const DstDesc c = cubes[cube];
+   const int p = c.p, r = c.r;  // r <= 32: lane j owns row j of U^T
+   T a = T(0);
+   const T* urow = ucm + c.u_off + (int64_t)min(lane, r - 1) * p;
+   for (int base = 0; base < p; base += 32) {
+      const T zv = base + lane < p ? zt[dst_points[c.point_off + base + lane]] : T(0);
+      const int cnt = min(32, p - base);
+#pragma unroll 8
+      for (int i = 0; i < cnt; i++) {
+         const T zi = __shfl_sync(kAll, zv, i);
+         if (lane < r) a += urow[base + i] * zi;
+      }
+   }
+   T g0 = T(0), g1 = T(0);
+   const T* uc = uti + c.uti_off + lane;
+#pragma unroll 4
+   for (int j = 0; j < r; j++) {
+      const T aj = __shfl_sync(kAll, a, j);
+      g0 += uc[(int64_t)j * N3] * aj;
+      g1 += uc[(int64_t)j * N3 + 32] * aj;
+   }
+   // r2c DFT of g: stage k, stage j, stage i (as far_forward_n4_kernel)
+   const int kq = lane & 3, jp = (lane >> 2) & 3, hi = lane >> 4;
+   T2 w1[N], w2[2][N], W[Np];
+#pragma unroll
+   for (int k = 0; k < N; k++) w1[k] = tw[((k + OFF) * kq) % Np];
+#pragma unroll
+   for (int sl = 0; sl < 2; sl++)
+#pragma unroll
+      for (int j = 0; j < N; j++) w2[sl][j] = tw[((j + OFF) * (jp + 4 * sl)) % Np];
+#pragma unroll
+   for (int q = 0; q < Np; q++) W[q] = tw[q];
+   T2 A[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T gv = h ? g1 : g0;
+      T2 s = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+         const T gk = __shfl_sync(kAll, gv, (lane & ~3) | k);
+         s.x += gk * w1[k].x;
+         s.y += gk * w1[k].y;
+      }
+      A[h] = s;
+   }
+   T2 B[2][2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      T2 Aj[N];
+#pragma unroll
+      for (int j = 0; j < N; j++) Aj[j] = shfl_c<T>(A[h], (lane & ~12) | (j << 2));
+#pragma unroll
+      for (int sl = 0; sl < 2; sl++) {
+         T2 s = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int j = 0; j < N; j++) s = Cx<T>::fma(Aj[j], w2[sl][j], s);
+         B[h][sl] = s;
+      }
+   }
+   T2 Bi[N];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T2 mine = hi ? B[h][1] : B[h][0];
+      const T2 recv = shfl_c<T>(hi ? B[h][0] : B[h][1], lane ^ 16);
+      Bi[2 * h] = hi ? recv : mine;
+      Bi[2 * h + 1] = hi ? mine : recv;
+   }
+   T2* out = out_spectra + c.s_off + lane;
+   if (lane < ROW) {
+#pragma unroll
+      for (int fi = 0; fi < Np; fi++) {
+         T2 o = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int i = 0; i < N; i++) o = Cx<T>::fma(Bi[i], W[((i + OFF) * fi) % Np], o);
+         out[fi * ROW] = o;
+      }
+   }
+}
+
+// per source cube: g = c2r DFT of the spectrum (cropped at offset 2, scaled by 1/343),
+// a_j = {PV_s[j] . g, PV_d[j] . g}, and per panel {VT^T a_s, VT^T a_d} into the level's
+// staging row
+template <typename T>
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forward_t_n4_kernel(
+    const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
+    const typename Vec2<T>::type* __restrict__ in_spectra, const T* __restrict__ vt,
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ staging,
+    int64_t total_panels) {
+   using T2 = typename Vec2<T>::type;
+   constexpr int N = 4, Np = 7, OFF = 2, N3 = 64, ROW = Np * N;
+   constexpr unsigned kAll = 0xffffffffu;
+   __shared__ T2 tw[Np];
+   __shared__ __align__(16) T2 work[kWarpCubes][N * ROW];  // P1 [i][jf][kf], later a
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (threadIdx.x < Np) {  // exp(+2 pi i k / 7)
+      T cs, sn;
+      Cx<T>::cis(threadIdx.x, Np, &cs, &sn);
+      tw[threadIdx.x] = Cx<T>::make(cs, sn);
+   }
+   __syncthreads();
+   const int cube = blockIdx.x * kWarpCubes + warp;
+   if (cube >= count) return;
+   const SrcDesc c = cubes[cube];
+   const int kq = lane & 3, jp = (lane >> 2) & 3;
+   T2 W[Np], w2[Np], w3[N];
+#pragma unroll
+   for (int q = 0; q < Np; q++) W[q] = tw[q];
+#pragma unroll
+   for (int jf = 0; jf < Np; jf++) w2[jf] = tw[((jp + OFF) * jf) % Np];
+#pragma unroll
+   for (int kf = 0; kf < N; kf++) w3[kf] = tw[((kq + OFF) * kf) % Np];
+   T2* P1 = work[warp];
+   // inverse along i (i < 4) of column (jf, kf) = (jp + 4 hi, kq), straight from global
+   if (lane < ROW) {
+      T2 S[Np];
+      const T2* in = in_spectra + c.spec_off + lane;
+#pragma unroll
+      for (int fi = 0; fi < Np; fi++) S[fi] = in[fi * ROW];
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+         T2 s = Cx<T>::make(T(0), T(0));
+#pragma unroll
+         for (int fi = 0; fi < Np; fi++) s = Cx<T>::fma(S[fi], W[((i + OFF) * fi) % Np], s);
+         P1[i * ROW + lane] = s;
+      }
+   }
+   __syncwarp();
+   // inverse along j (j = jp) for i = 2 h + hi, kf = kq
+   T2 P2[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const int i = 2 * h + (lane >> 4);
+      T2 s = Cx<T>::make(T(0), T(0));
+#pragma unroll
+      for (int jf = 0; jf < Np; jf++) s = Cx<T>::fma(P1[i * ROW + jf * N + kq], w2[jf], s);
+      P2[h] = s;
+   }
+   // Hermitian half along k -> real grid value at q = lane + 32 h, cropped and scaled
+   const T scale = T(1) / (T)(Np * Np * Np);
+   T g[2];
+#pragma unroll
+   for (int h = 0; h < 2; h++) {
+      const T2 p0 = shfl_c<T>(P2[h], lane & ~3);
+      T s = p0.x;
+#pragma unroll
+      for (int kf = 1; kf < N; kf++) {
+         const T2 pk = shfl_c<T>(P2[h], (lane & ~3) | kf);
+         s += T(2) * (pk.x * w3[kf].x - pk.y * w3[kf].y);
+      }
+      g[h] = s * scale;
+   }
+   __syncwarp();  // P1 is reused for a
+   T2* a = P1;
+   const int r = c.r, m = c.m;  // r <= 32
+   const T2* pvc = pv + c.pv_off + lane;
+   for (int j = 0; j < r; j++) {
+      const T2 w0 = pvc[(int64_t)j * N3], w1v = pvc[(int64_t)j * N3 + 32];
+      T s = w0.x * g[0] + w1v.x * g[1];
+      T d = w0.y * g[0] + w1v.y * g[1];
+      s = warp_sum(s);
+      d = warp_sum(d);
+      if (lane == 0) a[j] = Cx<T>::make(s, d);
+   }
+   __syncwarp();
+   T2* stage = staging + (int64_t)c.level * total_panels;
+   for (int i = lane; i < m; i += 32) {
+      T s = T(0), d = T(0);
+#pragma unroll 4
+      for (int j = 0; j < r; j++) {
+         const T v = vt[c.vt_off + (int64_t)j * m + i];
+         s += v * a[j].x;
+         d += v * a[j].y;
+      }
+      stage[src_panels[c.panel_off + i]] = Cx<T>::make(s, d);
+   }
+}
+
 constexpr int kNearThreads = 128;
 
 template <typename T> struct NearLoad;
@@ -2279,27 +2480,49 @@ void DeviceOperator<T>::apply_transpose(const double* x, double* y, cudaStream_t
       gather_points_kernel<T><<<ew, 256, 0, stream>>>(total_points_, point_out_.get(), x, zt_.get());
       FFTSVD_CHECK_LAUNCH();
    }
-   // far field, backwards: destinations -> translated slots -> (transposed tiles) -> source spectra
-   for (const LaunchGroup& g : dst_groups_) {
-      far_backward_t_kernel<T><<<g.count, far_threads(g.n), dst_smem_t_, stream>>>(
-          dst_.get() + g.begin, dst_points_.get(), zt_.get(), uti_.get(), u_.get(), translated_.get());
-      FFTSVD_CHECK_LAUNCH();
-   }
-   // sources that no destination reaches must read zero
+   // far field, backwards: destinations -> translated slots -> (transposed tiles) -> source
+   // spectra, one chain per grid size on the chains' streams (as the forward operator), the
+   // near-field column sums beside them; sources that no destination reaches must read zero
    FFTSVD_CUDA(cudaMemsetAsync(spectra_.get(), 0, sizeof(T2) * spectra_elems_, stream));
-   for (const TileGroup& g : adj_.groups)
-      launch_translate_tiles(adj_, g, translated_.get(), spectra_.get(), 1, BatchStrides(), stream);
-   for (const LaunchGroup& g : src_groups_) {
-      far_forward_t_kernel<T><<<g.count, far_threads(g.n), src_smem_t_, stream>>>(
-          src_.get() + g.begin, src_panels_.get(), spectra_.get(), vt_.get(), pv_.get(), staget_.get(),
-          total_panels_);
-      FFTSVD_CHECK_LAUNCH();
-   }
+   FFTSVD_CUDA(cudaEventRecord(fork_, stream));
    if (n_leaf_ > 0) {
-      near_t_kernel<T><<<(n_leaf_ + kWarpCubes - 1) / kWarpCubes, kWarpThreads, 0, stream>>>(
+      FFTSVD_CUDA(cudaStreamWaitEvent(near_stream_, fork_, 0));
+      near_t_kernel<T><<<(n_leaf_ + kWarpCubes - 1) / kWarpCubes, kWarpThreads, 0, near_stream_>>>(
           leaves_.get(), n_leaf_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), zt_.get(), ut_.get(), (int32_t)np);
       FFTSVD_CHECK_LAUNCH();
+      FFTSVD_CUDA(cudaEventRecord(near_done_, near_stream_));
    }
+   for (const Chain& ch : chains_) {
+      FFTSVD_CUDA(cudaStreamWaitEvent(ch.stream, fork_, 0));
+      for (int i : ch.dst) {
+         const LaunchGroup& g = dst_groups_[i];
+         if (warp_path(g) && g.n == 4)
+            far_backward_t_n4_kernel<T><<<(g.count + kWarpCubes - 1) / kWarpCubes, kWarpThreads, 0, ch.stream>>>(
+                dst_.get() + g.begin, g.count, dst_points_.get(), zt_.get(), uti_.get(), u_.get(), translated_.get());
+         else
+            far_backward_t_kernel<T><<<g.count, far_threads(g.n), dst_smem_t_, ch.stream>>>(
+                dst_.get() + g.begin, dst_points_.get(), zt_.get(), uti_.get(), u_.get(), translated_.get());
+         FFTSVD_CHECK_LAUNCH();
+      }
+      const int pgp = ((2 * ch.n - 1) * (2 * ch.n - 1) * ch.n + 15) & ~15;
+      for (const TileGroup& g : adj_.groups)
+         if (g.pg == pgp) launch_translate_tiles(adj_, g, translated_.get(), spectra_.get(), 1, BatchStrides(), ch.stream);
+      for (int i : ch.src) {
+         const LaunchGroup& g = src_groups_[i];
+         if (warp_path(g) && g.n == 4)
+            far_forward_t_n4_kernel<T><<<(g.count + kWarpCubes - 1) / kWarpCubes, kWarpThreads, 0, ch.stream>>>(
+                src_.get() + g.begin, g.count, src_panels_.get(), spectra_.get(), vt_.get(), pv_.get(), staget_.get(),
+                total_panels_);
+         else
+            far_forward_t_kernel<T><<<g.count, far_threads(g.n), src_smem_t_, ch.stream>>>(
+                src_.get() + g.begin, src_panels_.get(), spectra_.get(), vt_.get(), pv_.get(), staget_.get(),
+                total_panels_);
+         FFTSVD_CHECK_LAUNCH();
+      }
+      FFTSVD_CUDA(cudaEventRecord(ch.done, ch.stream));
+   }
+   for (const Chain& ch : chains_) FFTSVD_CUDA(cudaStreamWaitEvent(stream, ch.done, 0));
+   if (n_leaf_ > 0) FFTSVD_CUDA(cudaStreamWaitEvent(stream, near_done_, 0));
    if (np > 0) {
       scatter_panels_kernel<T><<<ew, 256, 0, stream>>>(np, ut_.get(), staget_.get(), stage_levels_, total_panels_,
                                                        panel_jump_.get(), panel_point_.get(), zt_.get(),

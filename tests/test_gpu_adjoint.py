@@ -87,3 +87,30 @@ def test_autograd_function(case):
     assert abs(float(energy) - e) < 1e-9 * abs(e)
     assert np.allclose(pos.grad.numpy(), 2.0 * dx, rtol=1e-6, atol=1e-9 * np.abs(dx).max() + 1e-15)
     assert np.allclose(chg.grad.numpy(), 2.0 * dq, rtol=1e-6, atol=1e-12)
+
+
+@pytest.fixture(scope="module")
+def warp_pair(gpu, monkeypatch_module):
+    """The blob3 surface twice: once with the default kernels and once with every small
+    grid on the one-cube-per-warp kernels (the 4^3 transposed transforms on their
+    register DFTs), which large surfaces select by cube count."""
+    tri, qpos, q, c = make_case("blob3")
+    make = lambda: Surface.from_problem(tri, qpos, q, c["eps_in"], c["eps_out"], c["kappa"], svd_tol=1e-4)
+    s_block = make()
+    monkeypatch_module.setenv("FFTSVD_B200_WARP_MIN_CUBES", "0")
+    s_warp = make()
+    monkeypatch_module.delenv("FFTSVD_B200_WARP_MIN_CUBES")
+    return s_block, s_warp
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+def test_warp_transpose_kernels(warp_pair, prec, tol):
+    from helpers import rel
+    s_block, s_warp = warp_pair
+    rng = np.random.default_rng(33)
+    for _ in range(2):
+        x, y = rng.standard_normal(s_warp.n), rng.standard_normal(s_warp.n)
+        aty = s_warp.matvec_transpose(y, prec)
+        assert rel(aty, s_block.matvec_transpose(y, prec)) < tol
+        ax = s_warp.matvec(x, prec)
+        assert abs(float(ax @ y) - float(x @ aty)) <= tol * np.linalg.norm(ax) * np.linalg.norm(y)
