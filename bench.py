@@ -19,6 +19,7 @@ line on rank 0.
 from __future__ import annotations
 
 import argparse
+import collections
 import ctypes as C
 import json
 import os
@@ -590,6 +591,10 @@ def run_many(args, cfg, ws, rank, local):
         sols.append(torch.empty_like(r))
         panels += len(tri)
     setup_s = time.time() - t0
+    # translation tile shapes per surface from the autotuner (launch shapes only: same results)
+    t1 = time.time()
+    tuned = [s.autotune() for s in surfs]
+    tune_s = time.time() - t1
     torch.cuda.synchronize()
 
     def sequential(precision):
@@ -633,7 +638,9 @@ def run_many(args, cfg, ws, rank, local):
                        "timing": "host clock around one fftsvd_b200_solve_many call (it returns after every solve)"},
             "sequential_ms": seq_ms, "concurrency_speedup": seq_ms / conc_ms, "fp64_ms": conc64,
             "speedup_mixed_vs_fp64": conc64 / conc_ms, "dG_rel_err_mixed_vs_fp64_max": max(errs) if errs else None,
-            "setup_s": setup_s, "clocks": clk.summary(),
+            "setup_s": setup_s, "autotune_s": tune_s,
+            "autotune_chosen_fp32": collections.Counter(str(t["candidates"][t["chosen_fp32"]]) for t in tuned),
+            "clocks": clk.summary(),
         }
         print(json.dumps(line))
     for s in surfs:

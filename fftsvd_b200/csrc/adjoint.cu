@@ -95,8 +95,13 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_charge_kernel(
             const FlatPanel& P = tile[k];
             const double4 dn = dens[k];
             double s, d, gs[3], gd[3];
-            laplace_panel(pt, P, &s, &d);
-            laplace_panel_grad(pt, P, gs, gd);
+            const int br = laplace_panel_branch(pt, P);
+            if (br != 0) {  // moment expansion: value and exact gradient in one pass
+               laplace_panel_far_grad(pt, P, br, &s, &d, gs, gd);
+            } else {
+               laplace_panel(pt, P, &s, &d);
+               laplace_panel_grad(pt, P, gs, gd);
+            }
             acc[0] += dn.y * s - dn.x * d;
             if (P.centroid[0] == pt[0] && P.centroid[1] == pt[1] && P.centroid[2] == pt[2]) acc[0] -= 4.0 * M_PI * dn.x;
             const double rx = pt[0] - P.centroid[0], ry = pt[1] - P.centroid[1], rz = pt[2] - P.centroid[2];
