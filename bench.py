@@ -394,8 +394,10 @@ def charge_groups(num_charges, groups, seed):
 
 
 def run_batch(args, cfg, ws, rank, local):
-    """Batched solve: every charge group's right-hand side in one lockstep GMRES over the
-    multi-vector matvec (mixed precision, then FP64), groups sharded over ranks."""
+    """Batched solve: every charge group's right-hand side in one block GMRES (one Krylov
+    space shared by the groups, mixed precision), groups sharded over ranks; beside it the
+    block FP64 solve, the lockstep batch (each column its own Krylov basis) in both
+    precisions and one FP64 solve alone."""
     import torch
     from fftsvd_b200.lib import load
     from fftsvd_b200.surface import Surface
@@ -417,59 +419,77 @@ def run_batch(args, cfg, ws, rank, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     maxit = 150
 
-    def timed(precision, steps, warm):
+    def timed(solve, precision, steps, warm):
         for _ in range(warm):
-            s.solve_batch_device(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
+            solve(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
         total, info = 0.0, None
         for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            info = s.solve_batch_device(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
+            info = solve(R.data_ptr(), S.data_ptr(), k, precision, GMRES_TOL, maxit)
             e1.record(stream)
             e1.synchronize()
             total += e0.elapsed_time(e1)
-        return total, info
+        return total / steps, info
 
     torch.cuda.synchronize()
     barrier(ws)
+    warm = max(1, args.warmup - 2)
     launches0 = lib.fftsvd_b200_launch_count()
     with ClockSampler(local) as clk:
-        t_mixed, info_m = timed("mixed", args.steps, max(1, args.warmup - 2))
-    launches = (lib.fftsvd_b200_launch_count() - launches0) // (args.steps + max(1, args.warmup - 2))
+        t_block, info_b = timed(s.solve_block_device, "mixed", args.steps, warm)
+    launches = (lib.fftsvd_b200_launch_count() - launches0) // (args.steps + warm)
     torch.cuda.synchronize()
     barrier(ws)
-    t_max = barrier_max(t_mixed / args.steps, ws)
-    e_mixed = s.group_energies_device(sub, S.data_ptr())
-    t64, info64 = timed("fp64", 1, 0)
+    t_max = barrier_max(t_block, ws)
+    e_block = s.group_energies_device(sub, S.data_ptr())
+    t_block64, info_b64 = timed(s.solve_block_device, "fp64", 1, 0)
+    e_block64 = s.group_energies_device(sub, S.data_ptr())
+    t_lock, info_m = timed(s.solve_batch_device, "mixed", 1, 0)
+    e_lock = s.group_energies_device(sub, S.data_ptr())
+    t_lock64, _ = timed(s.solve_batch_device, "fp64", 1, 0)
     e64 = s.group_energies_device(sub, S.data_ptr())
-    errs = [abs(a - b) / abs(b) for a, b in zip(e_mixed, e64) if b != 0.0]
-    # one right-hand side solved alone (same surface, same kernels) for the per-column comparison
+
+    def errs(e):
+        v = [abs(a - b) / abs(b) for a, b in zip(e, e64) if b != 0.0]
+        return max(v) if v else None
+
+    # one right-hand side solved alone (same surface, same kernels), both precisions
     one = R[0].clone()
     sol1 = torch.empty_like(one)
-    for _ in range(2):
-        s.solve_device(one.data_ptr(), sol1.data_ptr(), "mixed", GMRES_TOL)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(3):
-        s.solve_device(one.data_ptr(), sol1.data_ptr(), "mixed", GMRES_TOL)
-    e1.record(stream)
-    e1.synchronize()
-    single_ms = e0.elapsed_time(e1) / 3
+    single = {}
+    for prec in ("mixed", "fp64"):
+        for _ in range(2):
+            s.solve_device(one.data_ptr(), sol1.data_ptr(), prec, GMRES_TOL)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            s.solve_device(one.data_ptr(), sol1.data_ptr(), prec, GMRES_TOL)
+        e1.record(stream)
+        e1.synchronize()
+        single[prec] = e0.elapsed_time(e1) / 3
     if rank == 0:
         its = [info_m[c].iterations for c in range(k)]
+        bits = [info_b[c].iterations for c in range(k)]
         line = {
             "metric": f"batched mixed-precision PBE solve ms ({cfg['groups']} charge-group right-hand sides)",
             "value": t_max, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32 operator, f64 Krylov vectors and refinement", "data": "synthetic",
             "config": {"workload": cfg["name"], "groups": cfg["groups"], "rhs_per_rank": k, "gmres_tol": GMRES_TOL,
-                       "svd_tol": SVD_TOL, "l2": "256 MiB buffer written between timed solves"},
-            "ms_per_rhs": t_max / k, "fp64_batch_ms": t64, "speedup_mixed_vs_fp64": t64 / t_max,
-            "single_solve_ms": single_ms, "batch_throughput_vs_single": single_ms * k / t_max,
-            "dG_rel_err_mixed_vs_fp64_max": max(errs) if errs else None,
-            "iterations_mixed_max": max(its), "iterations_mixed_mean": sum(its) / len(its),
+                       "svd_tol": SVD_TOL, "solver": "block GMRES, one Krylov space for the block of groups",
+                       "l2": "256 MiB buffer written between timed solves"},
+            "ms_per_rhs": t_max / k, "block_fp64_ms": t_block64, "lockstep_mixed_ms": t_lock,
+            "lockstep_fp64_ms": t_lock64, "single_solve_mixed_ms": single["mixed"],
+            "single_solve_fp64_ms": single["fp64"],
+            "speedup_vs_fp64_single_solves": single["fp64"] * k / t_max,
+            "speedup_vs_lockstep_fp64": t_lock64 / t_max, "speedup_vs_lockstep_mixed": t_lock / t_max,
+            "dG_rel_err_vs_lockstep_fp64_max": {"block_mixed": errs(e_block), "block_fp64": errs(e_block64),
+                                                "lockstep_mixed": errs(e_lock)},
+            "block_steps_mixed_max": max(bits), "block_steps_fp64_max": max(info_b64[c].iterations for c in range(k)),
+            "lockstep_iterations_mixed_max": max(its), "lockstep_iterations_mixed_mean": sum(its) / len(its),
             "gpu_launches": launches, "clocks": clk.summary(),
         }
         print(json.dumps(line))

@@ -1,0 +1,481 @@
+// Block GMRES: many right-hand sides of one surface in one shared Krylov space.
+//
+// Where the lockstep batch (batch.cu) gives every column its own Krylov basis, block
+// GMRES grows one basis by a block of K vectors per step: V_{j+1} R_{j+1,j} =
+// P^-1 A V_j - sum_i V_i H_ij, with the block Gram-Schmidt coefficients H_ij and the
+// block QR factor R_{j+1,j}.  Each column's solution is sought in the span of all
+// blocks, so the columns help one another: on 256 charge-group right-hand sides of
+// an 81 920-unknown surface every column reaches 1e-6 in about 14 block steps, where a
+// column alone takes about 46 GMRES steps.  The Krylov spaces differ from the single
+// solves', so the columns agree with single solves to the tolerance, not bit for bit.
+//
+// Device: the multi-vector matvec and preconditioner of the batch, the block
+// Gram-Schmidt (two classical passes) and the products with the basis as FP64 GEMMs
+// (cuBLAS), the block QR as CholQR2 (Gram matrix, then Cholesky and triangular inverse
+// in a one-block kernel, twice), the final triangular solve (cuBLAS).  Host: the block
+// Hessenberg least-squares problem (block_ls.cpp), updated for step j while the device
+// runs step j + 1, so its cost hides behind the matvec.
+//
+// Refinement: each pass gathers the columns still above the tolerance, scales their
+// residuals to unit norm, pads them to a multiple of 8 with seeded random directions
+// (which keep the block full rank and are not monitored), runs one block GMRES cycle
+// and adds the scaled corrections back; the residual is then recomputed with the outer
+// operator (FP64 for the mixed mode, as the single solve's refinement).
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "block.h"
+#include "block_ls.h"
+#include "surface.h"
+
+#define FFTSVD_BLAS(call)                                                                     \
+   do {                                                                                      \
+      cublasStatus_t st_ = (call);                                                           \
+      if (st_ != CUBLAS_STATUS_SUCCESS)                                                      \
+         throw ::fftsvd::Error(FFTSVD_ERR_CUDA,                                              \
+                               std::string(#call) + ": cuBLAS status " + std::to_string((int)st_)); \
+   } while (0)
+
+namespace fftsvd {
+
+namespace {
+
+constexpr int kCholThreads = 1024;
+constexpr int kMaxPasses = 16;
+
+// G (K x K, symmetric, column-major) = R^T R: writes the upper-triangular R and its
+// inverse (column-major, zero below the diagonal).  *flag = 1 when a pivot is not above
+// 1e-24 of the largest diagonal entry (or not finite): the columns are numerically
+// dependent; that pivot is then replaced by 1 so that nothing turns into NaN.  One block.
+__global__ void __launch_bounds__(kCholThreads) chol_inv_kernel(int K, const double* __restrict__ G,
+                                                                double* __restrict__ R, double* __restrict__ Rinv,
+                                                                int32_t* __restrict__ flag) {
+   __shared__ double pivot, gmax;
+   const int tid = threadIdx.x;
+   for (int idx = tid; idx < K * K; idx += blockDim.x) {
+      const int r = idx % K, c = idx / K;
+      R[idx] = r <= c ? G[idx] : 0.0;
+   }
+   if (tid == 0) {
+      double m = 0.0;
+      for (int k = 0; k < K; k++) m = fmax(m, G[(int64_t)k * K + k]);
+      gmax = m;
+   }
+   __syncthreads();
+   for (int k = 0; k < K; k++) {
+      if (tid == 0) {
+         double a = R[(int64_t)k * K + k];
+         if (!(a > 1e-24 * gmax) || !isfinite(a)) {
+            *flag = 1;
+            a = 1.0;
+         }
+         pivot = sqrt(a);
+         R[(int64_t)k * K + k] = pivot;
+      }
+      __syncthreads();
+      for (int c = k + 1 + tid; c < K; c += blockDim.x) R[(int64_t)c * K + k] /= pivot;
+      __syncthreads();
+      const int m = K - k - 1;
+      for (int t = tid; t < m * m; t += blockDim.x) {
+         const int i = k + 1 + t % m, c = k + 1 + t / m;
+         if (i <= c) R[(int64_t)c * K + i] -= R[(int64_t)i * K + k] * R[(int64_t)c * K + k];
+      }
+      __syncthreads();
+   }
+   // inverse: column c solves R x = e_c by back substitution (one thread per column)
+   for (int c = tid; c < K; c += blockDim.x) {
+      double* x = Rinv + (int64_t)c * K;
+      for (int r = K - 1; r > c; r--) x[r] = 0.0;
+      for (int r = c; r >= 0; r--) {
+         double s = r == c ? 1.0 : 0.0;
+         for (int l = r + 1; l <= c; l++) s -= R[(int64_t)l * K + r] * x[l];
+         x[r] = s / R[(int64_t)r * K + r];
+      }
+   }
+}
+
+// Columns c0 <= c < c1 of v (column c at v + c * n): seeded uniform values in
+// [-scale, scale), the splitmix64 generator on the element index.
+__global__ void seeded_fill_kernel(int64_t n, int c0, int c1, double scale, double* __restrict__ v) {
+   const int64_t total = (int64_t)(c1 - c0) * n;
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+      uint64_t z = (uint64_t)(k + (int64_t)c0 * n + 1) * 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z ^= z >> 31;
+      v[(int64_t)c0 * n + k] = scale * ((double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0);
+   }
+}
+
+// grid (blocks, 1, columns): dst column a = fac[a] * src column idx[a]
+__global__ void gather_scale_kernel(int64_t n, const double* __restrict__ src, const int32_t* __restrict__ idx,
+                                    const double* __restrict__ fac, double* __restrict__ dst) {
+   const int a = blockIdx.z;
+   const double* s = src + (int64_t)idx[a] * n;
+   double* d = dst + (int64_t)a * n;
+   const double f = fac[a];
+   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      d[i] = f * s[i];
+}
+
+// grid (blocks, 1, columns): dst column idx[a] += fac[a] * src column a
+__global__ void scatter_add_kernel(int64_t n, const double* __restrict__ src, const int32_t* __restrict__ idx,
+                                   const double* __restrict__ fac, double* __restrict__ dst) {
+   const int a = blockIdx.z;
+   const double* s = src + (int64_t)a * n;
+   double* d = dst + (int64_t)idx[a] * n;
+   const double f = fac[a];
+   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      d[i] += f * s[i];
+}
+
+int pad8(int k) { return (k + kBatchGroup - 1) / kBatchGroup * kBatchGroup; }
+
+}  // namespace
+
+BlockWorkspace::~BlockWorkspace() {
+   if (blas) cublasDestroy((cublasHandle_t)blas);
+   for (auto& e : done)
+      if (e) cudaEventDestroy(e);
+   for (auto& p : hbuf)
+      if (p) cudaFreeHost(p);
+   for (auto& p : rbuf)
+      if (p) cudaFreeHost(p);
+   if (flag_h) cudaFreeHost(flag_h);
+}
+
+void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) {
+   if (!blas) {
+      cublasHandle_t h;
+      FFTSVD_BLAS(cublasCreate(&h));
+      blas = h;
+      for (auto& e : done) FFTSVD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      FFTSVD_CUDA(cudaMallocHost(&flag_h, 2 * sizeof(int)));
+   }
+   FFTSVD_BLAS(cublasSetStream((cublasHandle_t)blas, stream));
+   if (n_ == n && K_ <= K && mmax_ <= mmax) return;
+   if (n_ != n) K = mmax = 0;
+   n = n_;
+   K = std::max(K, K_);
+   mmax = std::max(mmax, mmax_);
+   const size_t kn = (size_t)K * n, kk = (size_t)K * K;
+   V.alloc((size_t)(mmax + 1) * kn);
+   for (DevBuf<double>* b : {&W, &S, &R0, &T, &Bc, &Xc, &Rc, &Tc}) b->alloc(kn);
+   H.alloc((size_t)(mmax + 1) * kk);
+   H2.alloc((size_t)(mmax + 1) * kk);
+   for (DevBuf<double>* b : {&G, &R1, &R1i, &R2, &R2i, &R}) b->alloc(kk);
+   Y.alloc((size_t)mmax * kk);
+   Rd.alloc((size_t)mmax * K * (size_t)mmax * K);
+   scal.alloc(K);
+   part.alloc((size_t)K * vec_blocks(n));
+   fac.alloc(K);
+   idx.alloc(K);
+   flag.alloc(1);
+   for (auto& p : hbuf) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      FFTSVD_CUDA(cudaMallocHost(&p, sizeof(double) * (size_t)(mmax + 1) * kk));
+   }
+   for (auto& p : rbuf) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      FFTSVD_CUDA(cudaMallocHost(&p, sizeof(double) * kk));
+   }
+}
+
+// Q R = X (n x K, both column-major with ld n) by CholQR2; R (K x K) is left in blk->R
+// and a rank deficiency raises blk->flag.
+void Surface::block_qr(const double* X, double* Q, int K) {
+   BlockWorkspace& B = *blk;
+   cublasHandle_t h = (cublasHandle_t)B.blas;
+   const double one = 1.0, zero = 0.0;
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, X, n, X, n, &zero, B.G.get(), K));
+   chol_inv_kernel<<<1, kCholThreads, 0, stream>>>(K, B.G.get(), B.R1.get(), B.R1i.get(), B.flag.get());
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, K, &one, X, n, B.R1i.get(), K, &zero, B.S.get(), n));
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, B.S.get(), n, B.S.get(), n, &zero, B.G.get(), K));
+   chol_inv_kernel<<<1, kCholThreads, 0, stream>>>(K, B.G.get(), B.R2.get(), B.R2i.get(), B.flag.get());
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, K, &one, B.S.get(), n, B.R2i.get(), K, &zero, Q, n));
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &one, B.R2.get(), K, B.R1.get(), K, &zero, B.R.get(),
+                           K));
+}
+
+// One cycle of block GMRES on P^-1 A T = R0 (K columns, A the operator `precision`),
+// T += the minimiser over the block Krylov space of up to mmax blocks.  Stops when each
+// monitored column c < nmon has residual <= target[c] (absolute, preconditioned), after
+// mmax block steps, or when a new block is numerically dependent on the basis (the
+// cycle then keeps the blocks before it).  res receives the residual estimates of the
+// K columns; returns the block steps used, 0 when the columns of R0 are dependent.
+int Surface::gmres_block(int precision, int K, const double* R0, double* T, int nmon, const std::vector<double>& target,
+                         int mmax, std::vector<double>& res) {
+   BlockWorkspace& B = *blk;
+   cublasHandle_t h = (cublasHandle_t)B.blas;
+   const double one = 1.0, zero = 0.0, minus = -1.0;
+   const int64_t vblk = (int64_t)K * n;
+   double* V = B.V.get();
+   res.assign(K, 0.0);
+   // V_0 S0 = R0
+   FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
+   block_qr(R0, V, K);
+   std::vector<double> S0((size_t)K * K);
+   FFTSVD_CUDA(cudaMemcpyAsync(S0.data(), B.R.get(), sizeof(double) * K * K, cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaMemcpyAsync(B.flag_h, B.flag.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   if (B.flag_h[0]) return 0;
+   BlockLeastSquares ls;
+   ls.init(K, mmax, S0.data());
+   // step j: W = P^-1 A V_j, two Gram-Schmidt passes against V_0 .. V_j, V_{j+1} R = W;
+   // the coefficients, R and the rank flag then go to the pinned host slot j & 1
+   auto issue = [&](int j) {
+      const int rows = (j + 1) * K;
+      apply_batch(precision, V + j * vblk, B.W.get(), K);
+      precond_batch(B.W.get(), B.W.get(), K);
+      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero, B.H.get(),
+                              rows));
+      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H.get(), rows, &one,
+                              B.W.get(), n));
+      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero, B.H2.get(),
+                              rows));
+      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H2.get(), rows, &one,
+                              B.W.get(), n));
+      FFTSVD_BLAS(cublasDgeam(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, K, &one, B.H.get(), rows, &one, B.H2.get(), rows,
+                              B.H.get(), rows));
+      FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
+      block_qr(B.W.get(), V + (j + 1) * vblk, K);
+      FFTSVD_CUDA(cudaMemcpyAsync(B.hbuf[j & 1], B.H.get(), sizeof(double) * (size_t)rows * K,
+                                  cudaMemcpyDeviceToHost, stream));
+      FFTSVD_CUDA(cudaMemcpyAsync(B.rbuf[j & 1], B.R.get(), sizeof(double) * (size_t)K * K, cudaMemcpyDeviceToHost,
+                                  stream));
+      FFTSVD_CUDA(cudaMemcpyAsync(B.flag_h + (j & 1), B.flag.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+      FFTSVD_CUDA(cudaEventRecord(B.done[j & 1], stream));
+   };
+   // residual estimates after the last two steps (before any step: the columns' norms)
+   std::vector<double> prev(K), prev2(K);
+   for (int c = 0; c < K; c++) {
+      double s = 0.0;
+      for (int r = 0; r <= c; r++) s += S0[(size_t)c * K + r] * S0[(size_t)c * K + r];
+      prev[c] = prev2[c] = std::sqrt(s);
+   }
+   // Step j + 1 is issued before the host takes step j unless the last convergence rate
+   // predicts that step j meets every target (then it would be wasted).
+   auto speculate = [&](int j) {
+      if (j == 0) return true;
+      for (int c = 0; c < nmon; c++) {
+         const double q = prev2[c] > 0.0 ? std::min(1.0, prev[c] / prev2[c]) : 1.0;
+         if (prev[c] * q > 2.0 * target[c]) return true;
+      }
+      return false;
+   };
+   int m = 0, issued = 0;
+   issue(0);
+   issued = 1;
+   for (int j = 0; j < mmax; j++) {
+      if (issued == j + 1 && j + 1 < mmax && speculate(j)) issue(issued++);
+      FFTSVD_CUDA(cudaEventSynchronize(B.done[j & 1]));
+      if (B.flag_h[j & 1]) break;  // V_{j+1} is not a basis: keep the first j blocks
+      ls.add_column(B.hbuf[j & 1], B.rbuf[j & 1], res.data());
+      m = j + 1;
+      bool all = true;
+      for (int c = 0; c < nmon && all; c++) all = res[c] <= target[c];
+      if (all) break;
+      prev2.swap(prev);
+      prev = res;
+      if (issued == j + 1 && j + 1 < mmax) issue(issued++);
+   }
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));  // a speculative step may still run
+   if (m == 0) return 0;
+   // Y = R^-1 g_top on the device: the triangular factor's block columns into the dense
+   // upper triangle Rd (ld mmax K), g_top into Y (ld mK)
+   const int rows = m * K;
+   const int64_t ldr = (int64_t)B.mmax * B.K;
+   for (int j = 0; j < m; j++)
+      FFTSVD_CUDA(cudaMemcpy2DAsync(B.Rd.get() + (int64_t)j * K * ldr, sizeof(double) * ldr, ls.rcol(j),
+                                    sizeof(double) * (j + 1) * K, sizeof(double) * (j + 1) * K, K,
+                                    cudaMemcpyHostToDevice, stream));
+   FFTSVD_CUDA(cudaMemcpy2DAsync(B.Y.get(), sizeof(double) * rows, ls.g(), sizeof(double) * ls.ldg(),
+                                 sizeof(double) * rows, K, cudaMemcpyHostToDevice, stream));
+   FFTSVD_BLAS(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, K,
+                           &one, B.Rd.get(), ldr, B.Y.get(), rows));
+   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &one, V, n, B.Y.get(), rows, &one, T, n));
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));  // ls is released with this frame
+   return m;
+}
+
+int Surface::solve_block(int precision, int k, const double* rhs, double* x, double tol, int maxit,
+                         fftsvd_solve_info* info) {
+   FFTSVD_REQUIRE(k > 0 && k <= kMaxBatch, "right-hand side count");
+   FFTSVD_REQUIRE(tol > 0.0 && maxit > 0, "tolerance and iteration cap must be positive");
+   FFTSVD_REQUIRE(precision == FFTSVD_PREC_FP64 || precision == FFTSVD_PREC_FP32 || precision == FFTSVD_PREC_MIXED,
+                  "unknown precision mode");
+   const auto clock_start = std::chrono::steady_clock::now();
+   const bool mixed = precision == FFTSVD_PREC_MIXED;
+   const int inner = mixed ? FFTSVD_PREC_FP32 : precision, outer = mixed ? FFTSVD_PREC_FP64 : precision;
+   if (!blk) blk = std::make_unique<BlockWorkspace>();
+   const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
+   const int nb = vec_blocks(n);
+   std::vector<int> iters(k, 0), refinements(k, 0), status(k, FFTSVD_OK);
+   std::vector<double> resid(k, 0.0);
+   for (int c0 = 0; c0 < k; c0 += kBlockMax) {
+      const int nc = std::min(kBlockMax, k - c0), ncp = pad8(nc);
+      // basis: up to maxit blocks (at most 64), as many as a third of the device memory
+      // that is free or already held by the basis allows
+      size_t free_b = 0, total_b = 0;
+      FFTSVD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      if (blk->n == n) free_b += blk->V.bytes() + blk->Rd.bytes();
+      const size_t per_blk = sizeof(double) * (size_t)ncp * n;
+      const int cap = (int)std::max<int64_t>(2, (int64_t)(free_b / 3 / per_blk) - 10);
+      const int mmax = std::max(1, std::min({maxit, cap - 1, 64}));
+      blk->ensure(n, ncp, mmax, stream);
+      BlockWorkspace& B = *blk;
+      FFTSVD_CUDA(cudaMemsetAsync(B.Bc.get(), 0, sizeof(double) * (size_t)ncp * n, stream));
+      FFTSVD_CUDA(cudaMemcpyAsync(B.Bc.get(), rhs + (int64_t)c0 * n, sizeof(double) * (size_t)nc * n,
+                                  cudaMemcpyDeviceToDevice, stream));
+      FFTSVD_CUDA(cudaMemsetAsync(B.Xc.get(), 0, sizeof(double) * (size_t)ncp * n, stream));
+      std::vector<double> bn(nc, 0.0), rn(ncp, 0.0);
+      int used = 0;
+      bool fallback = false;
+      for (int pass = 0;; pass++) {
+         // Rc = P^-1 (B - A X), the outer operator (P^-1 B on the first pass)
+         if (pass == 0) {
+            precond_batch(B.Bc.get(), B.Rc.get(), ncp);
+         } else {
+            apply_batch(outer, B.Xc.get(), B.Tc.get(), ncp);
+            sub_kernel<<<dim3(ew_blocks, 1, ncp), 256, 0, stream>>>(n, B.Bc.get(), B.Tc.get(), B.Tc.get(), n);
+            FFTSVD_CHECK_LAUNCH();
+            precond_batch(B.Tc.get(), B.Rc.get(), ncp);
+         }
+         norm_partial_kernel<<<dim3(nb, 1, ncp), kVecThreads, 0, stream>>>(n, B.Rc.get(), B.part.get(), n, nb);
+         FFTSVD_CHECK_LAUNCH();
+         reduce_partial_kernel<<<dim3(1, 1, ncp), 256, 0, stream>>>(1, nb, B.part.get(), B.scal.get(), 0, nb, 1);
+         FFTSVD_CHECK_LAUNCH();
+         FFTSVD_CUDA(cudaMemcpyAsync(rn.data(), B.scal.get(), sizeof(double) * ncp, cudaMemcpyDeviceToHost, stream));
+         FFTSVD_CUDA(cudaStreamSynchronize(stream));
+         std::vector<int32_t> act;
+         std::vector<double> target;
+         for (int a = 0; a < nc; a++) {
+            const int c = c0 + a;
+            rn[a] = std::sqrt(rn[a]);
+            if (pass == 0) {
+               bn[a] = rn[a];
+               if (!std::isfinite(bn[a])) {  // left out; its solution stays zero
+                  status[c] = FFTSVD_ERR_NONFINITE;
+                  resid[c] = bn[a];
+               }
+            }
+            if (status[c] != FFTSVD_OK || bn[a] == 0.0) continue;  // zero right-hand side: zero solution
+            resid[c] = rn[a] / bn[a];
+            if (!std::isfinite(resid[c])) {
+               status[c] = FFTSVD_ERR_NONFINITE;
+               continue;
+            }
+            if (resid[c] < tol) continue;
+            act.push_back(a);
+            // relative to the column's current residual: the single solve's inner target
+            // 0.3 tol / residual for a mixed correction, else the tolerance itself
+            target.push_back(mixed ? std::min(0.1, std::max(0.3 * tol / resid[c], 1e-13)) : tol / resid[c]);
+         }
+         if (act.empty() || used >= maxit || pass >= kMaxPasses) break;
+         const int na = (int)act.size(), K = pad8(na);
+         std::vector<double> f(na);
+         for (int a = 0; a < na; a++) f[a] = 1.0 / rn[act[a]];
+         FFTSVD_CUDA(cudaMemcpyAsync(B.idx.get(), act.data(), sizeof(int32_t) * na, cudaMemcpyHostToDevice, stream));
+         FFTSVD_CUDA(cudaMemcpyAsync(B.fac.get(), f.data(), sizeof(double) * na, cudaMemcpyHostToDevice, stream));
+         gather_scale_kernel<<<dim3(ew_blocks, 1, na), 256, 0, stream>>>(n, B.Rc.get(), B.idx.get(), B.fac.get(),
+                                                                       B.R0.get());
+         FFTSVD_CHECK_LAUNCH();
+         if (K > na) {
+            seeded_fill_kernel<<<ew_blocks, 256, 0, stream>>>(n, na, K, std::sqrt(3.0 / n), B.R0.get());
+            FFTSVD_CHECK_LAUNCH();
+         }
+         FFTSVD_CUDA(cudaMemsetAsync(B.T.get(), 0, sizeof(double) * (size_t)K * n, stream));
+         std::vector<double> est;
+         const int m = gmres_block(inner, K, B.R0.get(), B.T.get(), na, target, std::min(mmax, maxit - used), est);
+         if (m == 0) {
+            // dependent right-hand sides (or residuals): the lockstep batch handles them
+            fallback = pass == 0;
+            break;
+         }
+         for (int a = 0; a < na; a++) f[a] = rn[act[a]];
+         FFTSVD_CUDA(cudaMemcpyAsync(B.fac.get(), f.data(), sizeof(double) * na, cudaMemcpyHostToDevice, stream));
+         scatter_add_kernel<<<dim3(ew_blocks, 1, na), 256, 0, stream>>>(n, B.T.get(), B.idx.get(), B.fac.get(),
+                                                                      B.Xc.get());
+         FFTSVD_CHECK_LAUNCH();
+         used += m;
+         for (int a : act) {
+            iters[c0 + a] += m;
+            if (mixed) refinements[c0 + a]++;
+         }
+      }
+      if (fallback) {
+         std::vector<fftsvd_solve_info> sub(nc);
+         solve_batch(precision, nc, rhs + (int64_t)c0 * n, B.Xc.get(), tol, maxit, sub.data());
+         for (int a = 0; a < nc; a++) {
+            iters[c0 + a] = sub[a].iterations;
+            refinements[c0 + a] = sub[a].refinements;
+            status[c0 + a] = sub[a].status;
+            resid[c0 + a] = sub[a].residual;
+         }
+      }
+      for (int a = 0; a < nc; a++) {
+         const int c = c0 + a;
+         if (status[c] == FFTSVD_OK && !(resid[c] < tol) && bn[a] != 0.0) status[c] = FFTSVD_ERR_NOT_CONVERGED;
+      }
+      FFTSVD_CUDA(cudaMemcpyAsync(x + (int64_t)c0 * n, B.Xc.get(), sizeof(double) * (size_t)nc * n,
+                                  cudaMemcpyDeviceToDevice, stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   }
+   const auto clock_end = std::chrono::steady_clock::now();
+   const double ms = std::chrono::duration<double, std::milli>(clock_end - clock_start).count();
+   int first_bad = FFTSVD_OK;
+   for (int c = 0; c < k; c++) {
+      if (first_bad == FFTSVD_OK && status[c] != FFTSVD_OK) first_bad = status[c];
+      if (info) {
+         info[c].iterations = iters[c];
+         info[c].refinements = refinements[c];
+         info[c].status = status[c];
+         info[c].residual = resid[c];
+         info[c].setup_ms = 0.0;
+         info[c].solve_ms = ms;
+      }
+   }
+   return first_bad;
+}
+
+}  // namespace fftsvd
+
+using namespace fftsvd;
+
+extern "C" {
+
+int fftsvd_b200_solve_block_device(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                                   double tol, int32_t max_iterations, fftsvd_solve_info* info) {
+   if (!s || !rhs || !sol || nrhs <= 0) return FFTSVD_ERR_ARGUMENT;
+   int status = FFTSVD_OK;
+   const int rc = guarded([&] { status = s->s.solve_block(precision, nrhs, rhs, sol, tol, max_iterations, info); });
+   return rc != FFTSVD_OK ? rc : status;
+}
+
+int fftsvd_b200_solve_block(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                            double tol, int32_t max_iterations, fftsvd_solve_info* info) {
+   if (!s || !rhs || !sol || nrhs <= 0) return FFTSVD_ERR_ARGUMENT;
+   int status = FFTSVD_OK;
+   const int rc = guarded([&] {
+      Surface& S = s->s;
+      const size_t bytes = sizeof(double) * (size_t)nrhs * S.n;
+      DevBuf<double> din((size_t)nrhs * S.n), dout((size_t)nrhs * S.n);
+      FFTSVD_CUDA(cudaMemcpyAsync(din.get(), rhs, bytes, cudaMemcpyHostToDevice, S.stream));
+      status = S.solve_block(precision, nrhs, din.get(), dout.get(), tol, max_iterations, info);
+      FFTSVD_CUDA(cudaMemcpyAsync(sol, dout.get(), bytes, cudaMemcpyDeviceToHost, S.stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+   });
+   return rc != FFTSVD_OK ? rc : status;
+}
+
+}  // extern "C"

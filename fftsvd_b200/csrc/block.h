@@ -1,0 +1,37 @@
+// Workspace of the block GMRES solve; see block.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+
+namespace fftsvd {
+
+constexpr int kBlockMax = 256;  // right-hand sides per block Krylov space
+
+struct BlockWorkspace {
+   int64_t n = 0;
+   int K = 0;     // columns of a block (a multiple of 8)
+   int mmax = 0;  // block steps the basis holds
+   void* blas = nullptr;  // cublasHandle_t
+   DevBuf<double> V;                    // mmax + 1 blocks of K x n
+   DevBuf<double> W, S, R0, T;          // K x n
+   DevBuf<double> Bc, Xc, Rc, Tc;       // K x n: right-hand sides, iterate, residual, scratch
+   DevBuf<double> H, H2;                // (mmax + 1) K x K Gram-Schmidt coefficients
+   DevBuf<double> G, R1, R1i, R2, R2i, R;  // K x K
+   DevBuf<double> Y;                    // mmax K x K least-squares solution
+   DevBuf<double> Rd;                   // (mmax K)^2: dense triangular factor of the least squares
+   DevBuf<double> scal, part, fac;      // column norms and partial sums, column factors
+   DevBuf<int32_t> idx, flag;
+   cudaEvent_t done[2] = {nullptr, nullptr};
+   double* hbuf[2] = {nullptr, nullptr};  // pinned: coefficients of the last two steps
+   double* rbuf[2] = {nullptr, nullptr};  // pinned: their R blocks
+   int* flag_h = nullptr;                 // pinned: their rank flags
+   BlockWorkspace() = default;
+   BlockWorkspace(const BlockWorkspace&) = delete;
+   BlockWorkspace& operator=(const BlockWorkspace&) = delete;
+   ~BlockWorkspace();
+   void ensure(int64_t n, int K, int mmax, cudaStream_t stream);
+};
+
+}  // namespace fftsvd

@@ -125,6 +125,7 @@ void Preconditioner::apply(const double* r, double* z, cudaStream_t s, bool tran
 // ------------------------------------------------------------------ surface
 
 Surface::~Surface() {
+   blk.reset();  // its cuBLAS handle is bound to the stream
    if (st_host) cudaFreeHost(st_host);
    if (stream) cudaStreamDestroy(stream);
 }

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "batch.h"
+#include "block.h"
 #include "common.h"
 #include "gmres.cuh"
 #include "operator.h"
@@ -90,6 +91,14 @@ struct Surface {
                    std::vector<int>& iters, std::vector<int>& status);
    // k right-hand sides; info may be null or hold k entries.  Returns the first non-OK status.
    int solve_batch(int precision, int k, const double* rhs, double* x, double tol, int maxit,
+                   fftsvd_solve_info* info);
+
+   // ---- block GMRES over one shared Krylov space (block.cu)
+   std::unique_ptr<BlockWorkspace> blk;
+   void block_qr(const double* X, double* Q, int K);
+   int gmres_block(int precision, int K, const double* R0, double* X, int nmon, const std::vector<double>& target,
+                   int mmax, std::vector<double>& res);
+   int solve_block(int precision, int k, const double* rhs, double* x, double tol, int maxit,
                    fftsvd_solve_info* info);
 };
 

@@ -34,7 +34,7 @@ EXPORTED = [
     "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
     "fftsvd_b200_set_charges", "fftsvd_b200_matvec_transpose", "fftsvd_b200_matvec_transpose_device",
     "fftsvd_b200_adjoint", "fftsvd_b200_solve_many", "fftsvd_b200_surface_autotune",
-    "fftsvd_b200_surface_set_tile_limits",
+    "fftsvd_b200_surface_set_tile_limits", "fftsvd_b200_solve_block_device", "fftsvd_b200_solve_block",
 ]
 
 
@@ -90,7 +90,8 @@ def load():
     lib.fftsvd_b200_launch_count.restype = C.c_longlong
     lib.fftsvd_b200_reaction_potentials_noalloc.argtypes = [sp, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_matvec_batch_device.argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
-    for name in ("fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch"):
+    for name in ("fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch", "fftsvd_b200_solve_block_device",
+                 "fftsvd_b200_solve_block"):
         getattr(lib, name).argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
                                        C.POINTER(SolveInfo)]
     lib.fftsvd_b200_rhs_groups_device.argtypes = [sp, C.c_int32, _i32p, C.c_void_p]

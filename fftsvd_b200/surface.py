@@ -307,6 +307,28 @@ class Surface:
             check(rc)
         return sol, info
 
+    def solve_block_device(self, rhs_ptr: int, sol_ptr: int, nrhs: int, precision="mixed", tol=1e-6,
+                           max_iterations=1000, raise_on_error=True):
+        """Block GMRES over one shared Krylov space; returns the per-column SolveInfo array."""
+        info = (SolveInfo * int(nrhs))()
+        rc = load().fftsvd_b200_solve_block_device(self._h, int(nrhs), _prec(precision), C.c_void_p(rhs_ptr),
+                                                   C.c_void_p(sol_ptr), float(tol), int(max_iterations), info)
+        if raise_on_error:
+            check(rc)
+        return info
+
+    def solve_block(self, rhs, precision="mixed", tol=1e-6, max_iterations=1000, raise_on_error=True):
+        """Block GMRES; rhs: (k, n) host array.  Returns (solutions (k, n), per-column SolveInfo array)."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        k = rhs.shape[0]
+        sol = np.empty_like(rhs)
+        info = (SolveInfo * k)()
+        rc = load().fftsvd_b200_solve_block(self._h, k, _prec(precision), rhs.ctypes.data, sol.ctypes.data,
+                                            float(tol), int(max_iterations), info)
+        if raise_on_error:
+            check(rc)
+        return sol, info
+
     def rhs_groups_device(self, group_ptr, rhs_ptr: int):
         gp = i32(group_ptr)
         check(load().fftsvd_b200_rhs_groups_device(self._h, len(gp) - 1, ptr(gp, C.c_int32), C.c_void_p(rhs_ptr)))

@@ -325,6 +325,26 @@ int fftsvd_b200_solve_batch_device(fftsvd_surface* s, int32_t nrhs, int32_t prec
 /* Same with host pointers. */
 int fftsvd_b200_solve_batch(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
                             double tol, int32_t max_iterations, fftsvd_solve_info* info);
+/* Solves A x_c = rhs_c for nrhs columns by block GMRES (no counterpart in the
+   reference): the columns, in blocks of at most 256, share one Krylov space that
+   grows by one block of vectors per multi-vector matvec, so each column's solution
+   is sought in the span of every column's Krylov vectors and the block needs far
+   fewer steps than a column alone.  Stopping test per column as fftsvd_b200_solve:
+   preconditioned residual below tol relative to the preconditioned right-hand side,
+   the residual recomputed in FP64 for FFTSVD_PREC_MIXED (FP32-operator block
+   GMRES inside FP64 refinement; only unconverged columns take part in a refinement
+   pass).  Results agree with the single solves to the tolerance, not bit for bit.
+   max_iterations caps the block steps of each block of columns; iterations in info
+   counts the block steps a column took part in, refinements the refinement passes.
+   Zero columns get the zero solution; non-finite columns report
+   FFTSVD_ERR_NONFINITE and the others solve.  If the right-hand sides of a block
+   are linearly dependent the block falls back to fftsvd_b200_solve_batch_device.
+   Returns the first column's non-OK status, else FFTSVD_OK. */
+int fftsvd_b200_solve_block_device(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                                   double tol, int32_t max_iterations, fftsvd_solve_info* info);
+/* Same with host pointers. */
+int fftsvd_b200_solve_block(fftsvd_surface* s, int32_t nrhs, int32_t precision, const double* rhs, double* sol,
+                            double tol, int32_t max_iterations, fftsvd_solve_info* info);
 /* Solves `count` surfaces concurrently: rhs[i] and sol[i] are device vectors of
    surface i (fftsvd_b200_solve_device semantics per surface), info is NULL or count
    entries.  A pool of host threads drives the solves, each on its surface's device and
