@@ -10,9 +10,12 @@
 // solves', so the columns agree with single solves to the tolerance, not bit for bit.
 //
 // Device: the multi-vector matvec and preconditioner of the batch, the block
-// Gram-Schmidt (two classical passes) and the products with the basis as FP64 GEMMs
-// (cuBLAS), the block QR as CholQR2 (Gram matrix, then Cholesky and triangular inverse
-// in a one-block kernel, twice), the final triangular solve (cuBLAS).  Host: the block
+// Gram-Schmidt and the products with the basis as FP64 GEMMs (cuBLAS), the block QR as
+// CholQR2 (Gram matrix, Cholesky factor in a one-block kernel, triangular solve; twice),
+// the final triangular solve (cuBLAS).  Gram-Schmidt is one classical pass while no
+// column of a new block loses more than five digits in it (the new block is then
+// orthogonal to the basis to about 1e-11, far below what a solve to 1e-6 needs), two
+// passes from the first step where one does.  Host: the block
 // Hessenberg least-squares problem (block_ls.cpp), updated for step j while the device
 // runs step j + 1, so its cost hides behind the matvec.
 //
@@ -47,58 +50,91 @@ namespace fftsvd {
 namespace {
 
 constexpr int kCholThreads = 1024;
+constexpr int kCholBlock = 32;
 constexpr int kMaxPasses = 16;
+// A column whose norm falls below this fraction in the first Gram-Schmidt pass would be
+// left orthogonal to the basis only to eps / fraction: later steps then take two passes.
+constexpr double kReorthRatio = 1e-5;
 
-// G (K x K, symmetric, column-major) = R^T R: writes the upper-triangular R and its
-// inverse (column-major, zero below the diagonal).  *flag = 1 when a pivot is not above
-// 1e-24 of the largest diagonal entry (or not finite): the columns are numerically
-// dependent; that pivot is then replaced by 1 so that nothing turns into NaN.  One block.
-__global__ void __launch_bounds__(kCholThreads) chol_inv_kernel(int K, const double* __restrict__ G,
-                                                                double* __restrict__ R, double* __restrict__ Rinv,
-                                                                int32_t* __restrict__ flag) {
-   __shared__ double pivot, gmax;
-   const int tid = threadIdx.x;
+// G (K x K, symmetric, column-major, K <= kBlockMax) = R^T R: writes the upper-triangular
+// R (zero below the diagonal).  Right-looking, blocked by 32 rows: one warp factors the
+// 32 x 32 diagonal block in shared memory, one thread per column solves the panel to its
+// right (kept in shared memory), and all threads update the trailing upper triangle from
+// the panel.  *flag = 1 when a pivot is not above 1e-24 of the largest diagonal entry of G
+// (or not finite): the columns are numerically dependent; that pivot is then taken as 1
+// so that nothing turns into NaN.  One block, chol_smem(K) bytes of dynamic shared memory.
+__global__ void __launch_bounds__(kCholThreads) chol_kernel(int K, const double* __restrict__ G,
+                                                            double* __restrict__ R, int32_t* __restrict__ flag) {
+   extern __shared__ double sm[];
+   double* D = sm;                            // diagonal block, D[c * 32 + r]
+   double* P = sm + kCholBlock * kCholBlock;  // panel, P[l * K + c] (row l of the block, column c)
+   __shared__ double gmax;
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    for (int idx = tid; idx < K * K; idx += blockDim.x) {
       const int r = idx % K, c = idx / K;
       R[idx] = r <= c ? G[idx] : 0.0;
    }
-   if (tid == 0) {
+   if (warp == 0) {
       double m = 0.0;
-      for (int k = 0; k < K; k++) m = fmax(m, G[(int64_t)k * K + k]);
-      gmax = m;
+      for (int k = lane; k < K; k += 32) m = fmax(m, G[(int64_t)k * K + k]);
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) gmax = m;
    }
    __syncthreads();
-   for (int k = 0; k < K; k++) {
-      if (tid == 0) {
-         double a = R[(int64_t)k * K + k];
-         if (!(a > 1e-24 * gmax) || !isfinite(a)) {
-            *flag = 1;
-            a = 1.0;
+   for (int k0 = 0; k0 < K; k0 += kCholBlock) {
+      const int bs = min(kCholBlock, K - k0), k1 = k0 + bs, m = K - k1;
+      if (warp == 0) {  // lane = column of the diagonal block
+         for (int r = 0; r < bs; r++)
+            if (lane < bs) D[lane * 32 + r] = R[(int64_t)(k0 + lane) * K + k0 + r];
+         __syncwarp();
+         for (int kk = 0; kk < bs; kk++) {
+            double a = D[kk * 32 + kk];
+            const bool bad = !(a > 1e-24 * gmax) || !isfinite(a);
+            if (bad) a = 1.0;
+            const double p = sqrt(a);
+            if (lane == 0 && bad) *flag = 1;
+            __syncwarp();
+            double dk = 0.0;
+            if (lane > kk && lane < bs) {
+               dk = D[lane * 32 + kk] / p;
+               D[lane * 32 + kk] = dk;
+            }
+            if (lane == kk) D[kk * 32 + kk] = p;
+            __syncwarp();
+            if (lane > kk && lane < bs)
+               for (int i = kk + 1; i <= lane; i++) D[lane * 32 + i] -= D[i * 32 + kk] * dk;
+            __syncwarp();
          }
-         pivot = sqrt(a);
-         R[(int64_t)k * K + k] = pivot;
+         for (int r = 0; r < bs; r++)
+            if (lane < bs && r <= lane) R[(int64_t)(k0 + lane) * K + k0 + r] = D[lane * 32 + r];
       }
       __syncthreads();
-      for (int c = k + 1 + tid; c < K; c += blockDim.x) R[(int64_t)c * K + k] /= pivot;
-      __syncthreads();
-      const int m = K - k - 1;
-      for (int t = tid; t < m * m; t += blockDim.x) {
-         const int i = k + 1 + t % m, c = k + 1 + t / m;
-         if (i <= c) R[(int64_t)c * K + i] -= R[(int64_t)i * K + k] * R[(int64_t)c * K + k];
+      // panel: D^T X = R[k0:k1, k1:K] by forward substitution, one column per thread
+      for (int t = tid; t < m; t += blockDim.x) {
+         const int c = k1 + t;
+         for (int r = 0; r < bs; r++) {
+            double v = R[(int64_t)c * K + k0 + r];
+            for (int l = 0; l < r; l++) v -= D[r * 32 + l] * P[l * K + c];
+            v /= D[r * 32 + r];
+            P[r * K + c] = v;
+            R[(int64_t)c * K + k0 + r] = v;
+         }
       }
       __syncthreads();
-   }
-   // inverse: column c solves R x = e_c by back substitution (one thread per column)
-   for (int c = tid; c < K; c += blockDim.x) {
-      double* x = Rinv + (int64_t)c * K;
-      for (int r = K - 1; r > c; r--) x[r] = 0.0;
-      for (int r = c; r >= 0; r--) {
-         double s = r == c ? 1.0 : 0.0;
-         for (int l = r + 1; l <= c; l++) s -= R[(int64_t)l * K + r] * x[l];
-         x[r] = s / R[(int64_t)r * K + r];
+      // trailing upper triangle: R[i, c] -= sum over the panel rows of P[l, i] P[l, c]
+      for (int idx = tid; idx < m * m; idx += blockDim.x) {
+         const int ii = idx % m, cc = idx / m;
+         if (ii > cc) continue;
+         const int i = k1 + ii, c = k1 + cc;
+         double v = 0.0;
+         for (int l = 0; l < bs; l++) v += P[l * K + i] * P[l * K + c];
+         R[(int64_t)c * K + i] -= v;
       }
+      __syncthreads();
    }
 }
+
+size_t chol_smem(int K) { return sizeof(double) * ((size_t)kCholBlock * kCholBlock + (size_t)kCholBlock * K); }
 
 // Columns c0 <= c < c1 of v (column c at v + c * n): seeded uniform values in
 // [-scale, scale), the splitmix64 generator on the element index.
@@ -157,6 +193,8 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
       blas = h;
       for (auto& e : done) FFTSVD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       FFTSVD_CUDA(cudaMallocHost(&flag_h, 2 * sizeof(int)));
+      FFTSVD_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)chol_smem(kBlockMax)));
    }
    FFTSVD_BLAS(cublasSetStream((cublasHandle_t)blas, stream));
    if (n_ == n && K_ <= K && mmax_ <= mmax) return;
@@ -166,10 +204,10 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
    mmax = std::max(mmax, mmax_);
    const size_t kn = (size_t)K * n, kk = (size_t)K * K;
    V.alloc((size_t)(mmax + 1) * kn);
-   for (DevBuf<double>* b : {&W, &S, &R0, &T, &Bc, &Xc, &Rc, &Tc}) b->alloc(kn);
+   for (DevBuf<double>* b : {&W, &R0, &T, &Bc, &Xc, &Rc, &Tc}) b->alloc(kn);
    H.alloc((size_t)(mmax + 1) * kk);
    H2.alloc((size_t)(mmax + 1) * kk);
-   for (DevBuf<double>* b : {&G, &R1, &R1i, &R2, &R2i, &R}) b->alloc(kk);
+   for (DevBuf<double>* b : {&G, &R1, &R2, &R}) b->alloc(kk);
    Y.alloc((size_t)mmax * kk);
    Rd.alloc((size_t)mmax * K * (size_t)mmax * K);
    scal.alloc(K);
@@ -189,20 +227,22 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
    }
 }
 
-// Q R = X (n x K, both column-major with ld n) by CholQR2; R (K x K) is left in blk->R
-// and a rank deficiency raises blk->flag.
+// Q R = X (n x K, both column-major with ld n; X may be Q) by CholQR2: twice the Gram
+// matrix, its Cholesky factor and a triangular solve in place.  R (K x K) is left in
+// blk->R and a rank deficiency raises blk->flag.
 void Surface::block_qr(const double* X, double* Q, int K) {
    BlockWorkspace& B = *blk;
    cublasHandle_t h = (cublasHandle_t)B.blas;
    const double one = 1.0, zero = 0.0;
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, X, n, X, n, &zero, B.G.get(), K));
-   chol_inv_kernel<<<1, kCholThreads, 0, stream>>>(K, B.G.get(), B.R1.get(), B.R1i.get(), B.flag.get());
-   FFTSVD_CHECK_LAUNCH();
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, K, &one, X, n, B.R1i.get(), K, &zero, B.S.get(), n));
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, B.S.get(), n, B.S.get(), n, &zero, B.G.get(), K));
-   chol_inv_kernel<<<1, kCholThreads, 0, stream>>>(K, B.G.get(), B.R2.get(), B.R2i.get(), B.flag.get());
-   FFTSVD_CHECK_LAUNCH();
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, K, &one, B.S.get(), n, B.R2i.get(), K, &zero, Q, n));
+   if (X != Q)
+      FFTSVD_CUDA(cudaMemcpyAsync(Q, X, sizeof(double) * (size_t)K * n, cudaMemcpyDeviceToDevice, stream));
+   for (double* Rp : {B.R1.get(), B.R2.get()}) {
+      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, Q, n, Q, n, &zero, B.G.get(), K));
+      chol_kernel<<<1, kCholThreads, chol_smem(K), stream>>>(K, B.G.get(), Rp, B.flag.get());
+      FFTSVD_CHECK_LAUNCH();
+      FFTSVD_BLAS(cublasDtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, K,
+                              &one, Rp, K, Q, n));
+   }
    FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &one, B.R2.get(), K, B.R1.get(), K, &zero, B.R.get(),
                            K));
 }
@@ -231,8 +271,10 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
    if (B.flag_h[0]) return 0;
    BlockLeastSquares ls;
    ls.init(K, mmax, S0.data());
-   // step j: W = P^-1 A V_j, two Gram-Schmidt passes against V_0 .. V_j, V_{j+1} R = W;
-   // the coefficients, R and the rank flag then go to the pinned host slot j & 1
+   // step j: W = P^-1 A V_j, block Gram-Schmidt against V_0 .. V_j (a second pass once
+   // `reorth` is set), V_{j+1} R = W; the coefficients, R and the rank flag then go to the
+   // pinned host slot j & 1
+   bool reorth = false;
    auto issue = [&](int j) {
       const int rows = (j + 1) * K;
       apply_batch(precision, V + j * vblk, B.W.get(), K);
@@ -241,12 +283,14 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
                               rows));
       FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H.get(), rows, &one,
                               B.W.get(), n));
-      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero, B.H2.get(),
-                              rows));
-      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H2.get(), rows, &one,
-                              B.W.get(), n));
-      FFTSVD_BLAS(cublasDgeam(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, K, &one, B.H.get(), rows, &one, B.H2.get(), rows,
-                              B.H.get(), rows));
+      if (reorth) {
+         FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero,
+                                 B.H2.get(), rows));
+         FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H2.get(), rows, &one,
+                                 B.W.get(), n));
+         FFTSVD_BLAS(cublasDgeam(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, K, &one, B.H.get(), rows, &one, B.H2.get(), rows,
+                                 B.H.get(), rows));
+      }
       FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
       block_qr(B.W.get(), V + (j + 1) * vblk, K);
       FFTSVD_CUDA(cudaMemcpyAsync(B.hbuf[j & 1], B.H.get(), sizeof(double) * (size_t)rows * K,
@@ -282,6 +326,15 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
       if (B.flag_h[j & 1]) break;  // V_{j+1} is not a basis: keep the first j blocks
       ls.add_column(B.hbuf[j & 1], B.rbuf[j & 1], res.data());
       m = j + 1;
+      // the new block's norms after the projection against those before it
+      for (int c = 0; c < K && !reorth; c++) {
+         const double* hc = B.hbuf[j & 1] + (size_t)c * (j + 1) * K;
+         const double* rc = B.rbuf[j & 1] + (size_t)c * K;
+         double sh = 0.0, sr = 0.0;
+         for (int r = 0; r < (j + 1) * K; r++) sh += hc[r] * hc[r];
+         for (int r = 0; r <= c; r++) sr += rc[r] * rc[r];
+         if (sr < kReorthRatio * kReorthRatio * (sh + sr)) reorth = true;
+      }
       bool all = true;
       for (int c = 0; c < nmon && all; c++) all = res[c] <= target[c];
       if (all) break;

@@ -15,10 +15,10 @@ struct BlockWorkspace {
    int mmax = 0;  // block steps the basis holds
    void* blas = nullptr;  // cublasHandle_t
    DevBuf<double> V;                    // mmax + 1 blocks of K x n
-   DevBuf<double> W, S, R0, T;          // K x n
+   DevBuf<double> W, R0, T;             // K x n
    DevBuf<double> Bc, Xc, Rc, Tc;       // K x n: right-hand sides, iterate, residual, scratch
    DevBuf<double> H, H2;                // (mmax + 1) K x K Gram-Schmidt coefficients
-   DevBuf<double> G, R1, R1i, R2, R2i, R;  // K x K
+   DevBuf<double> G, R1, R2, R;         // K x K
    DevBuf<double> Y;                    // mmax K x K least-squares solution
    DevBuf<double> Rd;                   // (mmax K)^2: dense triangular factor of the least squares
    DevBuf<double> scal, part, fac;      // column norms and partial sums, column factors
