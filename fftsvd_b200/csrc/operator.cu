@@ -688,6 +688,9 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       g.count++;
       g.smem_elems = std::max(g.smem_elems, src_need(L.src[i]));
       g.max_rank = std::max(g.max_rank, L.src[i].r);
+      const int n = L.src[i].n, Np = 2 * n - 1;
+      g.batch_shared = std::max(g.batch_shared, 2 * std::min(L.src[i].m, 1024) + 2 * Np);
+      g.batch_per_rhs = std::max(g.batch_per_rhs, 2 * L.src[i].r + n * n * n + 2 * n * n * n + 2 * n * Np * n);
    }
    for (int i = 0; i < (int)L.dst.size(); i++) {
       if (L.dst_groups.empty() || L.dst_groups.back().n != L.dst[i].n) L.dst_groups.push_back({L.dst[i].n, i, 0, 0, 0});
@@ -695,6 +698,10 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       g.count++;
       g.smem_elems = std::max(g.smem_elems, dst_need(L.dst[i]));
       g.max_rank = std::max(g.max_rank, L.dst[i].r);
+      const int n = L.dst[i].n, Np = 2 * n - 1;
+      g.batch_shared = std::max(g.batch_shared, 2 * Np);
+      g.batch_per_rhs = std::max(g.batch_per_rhs, 2 * Np * Np * n + 2 * n * Np * n + 2 * n * n * n + n * n * n +
+                                                      L.dst[i].r);
    }
    return L;
 }
@@ -768,20 +775,31 @@ static int far_threads(int n) {
 }
 constexpr int kChunk = 1024;
 
-// One block per source cube: a = VT x (both layers), g = PV_s a_s + PV_d a_d on
-// the n^3 grid, F = r2c DFT of g placed at offset n/2 in the (2n-1)^3 box.
+// right-hand sides per block of the batched far-field kernels
 template <typename T>
+constexpr int far_rb() { return sizeof(T) == 4 ? 8 : 4; }
+// dynamic shared memory of a block of g serving rb right-hand sides (16-byte carve padding included)
+static int far_batch_smem(const LaunchGroup& g, int rb, size_t elem) {
+   return (int)((g.batch_shared + (size_t)rb * g.batch_per_rhs) * elem + 256);
+}
+
+// One block per source cube and RB right-hand sides: a = VT x (both layers), g = PV_s a_s +
+// PV_d a_d on the n^3 grid, F = r2c DFT of g placed at offset n/2 in the (2n-1)^3 box.
+// Every right-hand side goes through the arithmetic of RB = 1 (same loops, chunks and
+// reduction order); RB > 1 reads each PV row and twiddle once for RB right-hand sides and
+// runs the transform stages over all of them between barriers.
+template <typename T, int RB>
 __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
     const SrcDesc* __restrict__ cubes, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
-   xsd += rhs * bs.panels;
-   spectra += rhs * bs.spectra;
+   const int ngrp = bs.nrhs / RB;
+   const int rhs0 = (blockIdx.x % ngrp) * RB, unit = blockIdx.x / ngrp;  // right-hand sides fastest
    extern __shared__ __align__(16) char smem_raw[];
    const SrcDesc c = cubes[unit];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n;
+   const int NA = n * n * H, NB = n * Np * H, PG = Np * Np * H;
    const int m = c.m, r = c.r;
    const int ch = min(m, kChunk);
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -789,58 +807,68 @@ __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
    char* p = smem_raw;
    T* xs = carve<T>(p, ch);
    T* xd = carve<T>(p, ch);
-   T* as = carve<T>(p, r);
-   T* ad = carve<T>(p, r);
-   T* g = carve<T>(p, n3);
+   T* as = carve<T>(p, RB * r);
+   T* ad = carve<T>(p, RB * r);
+   T* g = carve<T>(p, RB * n3);
    T2* tw = carve<T2>(p, Np);
-   T2* A = carve<T2>(p, n * n * H);
-   T2* B = carve<T2>(p, n * Np * H);
+   T2* A = carve<T2>(p, RB * NA);
+   T2* B = carve<T2>(p, RB * NB);
 
-   for (int j = tid; j < r; j += blockDim.x) { as[j] = T(0); ad[j] = T(0); }
+   for (int j = tid; j < RB * r; j += blockDim.x) { as[j] = T(0); ad[j] = T(0); }
    for (int k = tid; k < Np; k += blockDim.x) {  // exp(-2 pi i k / Np)
       T cs, sn;
       Cx<T>::cis(k, Np, &cs, &sn);
       tw[k] = Cx<T>::make(cs, -sn);
    }
    // VT x, streamed over panel chunks; each row is owned by one warp
-   for (int base = 0; base < m; base += ch) {
-      const int cnt = min(ch, m - base);
-      __syncthreads();
-      for (int i = tid; i < cnt; i += blockDim.x) {
-         T2 v = xsd[src_panels[c.panel_off + base + i]];
-         xs[i] = v.x;
-         xd[i] = v.y;
-      }
-      __syncthreads();
-      for (int j = warp; j < r; j += nwarps) {
-         const T* row = vt + c.vt_off + (int64_t)j * m + base;
-         T s = T(0), d = T(0);
-         for (int i = lane; i < cnt; i += 32) {
-            T v = row[i];
-            s += v * xs[i];
-            d += v * xd[i];
+   for (int rb = 0; rb < RB; rb++) {
+      const T2* x = xsd + (int64_t)(rhs0 + rb) * bs.panels;
+      T* asr = as + rb * r;
+      T* adr = ad + rb * r;
+      for (int base = 0; base < m; base += ch) {
+         const int cnt = min(ch, m - base);
+         __syncthreads();
+         for (int i = tid; i < cnt; i += blockDim.x) {
+            T2 v = x[src_panels[c.panel_off + base + i]];
+            xs[i] = v.x;
+            xd[i] = v.y;
          }
-         s = warp_sum(s);
-         d = warp_sum(d);
-         if (lane == 0) { as[j] += s; ad[j] += d; }
+         __syncthreads();
+         for (int j = warp; j < r; j += nwarps) {
+            const T* row = vt + c.vt_off + (int64_t)j * m + base;
+            T s = T(0), d = T(0);
+            for (int i = lane; i < cnt; i += 32) {
+               T v = row[i];
+               s += v * xs[i];
+               d += v * xd[i];
+            }
+            s = warp_sum(s);
+            d = warp_sum(d);
+            if (lane == 0) { asr[j] += s; adr[j] += d; }
+         }
       }
    }
    __syncthreads();
    // grid charges
    for (int q = tid; q < n3; q += blockDim.x) {
       const T2* col = pv + c.pv_off + q;
-      T acc = T(0);
+      T acc[RB];
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++) acc[rb] = T(0);
       for (int j = 0; j < r; j++) {
          T2 w = col[(int64_t)j * n3];
-         acc += w.x * as[j] + w.y * ad[j];
+#pragma unroll
+         for (int rb = 0; rb < RB; rb++) acc[rb] += w.x * as[rb * r + j] + w.y * ad[rb * r + j];
       }
-      g[q] = acc;
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++) g[rb * n3 + q] = acc[rb];
    }
    __syncthreads();
    // DFT along k (input index k + off), half spectrum kf < H
-   for (int idx = tid; idx < n * n * H; idx += blockDim.x) {
-      const int kf = idx % H, ij = idx / H;
-      const T* line = g + ij * n;
+   for (int idx = tid; idx < RB * NA; idx += blockDim.x) {
+      const int rb = idx / NA, e = idx - rb * NA;
+      const int kf = e % H, ij = e / H;
+      const T* line = g + rb * n3 + ij * n;
       T2 acc = Cx<T>::make(T(0), T(0));
       for (int k = 0; k < n; k++) {
          T2 w = tw[((k + off) * kf) % Np];
@@ -851,20 +879,23 @@ __global__ void __launch_bounds__(kFarThreads) far_forward_kernel(
    }
    __syncthreads();
    // along j
-   for (int idx = tid; idx < n * Np * H; idx += blockDim.x) {
-      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+   for (int idx = tid; idx < RB * NB; idx += blockDim.x) {
+      const int rb = idx / NB, e = idx - rb * NB;
+      const int kf = e % H, jf = (e / H) % Np, i = e / (H * Np);
+      const T2* Ar = A + rb * NA;
       T2 acc = Cx<T>::make(T(0), T(0));
-      for (int j = 0; j < n; j++) acc = Cx<T>::fma(A[(i * n + j) * H + kf], tw[((j + off) * jf) % Np], acc);
+      for (int j = 0; j < n; j++) acc = Cx<T>::fma(Ar[(i * n + j) * H + kf], tw[((j + off) * jf) % Np], acc);
       B[idx] = acc;
    }
    __syncthreads();
    // along i, straight to global
-   T2* out = spectra + c.spec_off;
-   for (int idx = tid; idx < Np * Np * H; idx += blockDim.x) {
-      const int kf = idx % H, jf = (idx / H) % Np, fi = idx / (H * Np);
+   for (int idx = tid; idx < RB * PG; idx += blockDim.x) {
+      const int rb = idx / PG, e = idx - rb * PG;
+      const int kf = e % H, jf = (e / H) % Np, fi = e / (H * Np);
+      const T2* Br = B + rb * NB;
       T2 acc = Cx<T>::make(T(0), T(0));
-      for (int i = 0; i < n; i++) acc = Cx<T>::fma(B[(i * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
-      out[idx] = acc;
+      for (int i = 0; i < n; i++) acc = Cx<T>::fma(Br[(i * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
+      spectra[(int64_t)(rhs0 + rb) * bs.spectra + c.spec_off + e] = acc;
    }
 }
 
@@ -1104,29 +1135,31 @@ __global__ void __launch_bounds__(kTranslateThreads, 2) translate_kernel(
    }
 }
 
-// One block per destination cube: the translated spectrum S, c2r DFT cropped at
-// offset n/2 and scaled by 1/(2n-1)^3, u = UTI g, values U u written to this
-// level's staging row of each point (Cube_multiply_U_UTI_IFFT, Cube.c:2156-2225).
-template <typename T>
+// One block per destination cube and RB right-hand sides: the translated spectrum S, c2r
+// DFT cropped at offset n/2 and scaled by 1/(2n-1)^3, u = UTI g, values U u written to
+// this level's staging row of each point (Cube_multiply_U_UTI_IFFT, Cube.c:2156-2225).
+// Every right-hand side goes through the arithmetic of RB = 1 (same loops and reduction
+// order); RB > 1 reads each UTI and U row once for RB right-hand sides.
+template <typename T, int RB>
 __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
     const DstDesc* __restrict__ cubes, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
    using T2 = typename Vec2<T>::type;
-   const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
-   translated += rhs * bs.translated;
-   staging += rhs * bs.staging;
+   const int ngrp = bs.nrhs / RB;
+   const int rhs0 = (blockIdx.x % ngrp) * RB, unit = blockIdx.x / ngrp;  // right-hand sides fastest
    extern __shared__ __align__(16) char smem_raw[];
    const DstDesc c = cubes[unit];
    const int n = c.n, Np = 2 * n - 1, H = n, off = n / 2, n3 = n * n * n, pg = Np * Np * H;
+   const int NA = n * n * H, NB = n * Np * H, r = c.r;
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
 
    char* p = smem_raw;
-   T2* S = carve<T2>(p, pg);
-   T2* P1 = carve<T2>(p, n * Np * H);
-   T2* P2 = carve<T2>(p, n * n * H);
-   T* g = carve<T>(p, n3);
-   T* u = carve<T>(p, c.r);
+   T2* S = carve<T2>(p, RB * pg);
+   T2* P1 = carve<T2>(p, RB * NB);
+   T2* P2 = carve<T2>(p, RB * NA);
+   T* g = carve<T>(p, RB * n3);
+   T* u = carve<T>(p, RB * r);
    T2* tw = carve<T2>(p, Np);
 
    for (int k = tid; k < Np; k += blockDim.x) {  // exp(+2 pi i k / Np)
@@ -1134,29 +1167,37 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
       Cx<T>::cis(k, Np, &cs, &sn);
       tw[k] = Cx<T>::make(cs, sn);
    }
-   for (int f = tid; f < pg; f += blockDim.x) S[f] = translated[c.s_off + f];
+   for (int f = tid; f < RB * pg; f += blockDim.x) {
+      const int rb = f / pg;
+      S[f] = translated[(int64_t)(rhs0 + rb) * bs.translated + c.s_off + (f - rb * pg)];
+   }
    __syncthreads();
    // inverse along i (output i < n only)
-   for (int idx = tid; idx < n * Np * H; idx += blockDim.x) {
-      const int kf = idx % H, jf = (idx / H) % Np, i = idx / (H * Np);
+   for (int idx = tid; idx < RB * NB; idx += blockDim.x) {
+      const int rb = idx / NB, e = idx - rb * NB;
+      const int kf = e % H, jf = (e / H) % Np, i = e / (H * Np);
+      const T2* Sr = S + rb * pg;
       T2 acc = Cx<T>::make(T(0), T(0));
-      for (int fi = 0; fi < Np; fi++) acc = Cx<T>::fma(S[(fi * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
+      for (int fi = 0; fi < Np; fi++) acc = Cx<T>::fma(Sr[(fi * Np + jf) * H + kf], tw[((i + off) * fi) % Np], acc);
       P1[idx] = acc;
    }
    __syncthreads();
    // inverse along j (output j < n only)
-   for (int idx = tid; idx < n * n * H; idx += blockDim.x) {
-      const int kf = idx % H, j = (idx / H) % n, i = idx / (H * n);
+   for (int idx = tid; idx < RB * NA; idx += blockDim.x) {
+      const int rb = idx / NA, e = idx - rb * NA;
+      const int kf = e % H, j = (e / H) % n, i = e / (H * n);
+      const T2* P1r = P1 + rb * NB;
       T2 acc = Cx<T>::make(T(0), T(0));
-      for (int jf = 0; jf < Np; jf++) acc = Cx<T>::fma(P1[(i * Np + jf) * H + kf], tw[((j + off) * jf) % Np], acc);
+      for (int jf = 0; jf < Np; jf++) acc = Cx<T>::fma(P1r[(i * Np + jf) * H + kf], tw[((j + off) * jf) % Np], acc);
       P2[idx] = acc;
    }
    __syncthreads();
    // Hermitian half along k -> real, cropped, scaled
    const T scale = T(1) / (T)(Np * Np * Np);
-   for (int q = tid; q < n3; q += blockDim.x) {
-      const int k = q % n, ij = q / n;
-      const T2* line = P2 + ij * H;
+   for (int q = tid; q < RB * n3; q += blockDim.x) {
+      const int rb = q / n3, e = q - rb * n3;
+      const int k = e % n, ij = e / n;
+      const T2* line = P2 + rb * NA + ij * H;
       T acc = line[0].x;
       for (int kf = 1; kf < H; kf++) {
          T2 w = tw[((k + off) * kf) % Np];
@@ -1166,21 +1207,38 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
    }
    __syncthreads();
    // u = UTI g
-   for (int j = warp; j < c.r; j += nwarps) {
+   for (int j = warp; j < r; j += nwarps) {
       const T* row = uti + c.uti_off + (int64_t)j * n3;
-      T s = T(0);
-      for (int q = lane; q < n3; q += 32) s += row[q] * g[q];
-      s = warp_sum(s);
-      if (lane == 0) u[j] = s;
+      T s[RB];
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++) s[rb] = T(0);
+      for (int q = lane; q < n3; q += 32) {
+         const T v = row[q];
+#pragma unroll
+         for (int rb = 0; rb < RB; rb++) s[rb] += v * g[rb * n3 + q];
+      }
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++) {
+         const T t = warp_sum(s[rb]);
+         if (lane == 0) u[rb * r + j] = t;
+      }
    }
    __syncthreads();
    // U u -> staging (each point belongs to exactly one cube of this level)
-   T* stage = staging + (int64_t)c.stage * total_points;
    for (int q = tid; q < c.p; q += blockDim.x) {
       const T* col = ucm + c.u_off + q;
-      T acc = T(0);
-      for (int j = 0; j < c.r; j++) acc += col[(int64_t)j * c.p] * u[j];
-      stage[dst_points[c.point_off + q]] = acc;
+      T acc[RB];
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++) acc[rb] = T(0);
+      for (int j = 0; j < r; j++) {
+         const T v = col[(int64_t)j * c.p];
+#pragma unroll
+         for (int rb = 0; rb < RB; rb++) acc[rb] += v * u[rb * r + j];
+      }
+      const int32_t pt = dst_points[c.point_off + q];
+#pragma unroll
+      for (int rb = 0; rb < RB; rb++)
+         staging[(int64_t)(rhs0 + rb) * bs.staging + (int64_t)c.stage * total_points + pt] = acc[rb];
    }
 }
 
@@ -2327,8 +2385,20 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    spectra_elems_ = std::max<int64_t>(L.spectra_elems, 1);
    translated_elems_ = std::max<int64_t>(L.translated_elems, 1);
    batch_capacity_ = 0;
-   raise_smem_limit(far_forward_kernel<T>, src_smem_);
-   raise_smem_limit(far_backward_kernel<T>, dst_smem_);
+   raise_smem_limit(far_forward_kernel<T, 1>, src_smem_);
+   raise_smem_limit(far_backward_kernel<T, 1>, dst_smem_);
+   smem_optin_ = optin;
+   int src_b = 1, dst_b = 1;
+   for (const LaunchGroup& g : src_groups_) {
+      const int b = far_batch_smem(g, far_rb<T>(), sizeof(T));
+      if (b <= optin) src_b = std::max(src_b, b);
+   }
+   for (const LaunchGroup& g : dst_groups_) {
+      const int b = far_batch_smem(g, far_rb<T>(), sizeof(T));
+      if (b <= optin) dst_b = std::max(dst_b, b);
+   }
+   raise_smem_limit(far_forward_kernel<T, far_rb<T>()>, src_b);
+   raise_smem_limit(far_backward_kernel<T, far_rb<T>()>, dst_b);
    raise_smem_limit(near_kernel<T>, leaf_smem_max_);
    raise_smem_limit(far_forward_t_kernel<T>, std::max(src_smem_t_, 1));
    raise_smem_limit(far_backward_t_kernel<T>, std::max(dst_smem_t_, 1));
@@ -2415,9 +2485,16 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
          far_forward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd,
                                                                          vt_.get(), pv_.get(), b.spectra, b.bs);
    } else {
-      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_forward_kernel<T><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
-          src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
+      constexpr int RB = far_rb<T>();
+      const int smem_b = far_batch_smem(g, RB, sizeof(T));
+      if (b.nrhs % RB == 0 && smem_b <= smem_optin_) {  // RB right-hand sides per block
+         far_forward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g.n), smem_b, stream>>>(
+             src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
+      } else {
+         const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+         far_forward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
+             src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
+      }
    }
    FFTSVD_CHECK_LAUNCH();
 }
@@ -2547,9 +2624,18 @@ void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cud
          far_backward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(
              c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
    } else {
-      const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-      far_backward_kernel<T><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
-          dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
+      constexpr int RB = far_rb<T>();
+      const int smem_b = far_batch_smem(g, RB, sizeof(T));
+      if (b.nrhs % RB == 0 && smem_b <= smem_optin_) {  // RB right-hand sides per block
+         far_backward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g.n), smem_b, stream>>>(
+             dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_,
+             b.bs);
+      } else {
+         const int smem = (int)(g.smem_elems * sizeof(T) + 128);
+         far_backward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
+             dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_,
+             b.bs);
+      }
    }
    FFTSVD_CHECK_LAUNCH();
 }

@@ -145,6 +145,9 @@ struct LaunchGroup {
    int count = 0;
    int smem_elems = 0;  // in units of the operator element type
    int max_rank = 0;    // largest row (sources) or column (destinations) rank
+   // shared memory of a block that serves several right-hand sides: batch_shared +
+   // right-hand sides x batch_per_rhs elements
+   int batch_shared = 0, batch_per_rhs = 0;
 };
 
 // Per-right-hand-side strides of the planar batch buffers: right-hand side r of a
@@ -285,6 +288,7 @@ class DeviceOperator {
    bool warp_path(const LaunchGroup& g) const;
    int warp_min_cubes_ = kWarpMinCubes;
    int sm_count_ = 148;
+   int smem_optin_ = 0;  // largest dynamic shared memory a block may opt into
    int64_t spectra_elems_ = 1, translated_elems_ = 1;
    int batch_capacity_ = 0;
    DevBuf<T2> xsd_b_, spectra_b_, translated_b_;
