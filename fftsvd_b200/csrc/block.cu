@@ -55,6 +55,8 @@ constexpr int kMaxPasses = 16;
 // A column whose norm falls below this fraction in the first Gram-Schmidt pass would be
 // left orthogonal to the basis only to eps / fraction: later steps then take two passes.
 constexpr double kReorthRatio = 1e-5;
+// Inner target of a mixed-precision pass, as a fraction of the tolerance.
+constexpr double kMixedTarget = 0.9;
 
 // G (K x K, symmetric, column-major, K <= kBlockMax) = R^T R: writes the upper-triangular
 // R (zero below the diagonal).  Right-looking, blocked by 32 rows: one warp factors the
@@ -158,6 +160,16 @@ __global__ void gather_scale_kernel(int64_t n, const double* __restrict__ src, c
    const double f = fac[a];
    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
       d[i] = f * s[i];
+}
+
+// grid (blocks, 1, columns): dst column idx[a] = src column a
+__global__ void scatter_copy_kernel(int64_t n, const double* __restrict__ src, const int32_t* __restrict__ idx,
+                                    double* __restrict__ dst) {
+   const int a = blockIdx.z;
+   const double* s = src + (int64_t)a * n;
+   double* d = dst + (int64_t)idx[a] * n;
+   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      d[i] = s[i];
 }
 
 // grid (blocks, 1, columns): dst column idx[a] += fac[a] * src column a
@@ -392,17 +404,39 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
                                   cudaMemcpyDeviceToDevice, stream));
       FFTSVD_CUDA(cudaMemsetAsync(B.Xc.get(), 0, sizeof(double) * (size_t)ncp * n, stream));
       std::vector<double> bn(nc, 0.0), rn(ncp, 0.0);
+      std::vector<int32_t> last;  // columns corrected by the last pass
       int used = 0;
       bool fallback = false;
       for (int pass = 0;; pass++) {
-         // Rc = P^-1 (B - A X), the outer operator (P^-1 B on the first pass)
+         // Rc = P^-1 (B - A X), the outer operator (P^-1 B on the first pass).  Only the
+         // columns corrected by the last pass change; when they are fewer than all, their
+         // residuals are computed as a compact block and scattered back.
          if (pass == 0) {
             precond_batch(B.Bc.get(), B.Rc.get(), ncp);
-         } else {
+         } else if ((int)last.size() == nc) {
             apply_batch(outer, B.Xc.get(), B.Tc.get(), ncp);
             sub_kernel<<<dim3(ew_blocks, 1, ncp), 256, 0, stream>>>(n, B.Bc.get(), B.Tc.get(), B.Tc.get(), n);
             FFTSVD_CHECK_LAUNCH();
             precond_batch(B.Tc.get(), B.Rc.get(), ncp);
+         } else {
+            const int nl = (int)last.size(), Kl = pad8(nl);
+            const std::vector<double> ones(nl, 1.0);
+            FFTSVD_CUDA(cudaMemcpyAsync(B.idx.get(), last.data(), sizeof(int32_t) * nl, cudaMemcpyHostToDevice, stream));
+            FFTSVD_CUDA(cudaMemcpyAsync(B.fac.get(), ones.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, stream));
+            FFTSVD_CUDA(cudaMemsetAsync(B.R0.get(), 0, sizeof(double) * (size_t)Kl * n, stream));
+            FFTSVD_CUDA(cudaMemsetAsync(B.T.get(), 0, sizeof(double) * (size_t)Kl * n, stream));
+            gather_scale_kernel<<<dim3(ew_blocks, 1, nl), 256, 0, stream>>>(n, B.Xc.get(), B.idx.get(), B.fac.get(),
+                                                                          B.R0.get());
+            FFTSVD_CHECK_LAUNCH();
+            gather_scale_kernel<<<dim3(ew_blocks, 1, nl), 256, 0, stream>>>(n, B.Bc.get(), B.idx.get(), B.fac.get(),
+                                                                          B.T.get());
+            FFTSVD_CHECK_LAUNCH();
+            apply_batch(outer, B.R0.get(), B.W.get(), Kl);
+            sub_kernel<<<dim3(ew_blocks, 1, Kl), 256, 0, stream>>>(n, B.T.get(), B.W.get(), B.W.get(), n);
+            FFTSVD_CHECK_LAUNCH();
+            precond_batch(B.W.get(), B.R0.get(), Kl);
+            scatter_copy_kernel<<<dim3(ew_blocks, 1, nl), 256, 0, stream>>>(n, B.R0.get(), B.idx.get(), B.Rc.get());
+            FFTSVD_CHECK_LAUNCH();
          }
          norm_partial_kernel<<<dim3(nb, 1, ncp), kVecThreads, 0, stream>>>(n, B.Rc.get(), B.part.get(), n, nb);
          FFTSVD_CHECK_LAUNCH();
@@ -430,11 +464,14 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
             }
             if (resid[c] < tol) continue;
             act.push_back(a);
-            // relative to the column's current residual: the single solve's inner target
-            // 0.3 tol / residual for a mixed correction, else the tolerance itself
-            target.push_back(mixed ? std::min(0.1, std::max(0.3 * tol / resid[c], 1e-13)) : tol / resid[c]);
+            // relative to the column's current residual: for a mixed correction 0.9 tol /
+            // residual (the FP32 operator's share of the FP64 residual is far below 0.1 tol on
+            // these surfaces, and a column that still misses the tolerance takes a short
+            // pass of its own), else the tolerance itself
+            target.push_back(mixed ? std::min(0.1, std::max(kMixedTarget * tol / resid[c], 1e-13)) : tol / resid[c]);
          }
          if (act.empty() || used >= maxit || pass >= kMaxPasses) break;
+         last = act;
          const int na = (int)act.size(), K = pad8(na);
          std::vector<double> f(na);
          for (int a = 0; a < na; a++) f[a] = 1.0 / rn[act[a]];
