@@ -46,6 +46,10 @@ CONFIGS = {
     # adjoint forces on the blob system, checked by central differences on seeded atoms
     "adjoint": dict(name="blob L6 (81920 panels, 2500 charges): adjoint dG/dx and dG/dq", kind="blob",
                     level=6, radius=22.0, nq=2500, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=1, fd_atoms=50),
+    # adjoint forces on the large blob, central differences on fewer seeded atoms
+    "adjoint_large": dict(name="large blob L7 (327680 panels, 30000 charges): adjoint dG/dx and dG/dq", kind="blob",
+                          level=7, radius=60.0, nq=30000, eps_in=4.0, eps_out=80.0, kappa=0.125, seed=3,
+                          fd_atoms=10),
     # many surfaces: 64 seeded blobs of level 3 to 6 solved concurrently
     "many": dict(name="64 seeded blobs, level 3-6 icospheres (1280-81920 panels), 50-2500 charges", kind="many",
                  surfaces=64, seed=5, eps_in=4.0, eps_out=80.0, kappa=0.125),
