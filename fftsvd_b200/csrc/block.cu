@@ -390,13 +390,15 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
    for (int c0 = 0; c0 < k; c0 += kBlockMax) {
       const int nc = std::min(kBlockMax, k - c0), ncp = pad8(nc);
       // basis: up to maxit blocks (at most 64), as many as a third of the device memory
-      // that is free or already held by the basis allows
+      // that is free or already held by the basis allows, counting the mmax + 11 blocks of
+      // K x n (basis and work vectors) and the dense (mmax K)^2 least-squares factor
       size_t free_b = 0, total_b = 0;
       FFTSVD_CUDA(cudaMemGetInfo(&free_b, &total_b));
       if (blk->n == n) free_b += blk->V.bytes() + blk->Rd.bytes();
       const size_t per_blk = sizeof(double) * (size_t)ncp * n;
-      const int cap = (int)std::max<int64_t>(2, (int64_t)(free_b / 3 / per_blk) - 10);
-      const int mmax = std::max(1, std::min({maxit, cap - 1, 64}));
+      int mmax = std::max(1, std::min(maxit, 64));
+      while (mmax > 1 && (mmax + 11) * per_blk + sizeof(double) * (size_t)mmax * ncp * (size_t)mmax * ncp > free_b / 3)
+         mmax--;
       blk->ensure(n, ncp, mmax, stream);
       BlockWorkspace& B = *blk;
       FFTSVD_CUDA(cudaMemsetAsync(B.Bc.get(), 0, sizeof(double) * (size_t)ncp * n, stream));
