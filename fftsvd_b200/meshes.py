@@ -81,6 +81,14 @@ def icosphere(level: int, radius: float = 1.0, center=(0.0, 0.0, 0.0)) -> np.nda
     return _triangles(v * radius + np.asarray(center, dtype=np.float64), f)
 
 
+def icosphere_mesh(level: int, radius: float = 1.0, center=(0.0, 0.0, 0.0)):
+    """The icosphere as shared vertices (nv, 3) and faces (nf, 3) of vertex indices, in the
+    corner order of icosphere()."""
+    v, f = _unit_icosphere(level)
+    f = np.asarray(f, dtype=np.int64)[:, [0, 2, 1]]  # the corner order _triangles emits
+    return v * radius + np.asarray(center, dtype=np.float64), np.ascontiguousarray(f)
+
+
 def _real_sph_harm_table(lmax: int, theta: np.ndarray, phi: np.ndarray):
     """Real spherical harmonics up to degree lmax (orthonormal), as a dict (l, m) -> values."""
     x = np.cos(theta)

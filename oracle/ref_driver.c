@@ -507,3 +507,54 @@ void oref_export_free(fftsvd_tree_flat* f) {
    free((void*)f->t_ops);
    memset(f, 0, sizeof(*f));
 }
+
+/* ---- input front end (FFTSVDpbeAPI.c), for checking the product's readers ----
+ * getFlatPanels (:676-712) and readSRF (:776-1032) return reference Panel objects; these
+ * copy their corner coordinates (FlatPanel.vertex, in FlatPanel_allocate order) to plain
+ * arrays.  The reference's own readers must only be given valid files: they exit on errors. */
+static unsigned int copy_flat(Panel* panels, unsigned int n, double* verts, unsigned int room) {
+   unsigned int i, k;
+   for (i = 0; i < n && i < room; i++) {
+      FlatPanel fp = (FlatPanel)panels[i]->realpanel;
+      for (k = 0; k < 3; k++) {
+         verts[9 * (size_t)i + 3 * k + 0] = fp->vertex[k]->x;
+         verts[9 * (size_t)i + 3 * k + 1] = fp->vertex[k]->y;
+         verts[9 * (size_t)i + 3 * k + 2] = fp->vertex[k]->z;
+      }
+   }
+   return n < room ? n : room;
+}
+
+unsigned int oref_flat_panels(const char* basename, unsigned int accessible, unsigned int cavity,
+                              unsigned int qualocation, double* verts, unsigned int maxpanels) {
+   Panel* panels = NULL;
+   unsigned int n = 0;
+   usequalocation = qualocation;
+   getFlatPanels(basename, &panels, &n, accessible, cavity);
+   usequalocation = 0;
+   copy_flat(panels, n, verts, maxpanels);
+   return n;
+}
+
+/* counts: numsalts, numdielectrics, numdielectriccavities, numsaltcavities, numtotalpanels.
+ * layer_n: panels per layer, salts then dielectrics, dielectric cavities, salt cavities.
+ * parents: dielectricparent, dielectriccavityparent, saltcavityparent, in that order.
+ * verts: the panels of all layers in the same order (at most maxpanels). */
+void oref_read_srf(const char* filename, unsigned int* counts, unsigned int* layer_n, unsigned int* parents,
+                   unsigned int maxlayers, double* verts, unsigned int maxpanels) {
+   Panel **sp = NULL, **dp = NULL, **dcp = NULL, **scp = NULL;
+   unsigned int *nsp = NULL, *ndp = NULL, *ndcp = NULL, *nscp = NULL;
+   unsigned int ns = 0, nd = 0, ndc = 0, nsc = 0, total = 0;
+   unsigned int *dpar = NULL, *dcpar = NULL, *scpar = NULL;
+   unsigned int i, l = 0, p = 0, done = 0;
+   readSRF(filename, &sp, &nsp, &ns, &dp, &ndp, &nd, &dpar, &dcp, &ndcp, &ndc, &dcpar, &scp, &nscp, &nsc, &scpar,
+           &total);
+   counts[0] = ns; counts[1] = nd; counts[2] = ndc; counts[3] = nsc; counts[4] = total;
+   for (i = 0; i < ns && l < maxlayers; i++, l++) { layer_n[l] = nsp[i]; done += copy_flat(sp[i], nsp[i], verts + 9 * (size_t)done, maxpanels - done); }
+   for (i = 0; i < nd && l < maxlayers; i++, l++) { layer_n[l] = ndp[i]; done += copy_flat(dp[i], ndp[i], verts + 9 * (size_t)done, maxpanels - done); }
+   for (i = 0; i < ndc && l < maxlayers; i++, l++) { layer_n[l] = ndcp[i]; done += copy_flat(dcp[i], ndcp[i], verts + 9 * (size_t)done, maxpanels - done); }
+   for (i = 0; i < nsc && l < maxlayers; i++, l++) { layer_n[l] = nscp[i]; done += copy_flat(scp[i], nscp[i], verts + 9 * (size_t)done, maxpanels - done); }
+   for (i = 0; i < nd && p < maxlayers; i++) parents[p++] = dpar[i];
+   for (i = 0; i < ndc && p < maxlayers; i++) parents[p++] = dcpar[i];
+   for (i = 0; i < nsc && p < maxlayers; i++) parents[p++] = scpar[i];
+}
