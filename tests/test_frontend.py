@@ -162,6 +162,45 @@ def test_first_record_reads_the_counting_pass_leftovers(lib, tmp_path):
     assert (ours[0].x, ours[0].y, ours[0].z) == (7.5, -8.25, 9.0)
 
 
+def test_crd_xyzr_and_modpdb_match_the_reference(lib, tmp_path):
+    crd = str(tmp_path / "mol.crd")
+    with open(crd, "w") as f:
+        f.write("* synthetic coordinates\n*\n    3\n")
+        for num, resn, res, atom, x, y, z, seg, temp in [(1, 1, "ALA", "N", 1.5, -2.0, 0.25, "PROA", 0.0),
+                                                         (2, 1, "ALA", "CA", 2.5, -1.0, 0.75, "PROA", 1.5),
+                                                         (3, 2, "GLY", "O", -0.5, 3.0, -1.25, "PROB", 2.0)]:
+            f.write(f"{num:5d}{resn:5d} {res:<4} {atom:<4}{x:10.5f}{y:10.5f}{z:10.5f} {seg:<4} {resn:<4} {temp:10.5f}\n")
+    xyzr = str(tmp_path / "mol.xyzr")
+    with open(xyzr, "w") as f:
+        f.write("1.0 2.0 3.0 1.5\n-4.25 0.5e1 6 2\n7.5 8.5\n")
+    lib.readCRD.argtypes = lib.readXYZR.argtypes = [C.c_char_p, C.POINTER(C.c_uint), C.POINTER(C.POINTER(CPDB))]
+    lib.writeMODPDB.argtypes = [C.c_char_p, C.POINTER(CPDB), C.c_uint]
+    for reader, ours in ((lib.readCRD, F.readCRD(crd)), (lib.readXYZR, F.readXYZR(xyzr))):
+        n, p = C.c_uint(), C.POINTER(CPDB)()
+        with ref.stdout_to_stderr():
+            reader((crd if reader is lib.readCRD else xyzr).encode(), C.byref(n), C.byref(p))
+        assert n.value == len(ours)
+        for i, e in enumerate(ours):
+            r = p[i]
+            assert (e.atomnumber, e.residuenumber, e.residuename, e.atomname, e.chain) == (
+                r.atomnumber, r.residuenumber, r.residuename.decode(), r.atomname.decode(), _ch(r.chain)), i
+            assert (e.x, e.y, e.z, e.temperature, e.radius) == (r.x, r.y, r.z, r.temperature, r.radius), i
+    pdb, siz, crg = _write_molecule(str(tmp_path))
+    n, rp = _ref_pdb(lib, pdb)
+    ours = F.readPDB(pdb)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        F.assignRadiiCharges(ours, F.readSIZ(siz), F.readCRG(crg))
+    for i, e in enumerate(ours):
+        rp[i].radius, rp[i].charge = e.radius, e.charge
+    out_ref, out_ours = str(tmp_path / "ref.pdb"), str(tmp_path / "ours.pdb")
+    with ref.stdout_to_stderr():
+        lib.writeMODPDB(out_ref.encode(), rp, n)
+    F.writeMODPDB(out_ours, ours)
+    with open(out_ref, "rb") as a, open(out_ours, "rb") as b:
+        assert a.read() == b.read()
+
+
 def test_params_match_the_reference(lib, tmp_path):
     path = str(tmp_path / "param.prm")
     with open(path, "w") as f:
