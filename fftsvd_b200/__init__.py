@@ -6,6 +6,8 @@ this package is its host-side mirror:
 * ``surface``  — Surface objects and the reference-named entry points
   (generateSurfaceOperator, generateRHS, solveSurfaceOperator, collectPotentials);
 * ``meshes``   — seeded synthetic surfaces and charge sets;
+* ``frontend`` — the reference's input readers (parameters, PDB/CRD/XYZR, SIZ/CRG,
+  vert/face meshes, SRF) and the FFTSVDpbe input sequence;
 * ``lib``      — the ctypes binding (fails loudly when the library is absent).
 """
 from .lib import FFTSVDError, load  # noqa: F401
