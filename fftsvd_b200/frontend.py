@@ -685,7 +685,29 @@ def writeMODPDB(path: str, atoms: list[PDBentry]) -> None:
                 a.chain or "\0", a.residuenumber, a.residueinsertion or "\0", a.x, a.y, a.z, a.radius, a.charge))
 
 
+def writeFRC(path: str, atoms: list[PDBentry], params: Params) -> None:
+    """Site potentials of the atoms (their `potential` fields) in the DelPhi FRC layout
+    (FFTSVDpbeAPI.c:535-567)."""
+    with open(path, "w") as f:
+        f.write("FFTSVDpbe SITE POTENTIAL FILE\n")
+        f.write("grid size,percent fill: %3d %8f\n" % (0, 0.0))
+        f.write("inner,outer dielectric: %8f %8f\n" % (params.innerdielectric, params.outerdielectric))
+        f.write("ionic strength (M): %8f\n" % params.ionicstrength)
+        f.write("ion excl., probe radius: %8f %8f\n" % (params.ionexclusionradius, params.proberadius))
+        f.write("linear, nolinear iterations: %8d %8d\n" % (0, 0))
+        f.write("boundary condition: %2d\n" % 0)
+        f.write("Data Output: COORDINATES CHARGE POTENTIALS FIELDS\n")
+        f.write("title: FFTSVDpbe: BEM PBE Solver\n")
+        f.write("\n")
+        f.write("\n")
+        f.write("    ATOM COORDINATES (X,Y,Z)     CHARGE   GRID PT.    GRID FIELDS: (Ex, Ey, Ez)\n")
+        for a in atoms:
+            f.write("%9.3f%9.3f%9.3f%8.4f%15.6f  %9.4f%9.4f%9.4f\n" % (a.x, a.y, a.z, a.charge, a.potential, 0.0, 0.0,
+                                                                     0.0))
+        f.write("total energy =   %6f  kt\n" % 0.0)
+
+
 __all__ = ["FrontEndError", "Params", "PDBentry", "SIZentry", "CRGentry", "SRF", "PBESystem", "readParams",
            "checkParams", "readPDB", "readCRD", "readXYZR", "readSIZ", "readCRG", "assignRadiiCharges",
-           "getFlatPanels", "readSRF", "pbe_system", "pbe_surface", "write_vert_face", "writeMODPDB", "KT_CONVERSION",
+           "getFlatPanels", "readSRF", "pbe_system", "pbe_surface", "write_vert_face", "writeMODPDB", "writeFRC", "KT_CONVERSION",
            "DEBYE_CONSTANT"]

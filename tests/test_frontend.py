@@ -199,6 +199,19 @@ def test_crd_xyzr_and_modpdb_match_the_reference(lib, tmp_path):
     F.writeMODPDB(out_ours, ours)
     with open(out_ref, "rb") as a, open(out_ours, "rb") as b:
         assert a.read() == b.read()
+    # site potentials: the FRC writer with the reference's parameter globals
+    params = F.Params(innerdielectric=4.0, outerdielectric=80.0, ionicstrength=0.145, ionexclusionradius=2.0,
+                      proberadius=1.4)
+    for nm in ("innerdielectric", "outerdielectric", "ionicstrength", "ionexclusionradius", "proberadius"):
+        C.c_double.in_dll(lib, nm).value = getattr(params, nm)
+    for i, e in enumerate(ours):
+        e.potential = rp[i].potential = 0.125 * (i + 1) - 0.3
+    lib.writeFRC.argtypes = [C.c_char_p, C.POINTER(CPDB), C.c_uint]
+    with ref.stdout_to_stderr():
+        lib.writeFRC(out_ref.encode(), rp, n)
+    F.writeFRC(out_ours, ours, params)
+    with open(out_ref, "rb") as a, open(out_ours, "rb") as b:
+        assert a.read() == b.read()
 
 
 def test_params_match_the_reference(lib, tmp_path):
