@@ -70,7 +70,7 @@ def tree_multiplyboth(t: dict, xs: np.ndarray, xd: np.ndarray) -> np.ndarray:
             any_src = True
         if not any_src:
             continue
-        gp = np.fft.irfftn(S, s=(Np, Np, Np))[off:off + n, off:off + n, off:off + n].ravel()
+        gp = np.fft.irfftn(S, s=(Np, Np, Np), axes=(0, 1, 2))[off:off + n, off:off + n, off:off + n].ravel()
         UTI = t["uti"][t["cube_uti_ptr"][d]:t["cube_uti_ptr"][d + 1]].reshape(r, n ** 3)
         U = t["u"][t["cube_u_ptr"][d]:t["cube_u_ptr"][d + 1]].reshape(len(points), r)
         b[points] += U @ (UTI @ gp)

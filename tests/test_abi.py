@@ -15,7 +15,8 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 
 def declared_functions():
-    text = open(HEADER).read()
+    with open(HEADER) as f:
+        text = f.read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = set(re.findall(r"\b(fftsvd_b200_\w+)\s*\(", text))
     names |= set(re.findall(r"\bvoid\s+(solveSurfaceOperator|generateRHS|collectPotentials)\s*\(", text))
