@@ -596,58 +596,86 @@ void Tree::flatten(FlatTree& F) const {
    F.num_points = (int)(points->size() / 3);
    F.depth = depth;
    F.grid = grid;
-   for (const Cube& c : cubes) {
-      if (!c.leaf || c.points.empty() || c.dcols.empty()) continue;
-      F.leaf_row_ptr.push_back((int32_t)F.leaf_rows.size());
-      F.leaf_col_ptr.push_back((int32_t)F.leaf_cols.size());
-      F.leaf_d_ptr.push_back((int64_t)F.d_single.size());
-      F.leaf_rows.insert(F.leaf_rows.end(), c.points.begin(), c.points.end());
-      F.leaf_cols.insert(F.leaf_cols.end(), c.dcols.begin(), c.dcols.end());
-      F.d_single.insert(F.d_single.end(), c.Ds.begin(), c.Ds.end());
-      F.d_double.insert(F.d_double.end(), c.Dd.begin(), c.Dd.end());
-   }
-   F.leaf_row_ptr.push_back((int32_t)F.leaf_rows.size());
-   F.leaf_col_ptr.push_back((int32_t)F.leaf_cols.size());
-   F.leaf_d_ptr.push_back((int64_t)F.d_single.size());
-   std::vector<int> flat_of(cubes.size(), -1);
-   int nc = 0;
-   for (size_t i = 0; i < cubes.size(); i++)
-      if (!cubes[i].inter.empty()) flat_of[i] = nc++;
+   // offsets first (serial, cheap), then every leaf's and cube's blocks copied in parallel
+   std::vector<int> leaves, fcubes, flat_of(cubes.size(), -1);
    for (size_t i = 0; i < cubes.size(); i++) {
       const Cube& c = cubes[i];
-      if (c.inter.empty()) continue;
-      F.cube_level.push_back(c.level);
-      for (int k = 0; k < 3; k++) F.cube_index.push_back(c.idx[k]);
-      F.cube_panel_ptr.push_back((int32_t)F.cube_panels.size());
-      F.cube_panels.insert(F.cube_panels.end(), c.panels.begin(), c.panels.end());
-      F.cube_point_ptr.push_back((int32_t)F.cube_points.size());
-      F.cube_points.insert(F.cube_points.end(), c.points.begin(), c.points.end());
-      F.cube_row_rank.push_back(c.rowrank);
-      F.cube_col_rank.push_back(c.colrank);
-      F.cube_vt_ptr.push_back((int64_t)F.vt.size());
-      F.cube_pv_ptr.push_back((int64_t)F.pv_single.size());
-      F.cube_uti_ptr.push_back((int64_t)F.uti.size());
-      F.cube_u_ptr.push_back((int64_t)F.u.size());
-      if (c.rowrank > 0) {
-         F.vt.insert(F.vt.end(), c.VT.begin(), c.VT.end());
-         F.pv_single.insert(F.pv_single.end(), c.PVs.begin(), c.PVs.end());
-         F.pv_double.insert(F.pv_double.end(), c.PVd.begin(), c.PVd.end());
+      if (c.leaf && !c.points.empty() && !c.dcols.empty()) leaves.push_back((int)i);
+      if (!c.inter.empty()) {
+         flat_of[i] = (int)fcubes.size();
+         fcubes.push_back((int)i);
       }
-      if (c.colrank > 0) {
-         F.uti.insert(F.uti.end(), c.UTI.begin(), c.UTI.end());
-         F.u.insert(F.u.end(), c.U.begin(), c.U.end());
+   }
+   const int nl = (int)leaves.size(), nc = (int)fcubes.size();
+   F.leaf_row_ptr.assign(nl + 1, 0);
+   F.leaf_col_ptr.assign(nl + 1, 0);
+   F.leaf_d_ptr.assign(nl + 1, 0);
+   for (int l = 0; l < nl; l++) {
+      const Cube& c = cubes[leaves[l]];
+      F.leaf_row_ptr[l + 1] = F.leaf_row_ptr[l] + (int32_t)c.points.size();
+      F.leaf_col_ptr[l + 1] = F.leaf_col_ptr[l] + (int32_t)c.dcols.size();
+      F.leaf_d_ptr[l + 1] = F.leaf_d_ptr[l] + (int64_t)c.Ds.size();
+   }
+   F.leaf_rows.resize(F.leaf_row_ptr[nl]);
+   F.leaf_cols.resize(F.leaf_col_ptr[nl]);
+   F.d_single.resize(F.leaf_d_ptr[nl]);
+   F.d_double.resize(F.leaf_d_ptr[nl]);
+   F.cube_level.resize(nc);
+   F.cube_index.resize(3 * (size_t)nc);
+   F.cube_row_rank.resize(nc);
+   F.cube_col_rank.resize(nc);
+   for (auto* v : {&F.cube_panel_ptr, &F.cube_point_ptr, &F.inter_ptr}) v->assign(nc + 1, 0);
+   for (auto* v : {&F.cube_vt_ptr, &F.cube_pv_ptr, &F.cube_uti_ptr, &F.cube_u_ptr}) v->assign(nc + 1, 0);
+   for (int k = 0; k < nc; k++) {
+      const Cube& c = cubes[fcubes[k]];
+      F.cube_panel_ptr[k + 1] = F.cube_panel_ptr[k] + (int32_t)c.panels.size();
+      F.cube_point_ptr[k + 1] = F.cube_point_ptr[k] + (int32_t)c.points.size();
+      F.inter_ptr[k + 1] = F.inter_ptr[k] + (int32_t)c.inter.size();
+      F.cube_vt_ptr[k + 1] = F.cube_vt_ptr[k] + (c.rowrank > 0 ? (int64_t)c.VT.size() : 0);
+      F.cube_pv_ptr[k + 1] = F.cube_pv_ptr[k] + (c.rowrank > 0 ? (int64_t)c.PVs.size() : 0);
+      F.cube_uti_ptr[k + 1] = F.cube_uti_ptr[k] + (c.colrank > 0 ? (int64_t)c.UTI.size() : 0);
+      F.cube_u_ptr[k + 1] = F.cube_u_ptr[k] + (c.colrank > 0 ? (int64_t)c.U.size() : 0);
+   }
+   F.cube_panels.resize(F.cube_panel_ptr[nc]);
+   F.cube_points.resize(F.cube_point_ptr[nc]);
+   F.inter_cubes.resize(F.inter_ptr[nc]);
+   F.vt.resize(F.cube_vt_ptr[nc]);
+   F.pv_single.resize(F.cube_pv_ptr[nc]);
+   F.pv_double.resize(F.cube_pv_ptr[nc]);
+   F.uti.resize(F.cube_uti_ptr[nc]);
+   F.u.resize(F.cube_u_ptr[nc]);
+#pragma omp parallel
+   {
+#pragma omp for schedule(dynamic, 16) nowait
+      for (int l = 0; l < nl; l++) {
+         const Cube& c = cubes[leaves[l]];
+         std::copy(c.points.begin(), c.points.end(), F.leaf_rows.begin() + F.leaf_row_ptr[l]);
+         std::copy(c.dcols.begin(), c.dcols.end(), F.leaf_cols.begin() + F.leaf_col_ptr[l]);
+         std::copy(c.Ds.begin(), c.Ds.end(), F.d_single.begin() + F.leaf_d_ptr[l]);
+         std::copy(c.Dd.begin(), c.Dd.end(), F.d_double.begin() + F.leaf_d_ptr[l]);
       }
-      F.inter_ptr.push_back((int32_t)F.inter_cubes.size());
-      for (int o : c.inter) F.inter_cubes.push_back(flat_of[o]);
+#pragma omp for schedule(dynamic, 16)
+      for (int k = 0; k < nc; k++) {
+         const Cube& c = cubes[fcubes[k]];
+         F.cube_level[k] = c.level;
+         for (int q = 0; q < 3; q++) F.cube_index[3 * (size_t)k + q] = c.idx[q];
+         F.cube_row_rank[k] = c.rowrank;
+         F.cube_col_rank[k] = c.colrank;
+         std::copy(c.panels.begin(), c.panels.end(), F.cube_panels.begin() + F.cube_panel_ptr[k]);
+         std::copy(c.points.begin(), c.points.end(), F.cube_points.begin() + F.cube_point_ptr[k]);
+         for (size_t q = 0; q < c.inter.size(); q++) F.inter_cubes[F.inter_ptr[k] + q] = flat_of[c.inter[q]];
+         if (c.rowrank > 0) {
+            std::copy(c.VT.begin(), c.VT.end(), F.vt.begin() + F.cube_vt_ptr[k]);
+            std::copy(c.PVs.begin(), c.PVs.end(), F.pv_single.begin() + F.cube_pv_ptr[k]);
+            std::copy(c.PVd.begin(), c.PVd.end(), F.pv_double.begin() + F.cube_pv_ptr[k]);
+         }
+         if (c.colrank > 0) {
+            std::copy(c.UTI.begin(), c.UTI.end(), F.uti.begin() + F.cube_uti_ptr[k]);
+            std::copy(c.U.begin(), c.U.end(), F.u.begin() + F.cube_u_ptr[k]);
+         }
+      }
    }
    F.num_cubes = nc;
-   F.cube_panel_ptr.push_back((int32_t)F.cube_panels.size());
-   F.cube_point_ptr.push_back((int32_t)F.cube_points.size());
-   F.cube_vt_ptr.push_back((int64_t)F.vt.size());
-   F.cube_pv_ptr.push_back((int64_t)F.pv_single.size());
-   F.cube_uti_ptr.push_back((int64_t)F.uti.size());
-   F.cube_u_ptr.push_back((int64_t)F.u.size());
-   F.inter_ptr.push_back((int32_t)F.inter_cubes.size());
    int64_t off = 0;
    for (int d = 0; d < depth; d++) {
       F.t_level_ptr.push_back(off);
