@@ -557,16 +557,25 @@ void Tree::fill_bases() {
                   Pd[(size_t)g * m + k] += a * Qd[(size_t)q * m + k];
                }
             }
+         // VT transposed, so that the innermost loop runs over contiguous j; every PV entry
+         // still accumulates over k in ascending order
+         std::vector<double> VTt((size_t)m * r);
+         for (int j = 0; j < r; j++)
+            for (int k = 0; k < m; k++) VTt[(size_t)k * r + j] = c.VT[(size_t)j * m + k];
          c.PVs.assign((size_t)gp3 * r, 0.0);
          c.PVd.assign((size_t)gp3 * r, 0.0);
-         for (int g = 0; g < gp3; g++)
+         for (int g = 0; g < gp3; g++) {
+            double* pvs = &c.PVs[(size_t)g * r];
+            double* pvd = &c.PVd[(size_t)g * r];
             for (int k = 0; k < m; k++) {
                const double ps = Ps[(size_t)g * m + k], pd = Pd[(size_t)g * m + k];
+               const double* vt = &VTt[(size_t)k * r];
                for (int j = 0; j < r; j++) {
-                  c.PVs[(size_t)g * r + j] += ps * c.VT[(size_t)j * m + k];
-                  c.PVd[(size_t)g * r + j] += pd * c.VT[(size_t)j * m + k];
+                  pvs[j] += ps * vt[j];
+                  pvd[j] += pd * vt[j];
                }
             }
+         }
       }
       if (np > 0 && c.colrank > 0) {
          // I^T = (pinv Q2S_points)^T (np x gp3); UTI = U^T I^T (r x gp3)
@@ -574,12 +583,19 @@ void Tree::fill_bases() {
          std::vector<double> Qp((size_t)kNumSphere * np);
          for (int q = 0; q < kNumSphere; q++)
             for (int k = 0; k < np; k++) Qp[(size_t)q * np + k] = kernel.point(&(*points)[3 * (size_t)c.points[k]], sphere[q]);
-         std::vector<double> It((size_t)np * gp3, 0.0);
-         for (int g = 0; g < gp3; g++)
+         // accumulated transposed (contiguous in k; each entry still sums over q in ascending
+         // order), then turned back into np x gp3
+         std::vector<double> ItT((size_t)gp3 * np, 0.0), It((size_t)np * gp3);
+         for (int g = 0; g < gp3; g++) {
+            double* it = &ItT[(size_t)g * np];
             for (int q = 0; q < kNumSphere; q++) {
                const double a = Pi[(size_t)g * kNumSphere + q];
-               for (int k = 0; k < np; k++) It[(size_t)k * gp3 + g] += a * Qp[(size_t)q * np + k];
+               const double* qp = &Qp[(size_t)q * np];
+               for (int k = 0; k < np; k++) it[k] += a * qp[k];
             }
+         }
+         for (int g = 0; g < gp3; g++)
+            for (int k = 0; k < np; k++) It[(size_t)k * gp3 + g] = ItT[(size_t)g * np + k];
          c.UTI.assign((size_t)r * gp3, 0.0);
          for (int k = 0; k < np; k++)
             for (int j = 0; j < r; j++) {
