@@ -28,6 +28,10 @@ _libs = {}
 
 
 def library_path(fp64: bool) -> str:
+    """The compiled reference; FFTSVD_REF_LIB names another build of it (the CPU baseline
+    table times the as-shipped build through it)."""
+    if not fp64 and os.environ.get("FFTSVD_REF_LIB"):
+        return os.environ["FFTSVD_REF_LIB"]
     return os.path.join(REF_DIR, "libfftsvd_ref64.so" if fp64 else "libfftsvd_ref.so")
 
 
