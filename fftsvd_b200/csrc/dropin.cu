@@ -3,6 +3,8 @@
 //
 //   solveSurfaceOperator  FFTSVDpbeAPI.c:1884-1888 -> GMRES_SurfaceOperator (GMRES.c:446-539)
 //   generateRHS           FFTSVDpbeAPI.c:1871-1876 -> SurfaceOperator_makeRHS (SurfaceOperator.c:291-321)
+//   collectPotentials     FFTSVDpbeAPI.c:1896-1922 -> SurfaceOperator_calculateReactionPotentials,
+//                         direct branch (SurfaceOperator.c:364-401), plus the optional Coulomb sum
 //
 // The reference structures (layout in refabi.h) are read, never modified.  On
 // the first solve for a given (SurfaceOperator, Preconditioner) pair the
@@ -11,7 +13,10 @@
 // calls.  Errors are reported on stderr and leave *solution / *rhs NULL instead
 // of exiting the process.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
+#include <array>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -21,6 +26,7 @@
 #include <utility>
 #include <vector>
 
+#include "nbody.h"
 #include "refabi.h"
 #include "setup.h"
 #include "surface.h"
@@ -28,6 +34,12 @@
 // The reference keeps the GMRES tolerance in this process global
 // (FFTSVDpbeAPI.c:25); weak so that the library also links without it.
 extern "C" double errortolerance __attribute__((weak));
+// Parameters of collectPotentials, process globals of the reference API
+// (FFTSVDpbeAPI.c:20, 29).  Weak references make a program linked with the
+// reference objects export them to this library; a program that loads the
+// reference objects at run time is searched with dlsym instead.
+extern "C" double innerdielectric __attribute__((weak));
+extern "C" unsigned int addcoulombic __attribute__((weak));
 
 namespace fftsvd {
 namespace {
@@ -258,6 +270,121 @@ void rhs_region(const ref::SurfaceOperator* so, double* drhs) {
    for (unsigned k = 0; k < so->numchildren; k++) rhs_region(so->children[k], drhs);
 }
 
+template <typename T>
+const T* api_global(const T* weak_address, const char* name) {
+   if (weak_address) return weak_address;
+   return static_cast<const T*>(dlsym(RTLD_DEFAULT, name));
+}
+
+// Geometry of a reference flat panel from its stored vertices (FlatPanel.c:5-35).
+void reference_flat_panel(const ref::Panel* p, FlatPanel& out) {
+   FFTSVD_REQUIRE(p && p->type == 0 && p->realpanel, "only flat panels are supported");
+   const ref::FlatPanel* f = static_cast<const ref::FlatPanel*>(p->realpanel);
+   double v[3][3];
+   for (int k = 0; k < 3; k++) {
+      FFTSVD_REQUIRE(f->vertex[k], "flat panel without vertices");
+      v[k][0] = f->vertex[k]->x;
+      v[k][1] = f->vertex[k]->y;
+      v[k][2] = f->vertex[k]->z;
+   }
+   make_flat_panel(out, v[0], v[1], v[2]);
+}
+
+// Reaction potentials of every region that holds charges, added at
+// pot[charges->globalindexstart + j] (SurfaceOperator.c:364-401, direct
+// branch, recursing over the children).  A region's own panels enter with
+// (phi, dphi) and the coincidence term; its children's panels with
+// (-phi, -eps_child/eps dphi) and no coincidence term.  One launch serves both:
+// the scaled densities are laid out per panel, and the coincidence term the
+// kernel adds for a child panel (+4 pi phi) is taken off on the host.
+void reaction_regions(const ref::SurfaceOperator* so, const double* sol, std::vector<double>& pot) {
+   FFTSVD_REQUIRE(!so->M3, "regions with an M3 tree (accelerateM3) are not supported");
+   const ref::Charge* Q = so->charges;
+   if (Q && Q->numcharges > 0) {
+      const size_t nq = Q->numcharges, g0 = Q->globalindexstart;
+      FFTSVD_REQUIRE(g0 + nq <= pot.size(), "charges of a region lie beyond the collected entries");
+      std::vector<FlatPanel> panels;
+      std::vector<double> dens;
+      std::vector<int32_t> phi_row, dphi_row;
+      auto add_panel = [&](const ref::Panel* p, double phi, double dphi) {
+         panels.emplace_back();
+         reference_flat_panel(p, panels.back());
+         phi_row.push_back((int32_t)dens.size());
+         dens.push_back(phi);
+         dphi_row.push_back((int32_t)dens.size());
+         dens.push_back(dphi);
+      };
+      FFTSVD_REQUIRE(so->mynumpanels == 0 || (so->tree && so->tree->numpanels >= so->mynumpanels),
+                     "region panels do not match its tree");
+      for (unsigned i = 0; i < so->mynumpanels; i++)
+         add_panel(so->tree->panels[i], sol[so->startphi + i], sol[so->startdphi + i]);
+      // charge index -> coincident child panel phi values (exact centroid equality)
+      std::map<std::array<double, 3>, double> child_centroid_phi;
+      for (unsigned k = 0; k < so->numchildren; k++) {
+         const ref::SurfaceOperator* ch = so->children[k];
+         FFTSVD_REQUIRE(ch->mynumpanels == 0 || (ch->tree && ch->tree->numpanels >= ch->mynumpanels),
+                        "child region panels do not match its tree");
+         const double ratio = -ch->epsilon / so->epsilon;
+         for (unsigned i = 0; i < ch->mynumpanels; i++) {
+            const double phi = sol[ch->startphi + i];
+            add_panel(ch->tree->panels[i], -phi, ratio * sol[ch->startdphi + i]);
+            const FlatPanel& P = panels.back();
+            child_centroid_phi[{P.centroid[0], P.centroid[1], P.centroid[2]}] += phi;
+         }
+      }
+      std::vector<double> qpos(3 * nq);
+      for (size_t j = 0; j < nq; j++) {
+         FFTSVD_REQUIRE(Q->points[j], "charge without a position");
+         qpos[3 * j] = Q->points[j]->x;
+         qpos[3 * j + 1] = Q->points[j]->y;
+         qpos[3 * j + 2] = Q->points[j]->z;
+      }
+      std::vector<double> phi(nq, 0.0);
+      if (!panels.empty()) {
+         DevBuf<FlatPanel> d_panels;
+         DevBuf<int32_t> d_phi_row, d_dphi_row;
+         DevBuf<double> d_dens, d_qpos, d_out(nq);
+         d_panels.upload(panels);
+         d_phi_row.upload(phi_row);
+         d_dphi_row.upload(dphi_row);
+         d_dens.upload(dens);
+         d_qpos.upload(qpos);
+         reaction_points_device((int)panels.size(), d_panels.get(), d_phi_row.get(), d_dphi_row.get(), d_dens.get(),
+                                (int)nq, d_qpos.get(), d_out.get(), 0);
+         FFTSVD_CUDA(cudaMemcpy(phi.data(), d_out.get(), sizeof(double) * nq, cudaMemcpyDeviceToHost));
+      }
+      for (size_t j = 0; j < nq; j++) {
+         if (!child_centroid_phi.empty()) {
+            auto it = child_centroid_phi.find({qpos[3 * j], qpos[3 * j + 1], qpos[3 * j + 2]});
+            if (it != child_centroid_phi.end()) phi[j] -= 4.0 * M_PI * it->second;
+         }
+         pot[g0 + j] += phi[j];
+      }
+   }
+   for (unsigned k = 0; k < so->numchildren; k++) reaction_regions(so->children[k], sol, pot);
+}
+
+// The Coulomb term of collectPotentials (FFTSVDpbeAPI.c:1906-1919): one thread
+// per collected atom, input atoms in their order, pot[c] += kt q_a / (eps d).
+__global__ void coulomb_kernel(int nc, const double* __restrict__ cpos, int ni, const double* __restrict__ ipos,
+                               const double* __restrict__ iq, double kt, double eps, double* __restrict__ pot) {
+   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+   if (c >= nc) return;
+   const double x = cpos[3 * c], y = cpos[3 * c + 1], z = cpos[3 * c + 2];
+   double p = pot[c];
+   for (int a = 0; a < ni; a++) {
+      const double dx = ipos[3 * a] - x, dy = ipos[3 * a + 1] - y, dz = ipos[3 * a + 2] - z;
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      if (d > 0.0) p += kt * iq[a] / (eps * d);
+   }
+   pot[c] = p;
+}
+
+void charge_epsilons(const ref::SurfaceOperator* so, std::vector<double>& eps) {
+   if (so->charges && so->charges->numcharges > 0) eps.push_back(so->epsilon);
+   for (unsigned k = 0; k < so->numchildren; k++) charge_epsilons(so->children[k], eps);
+}
+
 }  // namespace
 }  // namespace fftsvd
 
@@ -309,5 +436,65 @@ extern "C" void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceope
    } catch (const std::exception& e) {
       set_last_error(e.what());
       std::fprintf(stderr, "fftsvd_b200 generateRHS: %s\n", e.what());
+   }
+}
+
+extern "C" void collectPotentials(struct PDBentry_s* PDBcollectentries, unsigned int numPDBcollectentries,
+                                  struct PDBentry_s* PDBinputentries, unsigned int numPDBinputentries,
+                                  struct _SurfaceOperator* pbesurfaceoperator, double* solution) {
+   constexpr double kKTConversion = 561.0;  // FFTSVDpbeAPI.h:13
+   try {
+      FFTSVD_REQUIRE(pbesurfaceoperator && solution, "null argument");
+      FFTSVD_REQUIRE(numPDBcollectentries == 0 || PDBcollectentries, "null collect entries");
+      FFTSVD_REQUIRE(numPDBinputentries == 0 || PDBinputentries, "null input entries");
+      const ref::SurfaceOperator* so = reinterpret_cast<const ref::SurfaceOperator*>(pbesurfaceoperator);
+      ref::PDBentry* collect = reinterpret_cast<ref::PDBentry*>(PDBcollectentries);
+      const ref::PDBentry* input = reinterpret_cast<const ref::PDBentry*>(PDBinputentries);
+      double eps_in = 0.0;
+      if (const double* g = api_global(&innerdielectric, "innerdielectric")) {
+         eps_in = *g;
+      } else {
+         std::vector<double> eps;
+         charge_epsilons(so, eps);
+         FFTSVD_REQUIRE(!eps.empty(), "innerdielectric is not defined and no region holds charges");
+         for (double e : eps)
+            FFTSVD_REQUIRE(e == eps[0], "innerdielectric is not defined and the charged regions differ in epsilon");
+         eps_in = eps[0];
+      }
+      FFTSVD_REQUIRE(eps_in > 0.0, "innerdielectric must be positive");
+      const unsigned int* coul = api_global(&addcoulombic, "addcoulombic");
+      const size_t nc = numPDBcollectentries;
+      std::vector<double> pot(nc, 0.0);
+      reaction_regions(so, solution, pot);
+      for (size_t a = 0; a < nc; a++) pot[a] = kKTConversion * pot[a] / eps_in;
+      if (coul && *coul && nc > 0) {
+         std::vector<double> cpos(3 * nc), ipos, iq;
+         for (size_t c = 0; c < nc; c++) {
+            cpos[3 * c] = collect[c].x;
+            cpos[3 * c + 1] = collect[c].y;
+            cpos[3 * c + 2] = collect[c].z;
+         }
+         for (unsigned a = 0; a < numPDBinputentries; a++)
+            if (std::toupper((unsigned char)input[a].chain) != 'X') {
+               ipos.insert(ipos.end(), {input[a].x, input[a].y, input[a].z});
+               iq.push_back(input[a].charge);
+            }
+         if (!iq.empty()) {
+            DevBuf<double> dcpos, dipos, diq, dpot;
+            dcpos.upload(cpos);
+            dipos.upload(ipos);
+            diq.upload(iq);
+            dpot.upload(pot);
+            const int ncol = (int)nc;
+            coulomb_kernel<<<(ncol + 127) / 128, 128>>>(ncol, dcpos.get(), (int)iq.size(), dipos.get(), diq.get(),
+                                                         kKTConversion, eps_in, dpot.get());
+            FFTSVD_CHECK_LAUNCH();
+            FFTSVD_CUDA(cudaMemcpy(pot.data(), dpot.get(), sizeof(double) * nc, cudaMemcpyDeviceToHost));
+         }
+      }
+      for (size_t a = 0; a < nc; a++) collect[a].potential = pot[a];
+   } catch (const std::exception& e) {
+      set_last_error(e.what());
+      std::fprintf(stderr, "fftsvd_b200 collectPotentials: %s\n", e.what());
    }
 }

@@ -175,6 +175,26 @@ void reaction_device(Surface& S, const double* sol, double* phi) {
    FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
 }
 
+void reaction_points_device(int np, const FlatPanel* panels, const int32_t* phi_row, const int32_t* dphi_row,
+                            const double* dens, int nq, const double* qpos, double* phi, cudaStream_t stream) {
+   FFTSVD_REQUIRE(np >= 0 && nq >= 0, "negative panel or point count");
+   if (nq == 0) return;
+   if (np == 0) {
+      FFTSVD_CUDA(cudaMemsetAsync(phi, 0, sizeof(double) * nq, stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(stream));
+      return;
+   }
+   const int chunks = std::max(1, std::min(kReactChunks, (np + kReactPanelTile - 1) / kReactPanelTile));
+   DevBuf<double> partial((size_t)chunks * nq);
+   dim3 grid((nq + kReactThreads - 1) / kReactThreads, chunks);
+   reaction_partial_kernel<<<grid, kReactThreads, 0, stream>>>(np, panels, phi_row, dphi_row, dens, nq, qpos,
+                                                               partial.get(), nullptr, 0);
+   FFTSVD_CHECK_LAUNCH();
+   reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, stream>>>(nq, chunks, partial.get(), phi);
+   FFTSVD_CHECK_LAUNCH();
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+}
+
 double energy_device(Surface& S, const double* phi) {
    std::vector<double> h(S.num_charges);
    if (S.num_charges == 0) return 0.0;

@@ -27,6 +27,12 @@ void set_charges(Surface& S, int num_charges, const double* pos, const double* q
 void rhs_device(Surface& S, double* rhs);
 // phi_j = sum_i (dphi_i SLP(x_j, i) - phi_i DLP(x_j, i)) - 4 pi phi_i [x_j == c_i].  Device pointers.
 void reaction_device(Surface& S, const double* sol, double* phi);
+// The same sum for nq points against an explicit panel set, all device arrays:
+// phi_j = sum_k (dens[dphi_row[k]] SLP(x_j, k) - dens[phi_row[k]] DLP(x_j, k))
+//         - 4 pi dens[phi_row[k]] [x_j == centroid_k].
+// np may be 0 (phi is zeroed).  Synchronises the stream.
+void reaction_points_device(int np, const FlatPanel* panels, const int32_t* phi_row, const int32_t* dphi_row,
+                            const double* dens, int nq, const double* qpos, double* phi, cudaStream_t stream);
 // 0.5 * sum q phi * 332.112 / eps_in
 double energy_device(Surface& S, const double* phi);
 

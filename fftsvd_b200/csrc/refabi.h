@@ -6,6 +6,7 @@
 // and types must match the reference headers exactly:
 //   Vector3D.h:3-7  Panel.h:3-25  FlatPanel.h:3-27  Charge.h:3-8  Tree.h:3-38
 //   Cube.h:3-54  SurfaceOperator.h:5-23  Preconditioner.h:3-17 (leading fields)
+//   FFTSVDpbeAPI.h:23-42 (PDBentry)
 #pragma once
 
 #include <cstdint>
@@ -130,6 +131,25 @@ struct Preconditioner {  // leading fields only; SuperLU factors follow
    unsigned int rows, columns, nnz;
    PreconditionerElement** P;
    unsigned int* numelements;
+};
+
+// One atom of the reference PBE API: read and written by collectPotentials.
+struct PDBentry {
+   char record[7];
+   unsigned int atomnumber;
+   char atomname[5];
+   char alternatelocation;
+   char residuename[4];
+   char chain;
+   unsigned int residuenumber;
+   char residueinsertion;
+   real x, y, z;
+   real occupancy;
+   real temperature;
+   unsigned int footnotenumber;
+   real radius;
+   real charge;
+   real potential;
 };
 
 }  // namespace ref

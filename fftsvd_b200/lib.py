@@ -30,6 +30,7 @@ EXPORTED = [
     "fftsvd_b200_host_operator_tree", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
     "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
     "fftsvd_b200_launch_count", "fftsvd_b200_reaction_potentials_noalloc", "solveSurfaceOperator", "generateRHS",
+    "collectPotentials",
     "fftsvd_b200_matvec_batch_device", "fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch",
     "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
     "fftsvd_b200_set_charges", "fftsvd_b200_matvec_transpose", "fftsvd_b200_matvec_transpose_device",

@@ -378,6 +378,19 @@ void solveSurfaceOperator(double** solution, struct _SurfaceOperator* pbesurface
                           struct _Preconditioner* preconditioner, double* rhs, unsigned int numtotalpanels);
 /* FFTSVDpbeAPI.h:150 — rhs is allocated with calloc (2*numtotalpanels doubles). */
 void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceoperator, unsigned int numtotalpanels);
+/* FFTSVDpbeAPI.h:156 — FFTSVDpbeAPI.c:1896-1922.  Writes
+   PDBcollectentries[a].potential = 561 * phi_reac[a] / innerdielectric (kT/e),
+   phi_reac[charges->globalindexstart + j] being the reaction potential of
+   charge j of every region that holds charges (SurfaceOperator.c:364-401,
+   evaluated on the GPU from the host vector solution); when the reference
+   global addcoulombic is set, adds 561 q_a / (innerdielectric d) over the input
+   entries whose chain is not 'X'.  innerdielectric and addcoulombic are the
+   reference's process globals; without an innerdielectric the dielectric
+   constant of the charged regions is used.  Regions with an M3 tree are
+   rejected.  Errors go to stderr and leave every entry unchanged. */
+void collectPotentials(struct PDBentry_s* PDBcollectentries, unsigned int numPDBcollectentries,
+                       struct PDBentry_s* PDBinputentries, unsigned int numPDBinputentries,
+                       struct _SurfaceOperator* pbesurfaceoperator, double* solution);
 
 #ifdef __cplusplus
 }

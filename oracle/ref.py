@@ -94,6 +94,37 @@ def _p(a):
     return a.ctypes.data_as(_f64p)
 
 
+class PDBentry(C.Structure):
+    """FFTSVDpbeAPI.h:23-42, the atom record collectPotentials reads and writes."""
+    _fields_ = [("record", C.c_char * 7), ("atomnumber", C.c_uint), ("atomname", C.c_char * 5),
+                ("alternatelocation", C.c_char), ("residuename", C.c_char * 4), ("chain", C.c_char),
+                ("residuenumber", C.c_uint), ("residueinsertion", C.c_char), ("x", C.c_double),
+                ("y", C.c_double), ("z", C.c_double), ("occupancy", C.c_double), ("temperature", C.c_double),
+                ("footnotenumber", C.c_uint), ("radius", C.c_double), ("charge", C.c_double),
+                ("potential", C.c_double)]
+
+
+def pdb_entries(pos, charge=None, chain=b"A", potential=0.0):
+    """A PDBentry array with the given positions, charges and chain letters."""
+    pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    arr = (PDBentry * len(pos))()
+    for i, p in enumerate(pos):
+        e = arr[i]
+        e.x, e.y, e.z = float(p[0]), float(p[1]), float(p[2])
+        e.charge = 0.0 if charge is None else float(charge[i])
+        e.chain = chain[i] if isinstance(chain, (list, tuple)) else chain
+        e.potential = potential
+    return arr
+
+
+def export_api_globals(fp64: bool = False) -> None:
+    """Put the compiled reference's symbols, among them the API's process globals
+    (innerdielectric, addcoulombic; FFTSVDpbeAPI.c:18-34), into the process-wide
+    symbol scope, as a program linked with the reference objects has them."""
+    _lib(fp64)
+    C.CDLL(library_path(fp64), mode=os.RTLD_GLOBAL | os.RTLD_NOLOAD)
+
+
 def set_threads(n: int) -> None:
     """OpenMP threads used by the reference's parallel regions (Tree.c:630-656)."""
     os.environ["OMP_NUM_THREADS"] = str(n)
@@ -186,6 +217,18 @@ class RefSystem:
     def energy(self, phi):
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         return float(self.lib.oref_energy(self.h, _p(phi)))
+
+    def collect_potentials(self, collect, inputs, sol, addcoulombic=0):
+        """The reference's own collectPotentials (FFTSVDpbeAPI.c:1896-1922) on this
+        API-built operator; writes collect[a].potential.  innerdielectric is the
+        eps_in the operator was built with (set by oref_create_api)."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        C.c_uint.in_dll(self.lib, "addcoulombic").value = int(addcoulombic)
+        try:
+            self.lib.collectPotentials(collect, C.c_uint(len(collect)), inputs, C.c_uint(len(inputs)),
+                                       C.c_void_p(self.surface_operator), _p(sol))
+        finally:
+            C.c_uint.in_dll(self.lib, "addcoulombic").value = 0
 
     def panel_integrals(self, kernel, kappa, pts, panel_of_point):
         pts = np.ascontiguousarray(pts, dtype=np.float64)
