@@ -318,7 +318,7 @@ void reaction_regions(const ref::SurfaceOperator* so, const double* sol, std::ve
                      "region panels do not match its tree");
       for (unsigned i = 0; i < so->mynumpanels; i++)
          add_panel(so->tree->panels[i], sol[so->startphi + i], sol[so->startdphi + i]);
-      // charge index -> coincident child panel phi values (exact centroid equality)
+      // child panel centroid -> sum of phi over the child panels there (matched by exact equality)
       std::map<std::array<double, 3>, double> child_centroid_phi;
       for (unsigned k = 0; k < so->numchildren; k++) {
          const ref::SurfaceOperator* ch = so->children[k];
