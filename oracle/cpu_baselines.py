@@ -6,8 +6,10 @@ eps 4/80, kappa 0.125, FFTSVD tolerance 1e-4, GMRES 1e-6) for each build and thr
   O3       oracle/_ref/libfftsvd_ref.so          -O3 -march=x86-64-v3, OpenMP (-DOMP)
   shipped  oracle/_ref/libfftsvd_ref_shipped.so  -g as in make-gcc.inc: no optimisation, no OpenMP
 
-Setup (generateSurfaceOperator's tree fill) and solve (GMRES_SurfaceOperator) are timed
-separately, each configuration in a fresh process. Build the shipped variant first with
+Setup (generateSurfaceOperator's tree fill), one matvec (SurfaceOperator_topmultiply),
+the solve (GMRES_SurfaceOperator) and the reaction-potential collection
+(SurfaceOperator_calculateReactionPotentials) are timed separately, each configuration in
+a fresh process. Build the shipped variant first with
 `make -C oracle shipped`.
 
     python oracle/cpu_baselines.py [--runs O3:1,O3:8,shipped:1] [--timeout SECONDS] > table.json
@@ -36,11 +38,18 @@ qpos, q = meshes.blob_charges(tri, 22.0, 2500, seed=2, surface_seed=1)
 t0 = time.perf_counter()
 rs = ref.RefSystem(tri, qpos, q, 4.0, 80.0, 0.125, svd_tol=1e-4)
 t1 = time.perf_counter()
+rhs = rs.rhs()
+tm0 = time.perf_counter()
+rs.matvec(rhs)
+tm1 = time.perf_counter()
 with ref.stdout_to_stderr():
-    sol, it = rs.solve(rs.rhs(), 1e-6)
+    sol, it = rs.solve(rhs, 1e-6)
 t2 = time.perf_counter()
-e = rs.energy(rs.reaction(sol))
-print(json.dumps(dict(setup_s=t1 - t0, solve_s=t2 - t1, iterations=it, dG=e)))
+phi = rs.reaction(sol)
+t3 = time.perf_counter()
+e = rs.energy(phi)
+print(json.dumps(dict(setup_s=t1 - t0, matvec_s=tm1 - tm0, solve_s=t2 - tm1, iterations=it,
+                      collect_s=t3 - t2, dG=e)))
 """
 
 
