@@ -99,6 +99,19 @@ def precond_solve(pre: dict, r: np.ndarray) -> np.ndarray:
     return np.linalg.solve(P, r)
 
 
+def precond_operator(pre: dict):
+    """precond_solve with the dense LU factored once, for repeated solves."""
+    import scipy.linalg as sl
+
+    n = pre["n"]
+    P = np.zeros((n, n))
+    for c in range(n):
+        for k in range(pre["col_ptr"][c], pre["col_ptr"][c + 1]):
+            P[pre["row_index"][k], c] += pre["value"][k]
+    lu = sl.lu_factor(P)
+    return lambda r: sl.lu_solve(lu, r)
+
+
 def gmres(apply, psolve, rhs: np.ndarray, tol: float, maxit: int = 1000):
     """Left-preconditioned full GMRES with MGS and Givens rotations (GMRES.c:3-22, 446-539)."""
     r = psolve(rhs)
