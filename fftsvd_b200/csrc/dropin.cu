@@ -9,17 +9,21 @@
 // The reference structures (layout in refabi.h) are read, never modified.  On
 // the first solve for a given (SurfaceOperator, Preconditioner) pair the
 // operator of every region tree is flattened and uploaded; later solves with
-// the same pair reuse the device copy, so the operator must not change between
-// calls.  Errors are reported on stderr and leave *solution / *rhs NULL instead
+// the same pair reuse the device copy while a sampled signature of the
+// operator (sizes, parameters, centroids, near-field blocks, preconditioner)
+// still matches; an operator changed in place in a way the sample misses must
+// not be passed again under the same addresses.  Errors are reported on stderr and leave *solution / *rhs NULL instead
 // of exiting the process.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
 #include <array>
 #include <cctype>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -181,16 +185,99 @@ void gather_regions(const ref::SurfaceOperator* so, std::vector<std::unique_ptr<
    for (unsigned c = 0; c < so->numchildren; c++) gather_regions(so->children[c], out);
 }
 
+// 64-bit signature of a caller's operator, built from its sizes, parameters
+// and a strided sample of its panel centroids, near-field blocks and
+// preconditioner values.  A cached device copy is reused only when the
+// signature still matches, so an operator allocated at the addresses of a
+// freed one (or rebuilt in place with another kappa or mesh) is uploaded anew.
+struct Signature {
+   uint64_t h = 1469598103934665603ull;
+   void add(uint64_t v) {
+      h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+      h *= 1099511628211ull;
+   }
+   void add(double d) {
+      uint64_t v;
+      std::memcpy(&v, &d, sizeof v);
+      add(v);
+   }
+   void add_floats(const float* p, size_t n) {
+      for (size_t i = 0; i < n; i++) {
+         uint32_t v;
+         std::memcpy(&v, p + i, sizeof v);
+         add((uint64_t)v);
+      }
+   }
+};
+
+constexpr size_t kSignatureSamples = 4096;
+
+void region_signature(const ref::SurfaceOperator* so, Signature& sg) {
+   sg.add(so->epsilon);
+   sg.add(so->kappa);
+   sg.add(((uint64_t)so->mynumpanels << 32) ^ so->numchildren);
+   sg.add(((uint64_t)so->startphi << 32) ^ so->startdphi);
+   const ref::Tree* t = so->tree;
+   if (t && t->numpanels > 0) {
+      sg.add(((uint64_t)t->numpanels << 32) ^ t->numpoints);
+      sg.add(((uint64_t)t->partitioningdepth << 32) ^ t->gridpoints);
+      sg.add(t->epsilon);
+      const size_t stride = std::max<size_t>(1, t->numpanels / kSignatureSamples);
+      for (size_t i = 0; i < t->numpanels; i += stride) {
+         const ref::Vec3* c = t->panels[i]->centroid;
+         sg.add(c->x);
+         sg.add(c->y);
+         sg.add(c->z);
+      }
+      std::vector<ref::Cube*> all;
+      collect_cubes(t->root, all);
+      std::vector<const ref::Cube*> leaves;
+      for (const ref::Cube* c : all)
+         if (c->leaf && c->drows > 0 && c->dcolumns > 0 && c->D_single && c->D_double) leaves.push_back(c);
+      const size_t lstride = std::max<size_t>(1, leaves.size() / 64);
+      for (size_t l = 0; l < leaves.size(); l += lstride) {
+         const ref::Cube* c = leaves[l];
+         const size_t cnt = std::min<size_t>((size_t)c->drows * c->dcolumns, 64);
+         sg.add_floats(c->D_single[0], cnt);
+         sg.add_floats(c->D_double[0], cnt);
+      }
+   }
+   for (unsigned c = 0; c < so->numchildren; c++) region_signature(so->children[c], sg);
+}
+
+uint64_t operator_signature(const ref::SurfaceOperator* so, const ref::Preconditioner* P) {
+   Signature sg;
+   region_signature(so, sg);
+   const size_t stride = std::max<size_t>(1, P->columns / kSignatureSamples);
+   for (size_t c = 0; c < P->columns; c += stride) {
+      sg.add((uint64_t)P->numelements[c]);
+      for (unsigned e = 0; e < P->numelements[c]; e++) {
+         sg.add((uint64_t)P->P[c][e].row);
+         sg.add(P->P[c][e].value);
+      }
+   }
+   return sg.h;
+}
+
+struct CachedSurface {
+   uint64_t signature = 0;
+   std::unique_ptr<fftsvd_surface> surface;
+};
+
 std::mutex g_cache_mutex;
-std::map<std::pair<const void*, const void*>, std::unique_ptr<fftsvd_surface>> g_cache;
+std::map<std::pair<const void*, const void*>, CachedSurface> g_cache;
 
 fftsvd_surface* surface_for(const ref::SurfaceOperator* so, const ref::Preconditioner* P, unsigned numtotalpanels) {
    std::lock_guard<std::mutex> lock(g_cache_mutex);
-   auto key = std::make_pair((const void*)so, (const void*)P);
-   auto it = g_cache.find(key);
-   if (it != g_cache.end()) return it->second.get();
    const int n = 2 * (int)numtotalpanels;
    FFTSVD_REQUIRE(P && P->rows == (unsigned)n && P->columns == (unsigned)n, "preconditioner size mismatch");
+   const uint64_t signature = operator_signature(so, P);
+   auto key = std::make_pair((const void*)so, (const void*)P);
+   auto it = g_cache.find(key);
+   if (it != g_cache.end()) {
+      if (it->second.signature == signature) return it->second.surface.get();
+      g_cache.erase(it);  // another operator now lives at these addresses
+   }
    std::vector<std::unique_ptr<RegionArrays>> regions;
    gather_regions(so, regions);
    FFTSVD_REQUIRE(!regions.empty(), "surface operator without panels");
@@ -214,7 +301,7 @@ fftsvd_surface* surface_for(const ref::SurfaceOperator* so, const ref::Precondit
    auto s = std::make_unique<fftsvd_surface>();
    init_surface(s->s, n, (int)regions.size(), views.data(), maps.data(), &pc);
    fftsvd_surface* out = s.get();
-   g_cache[key] = std::move(s);
+   g_cache[key] = CachedSurface{signature, std::move(s)};
    return out;
 }
 

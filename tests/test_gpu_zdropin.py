@@ -1,6 +1,7 @@
-"""The drop-in collectPotentials (FFTSVDpbeAPI.c:1896-1922) of this library
-against the reference's own collectPotentials, both called on one operator
-built by the reference's generateSurfaceOperator and on the same solution.
+"""The drop-in entry points on operators built by the reference's
+generateSurfaceOperator: collectPotentials (FFTSVDpbeAPI.c:1896-1922) against
+the reference's own collectPotentials on the same solution, and the operator
+cache of solveSurfaceOperator when a second operator is passed.
 
 Tolerance: the reaction potentials are the same FP64 panel integrals summed in
 another order (the library's reaction-potential test holds them to 1e-11), and
@@ -68,6 +69,26 @@ def test_collect_rejects_bad_calls_and_leaves_entries(api_case):
     assert b"null argument" in lib.fftsvd_b200_last_error()
 
 
+def test_dropin_solve_without_device_returns_null(api_case):
+    """Without a CUDA device the drop-in solve reads the caller's operator
+    (layout walk and cache signature), then reports the missing device and
+    leaves the solution NULL."""
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a CUDA device is present; the GPU tests cover the solve")
+    rs, c, tri, qpos, q, sol, collect_pos, chains = api_case
+    lib = F.load()
+    lib.solveSurfaceOperator.restype = None
+    lib.solveSurfaceOperator.argtypes = [C.POINTER(C.POINTER(C.c_double)), C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_double), C.c_uint]
+    rhs = np.ascontiguousarray(rs.rhs())
+    out = C.POINTER(C.c_double)()
+    lib.solveSurfaceOperator(C.byref(out), C.c_void_p(rs.surface_operator), C.c_void_p(rs.preconditioner),
+                             rhs.ctypes.data_as(C.POINTER(C.c_double)), len(tri))
+    assert not out
+    assert lib.fftsvd_b200_last_error()
+
+
 @pytest.mark.gpu
 def test_collect_matches_reference_without_coulomb(api_case, gpu):
     rs, c, tri, qpos, q, sol, collect_pos, chains = api_case
@@ -121,3 +142,33 @@ def test_collect_matches_reference_with_coulomb_and_globals(api_case, gpu):
     finally:
         coul.value = 0
         inner.value = c["eps_in"]
+
+
+@pytest.mark.gpu
+def test_dropin_solve_rebuilds_for_another_operator_at_same_addresses(gpu):
+    """Operators freed and rebuilt (here: the same mesh with another kappa, then
+    another mesh) may reuse the addresses of the previous ones; every solve must
+    still match the reference solve of the operator it was given."""
+    lib = F.load()
+    lib.solveSurfaceOperator.restype = None
+    lib.solveSurfaceOperator.argtypes = [C.POINTER(C.POINTER(C.c_double)), C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_double), C.c_uint]
+    tri3, qpos3, q3, c3 = make_case("blob3")
+    born, bpos, bq, cb = make_case("born3")
+    systems = [(tri3, qpos3, q3, c3["eps_in"], c3["eps_out"], c3["kappa"]),
+               (tri3, qpos3, q3, c3["eps_in"], c3["eps_out"], 0.3),
+               (born, bpos, bq, cb["eps_in"], cb["eps_out"], cb["kappa"])]
+    for tri, qpos, q, eps_in, eps_out, kappa in systems:
+        with ref.stdout_to_stderr():
+            rs = ref.RefSystem(tri, qpos, q, eps_in, eps_out, kappa, via_api=True, gmres_tol=1e-6)
+        rhs = np.ascontiguousarray(rs.rhs())
+        out = C.POINTER(C.c_double)()
+        lib.solveSurfaceOperator(C.byref(out), C.c_void_p(rs.surface_operator), C.c_void_p(rs.preconditioner),
+                                 rhs.ctypes.data_as(C.POINTER(C.c_double)), len(tri))
+        assert out
+        x = np.ctypeslib.as_array(out, shape=(2 * len(tri),)).copy()
+        C.CDLL(None).free(out)
+        x_ref, _ = rs.solve(rhs, 1e-6)
+        e, e_ref = rs.energy(rs.reaction(x)), rs.energy(rs.reaction(x_ref))
+        assert abs(e - e_ref) < 2e-6 * abs(e_ref), (kappa, e, e_ref)
+        rs.close()
