@@ -69,6 +69,24 @@ def test_collect_rejects_bad_calls_and_leaves_entries(api_case):
     assert b"null argument" in lib.fftsvd_b200_last_error()
 
 
+def test_collect_reads_the_reference_globals(api_case):
+    """innerdielectric is taken from the reference's process global once that is
+    in the global symbol scope: a zero value is rejected before any device work."""
+    rs, c, tri, qpos, q, sol, collect_pos, chains = api_case
+    lib = _lib()
+    ref.export_api_globals()
+    inner = C.c_double.in_dll(rs.lib, "innerdielectric")
+    assert C.c_double.in_dll(C.CDLL(None), "innerdielectric").value == inner.value == c["eps_in"]
+    entries = ref.pdb_entries(collect_pos, potential=7.0)
+    try:
+        inner.value = 0.0
+        _collect(lib, rs, entries, ref.pdb_entries(qpos, q), sol)
+    finally:
+        inner.value = c["eps_in"]
+    assert np.all(_potentials(entries) == 7.0)
+    assert b"innerdielectric must be positive" in lib.fftsvd_b200_last_error()
+
+
 def test_dropin_solve_without_device_returns_null(api_case):
     """Without a CUDA device the drop-in solve reads the caller's operator
     (layout walk and cache signature), then reports the missing device and
