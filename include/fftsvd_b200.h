@@ -366,7 +366,11 @@ int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const 
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
 
-/* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ---- */
+/* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ----
+   A reference program keeps including FFTSVDpbeAPI.h, whose declarations of
+   these three are ABI-identical; it does not include them from this header as
+   well (PDBentry is an unnamed struct there, so the two declarations of
+   collectPotentials would not be the same C type). */
 
 struct _SurfaceOperator;
 struct _Preconditioner;
