@@ -1,10 +1,13 @@
 """ORACLE — test infrastructure only (never imported by the product path).
 
 CPU restatement (numpy, FP64) of the FFTSVD PBE hot path over the flat
-operator layout declared in include/fftsvd_b200.h.  Each function cites the
-reference code it restates.  It is checked against the reference itself
-(oracle/_ref/, tests/test_oracle.py) and then used as the checker for the
-device kernels where the compiled reference is not available.
+operator layout declared in include/fftsvd_b200.h: the matvec, preconditioner,
+GMRES and right-hand side, and from the panel geometry the Laplace panel
+integrals, the reaction potentials and the energy.  Each function cites the
+reference code it restates.  It is checked against the compiled reference
+(oracle/_ref/) and its golden fixtures (tests/golden/, tests/test_golden.py,
+tests/test_setup.py) and serves as the checker where the compiled reference is
+not available.
 """
 from __future__ import annotations
 
@@ -167,3 +170,173 @@ def rhs(centroids: np.ndarray, qpos: np.ndarray, q: np.ndarray, n_unknowns: int)
     d = np.linalg.norm(qpos[None, :, :] - centroids[:, None, :], axis=2)
     out[:len(centroids)] = (q[None, :] / d).sum(axis=1)
     return out
+
+
+# ---- Laplace panel integrals and reaction potentials ---------------------------------------------
+# The truncated constants of FlatIntegration.c:3-9 and the moment coefficients of FlatPanel.c:218-219,
+# kept as the reference has them: the far-field moment expansion depends on these exact values.
+_ONE3, _FIVE3, _ONE6, _SEVEN3 = 0.3333333333333, 1.666666666667, 0.16666666666667, 2.3333333333333
+_LIMITFOURTH, _LIMITSECOND = 9.0, 36.0
+_CS = (0.0, 1.0, 1.0, 1.5, 1.5, 3.75, 1.0, 3.0, 1.5, 7.5, 1.5, 1.5, 3.75, 1.5, 7.5, 3.75)
+
+
+def _unit(v):
+    return v / np.sqrt(v @ v)
+
+
+def flat_panel(v1, v2, v3) -> dict:
+    """The fields of a flat triangle the Laplace integral reads (FlatPanel.c:5-150): centroid, panel
+    frame (axis 0 along v3-v1, axis 2 the normal (v3-v1)x(v2-v1)), vertices in that frame relative to
+    the centroid, edge lengths and direction cosines, largest edge, area and moments."""
+    v = [np.asarray(x, dtype=np.float64) for x in (v1, v2, v3)]
+    centroid = ((v[0] + v[1]) + v[2]) * (1.0 / 3.0)
+    edge = [np.sqrt((v[1] - v[0]) @ (v[1] - v[0])), np.sqrt((v[2] - v[1]) @ (v[2] - v[1])),
+            np.sqrt((v[0] - v[2]) @ (v[0] - v[2]))]
+    a0 = v[2] - v[0]
+    a2 = np.cross(a0, v[1] - v[0])
+    area = 0.5 * np.sqrt(a2 @ a2)
+    a2 = _unit(a2)
+    a0 = _unit(a0)
+    a1 = np.cross(a2, a0)
+    axis = np.array([a0, a1, a2])
+    pv = np.array([axis @ (x - centroid) for x in v])
+    cC = [(pv[(i + 1) % 3, 0] - pv[i, 0]) / edge[i] for i in range(3)]
+    cS = [(pv[(i + 1) % 3, 1] - pv[i, 1]) / edge[i] for i in range(3)]
+    return dict(centroid=centroid, axis=axis, pv=pv, edge=edge, cC=cC, cS=cS, max_diag=max(edge), area=area,
+                moments=panel_moments(pv, area))
+
+
+def panel_moments(pv, area) -> list:
+    """FastCap's Euclidean moments up to order 4 by edge recurrences, scaled into the S vector
+    (FlatPanel.c:214-318); S[1..15], S[0] unused."""
+    order = 4
+    IM = np.zeros((order + 1, order + 1))
+    XP = [[pv[i, 0] ** j if j else 0.0 for j in range(order + 3)] for i in range(3)]
+    YP = [[pv[i, 1] ** j if j else 0.0 for j in range(order + 3)] for i in range(3)]
+    for i in range(3):  # repeated products, as the reference forms the powers
+        for j in range(2, order + 3):
+            XP[i][j] = XP[i][j - 1] * XP[i][1]
+            YP[i][j] = YP[i][j - 1] * YP[i][1]
+    IM[0, 0] = area
+    for side in range(3):
+        xp, yp = XP[side], YP[side]
+        xpn, ypn = XP[(side + 1) % 3], YP[(side + 1) % 3]
+        dx, dy = xpn[1] - xp[1], ypn[1] - yp[1]
+        if abs(dx) >= abs(dy):
+            dydx = dy / dx
+            for M in range(2, order + 1):
+                M1, M2 = M + 1, M + 2
+                SI = (xpn[M1] * ypn[1] - xp[M1] * yp[1]) / M1 + dydx * (xp[M2] - xpn[M2]) / (M1 * M2)
+                IM[M, 0] += SI
+                for N in range(1, M + 1):
+                    N1, MN1 = N + 1, M - N + 1
+                    SI = (xpn[MN1] * ypn[N1] - xp[MN1] * yp[N1]) / (MN1 * N1) - (dydx * N * SI) / MN1
+                    IM[M - N, N] += SI
+        else:
+            dxdy = dx / dy
+            for M in range(2, order + 1):
+                M1, M2 = M + 1, M + 2
+                SI = (dxdy / (M1 * M2)) * (ypn[M2] - yp[M2])
+                IM[0, M] += SI
+                for N in range(1, M + 1):
+                    MN1 = M - N + 1
+                    MN2 = MN1 + 1
+                    SI = dxdy * ((xpn[N] * ypn[MN2] - xp[N] * yp[MN2]) / (MN1 * MN2) - (N * SI / MN1))
+                    IM[N, M - N] += SI
+    S = [0.0] * 16
+    i = 0
+    for M in range(5):
+        for N in range(5 - M):
+            i += 1
+            S[i] = IM[M, N] * _CS[i]
+    return S
+
+
+def laplace_panel(point, P) -> tuple:
+    """Single- and double-layer integrals of 1/r over a flat panel at a point (FlatIntegration.c:295-429):
+    the moment expansion when r^2 > 9 diag^2 (third and fourth moments below 36 diag^2), else the analytic
+    edge formula; the double layer of the panel's own centroid is 2 pi."""
+    point = np.asarray(point, dtype=np.float64)
+    pmc = point - P["centroid"]
+    xn, yn, zn = (float(P["axis"][k] @ pmc) for k in range(3))
+    xsq, ysq, zsq = xn * xn, yn * yn, zn * zn
+    rsq = xsq + ysq + zsq
+    diagsq = P["max_diag"] * P["max_diag"]
+    s = P["moments"]
+    if rsq > _LIMITFOURTH * diagsq:
+        r2Inv = 1.0 / rsq
+        rInv = np.sqrt(r2Inv)
+        r3Inv = r2Inv * rInv
+        r5Inv = r3Inv * r2Inv
+        zr2Inv = zn * r2Inv
+        ss1 = s[1] * rInv
+        ss3 = -(s[3] + s[10]) * r3Inv
+        ss5 = (xsq * s[10] + (xn * yn * s[7]) + ysq * s[3]) * r5Inv
+        fs = ss1 + _ONE3 * ss3 + ss5
+        fd = zr2Inv * (ss1 + ss3 + 5.0 * ss5)
+        if rsq < _LIMITSECOND * diagsq:
+            s914, s813, s411 = s[9] + s[14], s[8] + s[13], s[4] + s[11]
+            s512, s1215 = s[5] + s[12], s[12] + s[15]
+            r7Inv = r5Inv * r2Inv
+            r9Inv = r7Inv * r2Inv
+            t5 = (-xn * s813 - yn * s411 + 0.1 * (s512 + s1215)) * r5Inv
+            t7 = (_FIVE3 * ((xn * xsq * s[13] + yn * ysq * s[4]) + 3.0 * xn * yn * (xn * s[11] + yn * s[8]))
+                  - xsq * s1215 - ysq * s512 - xn * yn * s914) * r7Inv
+            t9 = (7.0 * (_ONE6 * (xsq * xsq * s[15] + ysq * ysq * s[5]) + xsq * ysq * s[12])
+                  + _SEVEN3 * xn * yn * (xsq * s[14] + ysq * s[9])) * r9Inv
+            fs += t5 + t7 + t9
+            fd += zr2Inv * (5.0 * t5 + 7.0 * t7 + 9.0 * t9)
+        return fs, fd
+    znabs = abs(zn)
+    pv = P["pv"]
+    xm = [xn - pv[i, 0] for i in range(3)]
+    ym = [yn - pv[i, 1] for i in range(3)]
+    fe = [xm[i] * xm[i] + (zn - pv[i, 2]) ** 2 for i in range(3)]
+    r = [np.sqrt(ym[i] * ym[i] + fe[i]) for i in range(3)]
+    ok = all(r[i] >= 1.005 * znabs for i in range(3))
+    fs = fd = 0.0
+    for i in range(3):
+        nx = (i + 1) % 3
+        cC, cS = P["cC"][i], P["cS"][i]
+        v = xm[i] * cS - ym[i] * cC
+        arg = (r[i] + r[nx] - P["edge"][i]) / (r[i] + r[nx] + P["edge"][i])
+        if arg > 0.0:
+            fs -= v * np.log(arg)
+        if ok:
+            s1, c1 = v * r[i], znabs * (xm[i] * cC + ym[i] * cS)
+            s2, c2 = v * r[nx], znabs * (xm[nx] * cC + ym[nx] * cS)
+        else:
+            s1, c1 = fe[i] * cS - xm[i] * ym[i] * cC, znabs * r[i] * cC
+            s2, c2 = fe[nx] * cS - xm[nx] * ym[nx] * cC, znabs * r[nx] * cC
+        fd += np.arctan2(s1 * c2 - s2 * c1, c1 * c2 + s1 * s2)
+    if fd < 0.0:
+        fd += 2.0 * np.pi
+    if zn < 0.0:
+        fd = -fd
+    fs -= zn * fd
+    if np.array_equal(P["centroid"], point):
+        fd = 2.0 * np.pi
+    return fs, fd
+
+
+def reaction(tri, phi, dphi, qpos) -> np.ndarray:
+    """Reaction potentials at the charges of the region that owns the panels, direct branch
+    (SurfaceOperator.c:364-396): phi_j = sum_i dphi_i SLP(x_j, i) - phi_i DLP(x_j, i), minus 4 pi phi_i
+    where x_j is panel i's centroid.  tri: n x 9 vertices; phi, dphi: the region's slices of the solution."""
+    tri = np.asarray(tri, dtype=np.float64).reshape(-1, 3, 3)
+    panels = [flat_panel(*t) for t in tri]
+    out = np.zeros(len(qpos))
+    for j, x in enumerate(np.asarray(qpos, dtype=np.float64)):
+        acc = 0.0
+        for i, P in enumerate(panels):
+            slp, dlp = laplace_panel(x, P)
+            acc += dphi[i] * slp - phi[i] * dlp
+            if np.array_equal(x, P["centroid"]):
+                acc -= 4.0 * np.pi * phi[i]
+        out[j] = acc
+    return out
+
+
+def energy(q, phi, eps_in) -> float:
+    """0.5 sum q phi * 332.112 / eps_in in kcal/mol (FFTSVDsalt.c:167-170)."""
+    return 0.5 * float(np.dot(q, phi)) * 332.112 / eps_in
