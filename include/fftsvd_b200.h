@@ -367,10 +367,10 @@ int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const 
 long long fftsvd_b200_launch_count(void);
 
 /* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ----
-   A reference program keeps including FFTSVDpbeAPI.h, whose declarations of
-   these three are ABI-identical; it does not include them from this header as
-   well (PDBentry is an unnamed struct there, so the two declarations of
-   collectPotentials would not be the same C type). */
+   The declarations in FFTSVDpbeAPI.h are ABI-identical.  PDBentry is an
+   unnamed struct there, so the two declarations of collectPotentials are not
+   the same C type: a file that includes FFTSVDpbeAPI.h before this header
+   gets the reference's declaration only (guarded by its include guard). */
 
 struct _SurfaceOperator;
 struct _Preconditioner;
@@ -392,9 +392,11 @@ void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceoperator, unsi
    reference's process globals; without an innerdielectric the dielectric
    constant of the charged regions is used.  Regions with an M3 tree are
    rejected.  Errors go to stderr and leave every entry unchanged. */
+#ifndef FFTSVDpbeAPI_H
 void collectPotentials(struct PDBentry_s* PDBcollectentries, unsigned int numPDBcollectentries,
                        struct PDBentry_s* PDBinputentries, unsigned int numPDBinputentries,
                        struct _SurfaceOperator* pbesurfaceoperator, double* solution);
+#endif
 
 #ifdef __cplusplus
 }

@@ -74,3 +74,14 @@ def test_refabi_mirrors_match_reference_layout(tmp_path):
     assert len(ref_lines) == len(mirror_lines) > 100
     diff = [(a, b) for a, b in zip(ref_lines, mirror_lines) if a != b]
     assert not diff, diff
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference sources not present")
+def test_public_header_compiles_after_the_reference_api_header(tmp_path):
+    """A C file of the reference side (the oracle driver is one) may include the
+    reference's FFTSVDpbeAPI.h and then this library's header."""
+    src = tmp_path / "both.c"
+    src.write_text('#include "FFTSVDpbeAPI.h"\n#include "fftsvd_b200.h"\nint main(void) { return 0; }\n')
+    subprocess.run(["gcc", "-std=gnu99", "-fsyntax-only", "-Werror", "-include", "assert.h", "-D_MALLOC",
+                    "-DPWD=\"/nonexistent\"", "-I" + os.path.join(ROOT, "oracle", "shim"), "-I" + REFERENCE,
+                    "-I" + os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)
