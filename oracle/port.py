@@ -2,8 +2,8 @@
 
 CPU restatement (numpy, FP64) of the FFTSVD PBE hot path over the flat
 operator layout declared in include/fftsvd_b200.h: the matvec, preconditioner,
-GMRES and right-hand side, and from the panel geometry the Laplace panel
-integrals, the reaction potentials and the energy.  Each function cites the
+GMRES and right-hand side, and from the panel geometry the Laplace and Yukawa
+panel integrals, the reaction potentials and the energy.  Each function cites the
 reference code it restates.  It is checked against the compiled reference
 (oracle/_ref/) and its golden fixtures (tests/golden/, tests/test_golden.py,
 tests/test_setup.py) and serves as the checker where the compiled reference is
@@ -202,8 +202,28 @@ def flat_panel(v1, v2, v3) -> dict:
     pv = np.array([axis @ (x - centroid) for x in v])
     cC = [(pv[(i + 1) % 3, 0] - pv[i, 0]) / edge[i] for i in range(3)]
     cS = [(pv[(i + 1) % 3, 1] - pv[i, 1]) / edge[i] for i in range(3)]
+    # the second, edge-aligned frame the Yukawa edge integrals use, and the edge lines in it (FlatPanel.c:53-128)
+    e = [(v[1] - v[0]) * (1.0 / np.sqrt((v[1] - v[0]) @ (v[1] - v[0]))),
+         (v[2] - v[1]) * (1.0 / np.sqrt((v[2] - v[1]) @ (v[2] - v[1]))),
+         (v[0] - v[2]) * (1.0 / np.sqrt((v[0] - v[2]) @ (v[0] - v[2])))]
+    n0, n1 = e[0].copy(), e[1].copy()
+    if abs(e[2] @ n0) < abs(n1 @ n0):
+        n1 = -e[2]
+    alpha = n1 @ n0
+    n1 = n1 + e[0] * (-alpha)
+    n1 = n1 * (1.0 / np.sqrt(n1 @ n1))
+    axisnum = np.array([n0, n1, np.cross(n0, n1)])
+    pvnum = np.array([axisnum @ (x - centroid) for x in v])
+    lines, rhs, ov = [], [], []
+    for i in range(3):
+        d = pvnum[(i + 1) % 3] - pvnum[i]
+        line = np.array([-d[1], d[0], d[2]])
+        lines.append(line)
+        rhs.append(pvnum[i] @ line)
+        ov.append(pvnum[(i + 2) % 3] @ line - rhs[-1])
     return dict(centroid=centroid, axis=axis, pv=pv, edge=edge, cC=cC, cS=cS, max_diag=max(edge), area=area,
-                moments=panel_moments(pv, area))
+                moments=panel_moments(pv, area), axisnum=axisnum, pvnum=pvnum, edgeline=lines, edgeRHS=rhs,
+                edgeOV=ov)
 
 
 def panel_moments(pv, area) -> list:
@@ -316,6 +336,117 @@ def laplace_panel(point, P) -> tuple:
     fs -= zn * fd
     if np.array_equal(P["centroid"], point):
         fd = 2.0 * np.pi
+    return fs, fd
+
+
+_DBL_EPS, _FLT_EPS = 2.220446049250313e-16, 1.1920928955078125e-07
+
+
+def _gauss4():
+    """The 4-point Gauss-Legendre rule on [0, 1] (QuadratureRule_allocate(4), QuadratureRule.c:3-125)."""
+    t, w = np.polynomial.legendre.leggauss(4)
+    return (t + 1.0) / 2.0, w / 2.0
+
+
+def _yukawa_line(z, x, y1, y2, kappa):
+    """Angular integral over one edge strip, single and double layer (FlatIntegration.c:473-635, Helmholtz):
+    the angle range is split geometrically (factors of 10) and each piece takes the 4-point rule."""
+    X, W = _gauss4()
+    absZ = abs(z)
+    x = abs(x)
+    startY = y1
+    if x < y1:
+        endY = 10.0 * y1 if y2 > 10.0 * y1 else y2
+    else:
+        endY = y2 if x > y2 else x
+    signZ = 1.0 if z > 0.0 else (-1.0 if z < 0.0 else 0.0)
+    ls = ld = 0.0
+    pieces = 0
+    while startY < y2:
+        pieces += 1
+        if pieces > 1000:
+            raise RuntimeError("line integral subdivision did not end")
+        phi1, phi2 = np.arctan2(startY, x), np.arctan2(endY, x)
+        dPhi = phi2 - phi1
+        for i in range(4):
+            theta = phi1 + (phi2 - phi1) * X[i]
+            RT = np.sqrt((x * (1.0 / np.cos(theta))) ** 2 + z * z)
+            ls -= W[i] * dPhi * (np.exp(-kappa * RT) - np.exp(-kappa * absZ)) / kappa
+            ld -= W[i] * dPhi * (signZ * np.exp(-kappa * absZ) - (z / RT) * np.exp(-kappa * RT))
+        startY = endY
+        if endY == y2:
+            endY = 10.0 * y2
+        elif endY * 10.0 > y2:
+            endY = y2
+        else:
+            endY = 10.0 * endY
+    return ls, ld
+
+
+def _rot(m, v):
+    return np.array([m[0] * v[0] + m[1] * v[1] + m[2] * v[2], m[3] * v[0] + m[4] * v[1] + m[5] * v[2],
+                     m[6] * v[0] + m[7] * v[1] + m[8] * v[2]])
+
+
+def _yukawa_edge(v1, v2, p, kappa):
+    """One edge (FlatIntegration.c:431-471, 637-799): rotate the plane through the edge and the point
+    level, translate the point onto the z axis, turn the edge parallel to y, integrate both sides."""
+    v1, v2, p = (np.array(a, dtype=np.float64) for a in (v1, v2, p))
+    n = np.cross(v1, v2)
+    if np.sqrt(n[0] ** 2 + n[1] ** 2) > 10 * _DBL_EPS:
+        th = -np.arctan2(n[1], n[0])
+        c, s = np.cos(th), np.sin(th)
+        Z = (c, -s, 0.0, s, c, 0.0, 0.0, 0.0, 1.0)
+        v1, v2, p = _rot(Z, v1), _rot(Z, v2), _rot(Z, p)
+        Np = np.cross(v1, v2)
+        th = np.pi / 2 - np.arctan2(Np[2], Np[0])
+        c, s = np.cos(th), np.sin(th)
+        Y = (c, 0.0, -s, 0.0, 1.0, 0.0, s, 0.0, c)
+        v1, v2, p = _rot(Y, v1), _rot(Y, v2), _rot(Y, p)
+    t = np.array([-p[0], -p[1], -v1[2]])
+    v1, v2, p = v1 + t, v2 + t, p + t
+    if abs(v1[2] - v2[2]) > 1e-6:
+        raise RuntimeError("edge did not rotate onto the plane")
+    dv = np.array([v1[0] - v2[0], v1[1] - v2[1], 0.0])
+    dv = dv * (1.0 / np.sqrt(dv @ dv))
+    c, s = dv[0], dv[1]
+    v1x, v1y = s * v1[0] - c * v1[1], c * v1[0] + s * v1[1]
+    v2y = c * v2[0] + s * v2[1]
+    if abs(v1x) < 10 * _DBL_EPS:
+        return 0.0, 0.0
+    z, x1, y1, y2 = p[2], v1x, v2y, v1y
+    if y2 < 0 and y1 < 0:
+        y1, y2 = -y1, -y2
+    if y2 < y1:
+        y1, y2 = y2, y1
+    s0, d0 = _yukawa_line(z, x1, y1 if y1 >= 0 else 0.0, y2, kappa)
+    if y1 < 0.0:
+        s1, d1 = _yukawa_line(z, x1, 0.0, -y1, kappa)
+        s0, d0 = s0 + s1, d0 + d1
+    return s0, d0
+
+
+def yukawa_panel(point, P, kappa) -> tuple:
+    """Single- and double-layer integrals of exp(-kappa r)/r over a flat panel (FlatIntegration.c:882-949,
+    1035-1049): signed edge integrals in the panel's edge-aligned frame; the double layer in the panel's
+    plane is 2 pi inside and 0 outside; kappa < 1e-6 takes the Laplace formula."""
+    if kappa < 1e-6:
+        return laplace_panel(point, P)
+    pnt = P["axisnum"] @ (np.asarray(point, dtype=np.float64) - P["centroid"])
+    fs = fd = 0.0
+    left = 0
+    for j in range(3):
+        d = pnt @ P["edgeline"][j] - P["edgeRHS"][j]
+        if (d > 0.0 and P["edgeOV"][j] > 0.0) or (d < 0.0 and P["edgeOV"][j] < 0.0):
+            left += 1
+            sign = 1.0
+        else:
+            sign = -1.0
+        s, dd = _yukawa_edge(P["pvnum"][j], P["pvnum"][(j + 1) % 3], pnt, kappa)
+        fs += sign * s
+        fd += sign * dd
+    if abs(pnt[2]) < 10 * _FLT_EPS:
+        fd = 2.0 * np.pi if left == 3 else 0.0
     return fs, fd
 
 

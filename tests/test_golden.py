@@ -117,3 +117,31 @@ def test_restated_panel_integrals_match_compiled_reference():
         s, d = port.laplace_panel(p, port.flat_panel(*tri[i]))
         assert abs(s - s_ref[k]) <= 1e-12 * max(1.0, abs(s_ref[k])), (k, s, s_ref[k])
         assert abs(d - d_ref[k]) <= 1e-12 * max(1.0, abs(d_ref[k])), (k, d, d_ref[k])
+
+
+@pytest.mark.skipif(not ref.available(fp64=True), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kappa", [0.125, 1.0])
+def test_restated_yukawa_integrals_match_compiled_reference(kappa):
+    """The Yukawa panel integrals (edge line integrals, FlatIntegration.c:431-949, 1035-1049) point by
+    point against the reference's Integration: points on the panel's plane (inside and outside), just
+    off it, above a vertex, and at several distances along the normal."""
+    g = load("blob3")
+    with ref.stdout_to_stderr():
+        rs = ref.RefSystem(g["tri"], g["qpos"], g["q"], float(g["eps_in"]), float(g["eps_out"]),
+                           float(g["kappa"]), svd_tol=float(g["svd_tol"]), fp64=True)
+    tri = g["tri"].reshape(-1, 3, 3)
+    pts, owner = [], []
+    for i in np.random.default_rng(4).choice(len(tri), 8, replace=False):
+        P = port.flat_panel(*tri[i])
+        c, nrm, d = P["centroid"], P["axis"][2], P["max_diag"]
+        for h in (0.0, 1e-9, 1e-3, 0.05, 0.4, 1.5, 3.0, 7.0, 20.0):
+            for p in (c + h * d * nrm, c - h * d * nrm, tri[i][1] + max(h, 1e-3) * d * nrm,
+                      c + (h + 0.5) * d * P["axis"][0]):
+                pts.append(p)
+                owner.append(i)
+    pts = np.array(pts)
+    s_ref, d_ref = rs.panel_integrals(1, kappa, pts, np.array(owner))
+    for k, (p, i) in enumerate(zip(pts, owner)):
+        s, d = port.yukawa_panel(p, port.flat_panel(*tri[i]), kappa)
+        assert abs(s - s_ref[k]) <= 1e-12 * max(1.0, abs(s_ref[k])), (k, s, s_ref[k])
+        assert abs(d - d_ref[k]) <= 1e-12 * max(1.0, abs(d_ref[k])), (k, d, d_ref[k])
