@@ -63,3 +63,14 @@ def test_create_without_device_reports_status():
     rc = lib.fftsvd_b200_surface_create_flat(n, 0, None, None, C.byref(P), 0, None, None, 1.0, C.byref(h))
     assert rc in (_abi.FFTSVD_ERR_NO_DEVICE, _abi.FFTSVD_ERR_ARGUMENT)
     assert not h.value
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """No fallback: without the built library the package refuses to run."""
+    code = ("import fftsvd_b200.lib as L\n"
+            f"L.LIB_PATH = {str(tmp_path / 'absent.so')!r}\n"
+            "L._lib = None\n"
+            "try:\n    L.load()\nexcept ImportError as e:\n    print('raised', e)\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([os.sys.executable, "-c", code], cwd=root, capture_output=True, text=True, check=True)
+    assert out.stdout.startswith("raised") and "is missing" in out.stdout
