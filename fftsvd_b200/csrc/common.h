@@ -53,6 +53,8 @@ inline int guarded(F&& f) {
 // Every kernel launch of the library is followed by this check, which also
 // counts the launch (fftsvd_b200_launch_count).
 extern std::atomic<long long> g_kernel_launches;
+// Device allocations (cudaMalloc) made by the library (fftsvd_b200_device_alloc_count).
+extern std::atomic<long long> g_device_allocs;
 #define FFTSVD_CHECK_LAUNCH()                                        \
    do {                                                              \
       ::fftsvd::g_kernel_launches.fetch_add(1, std::memory_order_relaxed); \
@@ -81,7 +83,10 @@ class DevBuf {
    void alloc(size_t n) {
       release();
       n_ = n;
-      if (n) FFTSVD_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+      if (n) {
+         g_device_allocs.fetch_add(1, std::memory_order_relaxed);
+         FFTSVD_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+      }
    }
    void upload(const T* host, size_t n) {
       alloc(n);

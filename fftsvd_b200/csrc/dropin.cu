@@ -305,22 +305,26 @@ fftsvd_surface* surface_for(const ref::SurfaceOperator* so, const ref::Precondit
    return out;
 }
 
-__global__ void rhs_targets_kernel(int nt, const double* __restrict__ cent, const int32_t* __restrict__ rows, int nq,
-                                   const double* __restrict__ qpos, const double* __restrict__ q,
-                                   double* __restrict__ rhs) {
-   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-   if (i >= nt) return;
-   const double cx = cent[3 * i], cy = cent[3 * i + 1], cz = cent[3 * i + 2];
-   double acc = 0.0;
-   for (int j = 0; j < nq; j++) {
-      const double qj = q[j];
-      if (qj == 0.0) continue;
-      const double dx = qpos[3 * j] - cx, dy = qpos[3 * j + 1] - cy, dz = qpos[3 * j + 2] - cz;
-      acc += qj / sqrt(dx * dx + dy * dy + dz * dz);
-   }
-   rhs[rows[i]] += acc;
+// The stream the drop-in right-hand side and collection run on: one non-blocking
+// stream per device, created on first use and owned by the library, so these
+// calls neither use nor wait on the legacy default stream.
+cudaStream_t dropin_stream() {
+   static std::mutex mu;
+   static std::map<int, cudaStream_t> streams;
+   int dev = 0;
+   FFTSVD_CUDA(cudaGetDevice(&dev));
+   std::lock_guard<std::mutex> lock(mu);
+   auto it = streams.find(dev);
+   if (it != streams.end()) return it->second;
+   cudaStream_t st = nullptr;
+   FFTSVD_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+   streams[dev] = st;
+   return st;
 }
 
+// SurfaceOperator_makeRHS (SurfaceOperator.c:291-321) over the caller's region tree:
+// one launch of the library's tiled right-hand-side kernel per region with charges,
+// its own panels' phi rows and its children's dphi rows as targets.
 void rhs_region(const ref::SurfaceOperator* so, double* drhs) {
    if (so->charges && so->charges->numcharges > 0) {
       std::vector<double> cent;
@@ -349,9 +353,10 @@ void rhs_region(const ref::SurfaceOperator* so, double* drhs) {
          dq.upload(qv);
          dqp.upload(qpos);
          const int nt = (int)rows.size();
-         rhs_targets_kernel<<<(nt + 255) / 256, 256>>>(nt, dc.get(), dr.get(), (int)qv.size(), dqp.get(), dq.get(), drhs);
-         FFTSVD_CHECK_LAUNCH();
-         FFTSVD_CUDA(cudaDeviceSynchronize());
+         const cudaStream_t stream = dropin_stream();
+         rhs_points_device(nt, dc.get(), dr.get(), (int)qv.size(), dqp.get(), dq.get(), drhs, stream);
+         // the staging buffers are freed on return
+         FFTSVD_CUDA(cudaStreamSynchronize(stream));
       }
    }
    for (unsigned k = 0; k < so->numchildren; k++) rhs_region(so->children[k], drhs);
@@ -436,9 +441,11 @@ void reaction_regions(const ref::SurfaceOperator* so, const double* sol, std::ve
          d_dphi_row.upload(dphi_row);
          d_dens.upload(dens);
          d_qpos.upload(qpos);
+         const cudaStream_t stream = dropin_stream();
          reaction_points_device((int)panels.size(), d_panels.get(), d_phi_row.get(), d_dphi_row.get(), d_dens.get(),
-                                (int)nq, d_qpos.get(), d_out.get(), 0);
-         FFTSVD_CUDA(cudaMemcpy(phi.data(), d_out.get(), sizeof(double) * nq, cudaMemcpyDeviceToHost));
+                                (int)nq, d_qpos.get(), d_out.get(), stream);
+         FFTSVD_CUDA(cudaMemcpyAsync(phi.data(), d_out.get(), sizeof(double) * nq, cudaMemcpyDeviceToHost, stream));
+         FFTSVD_CUDA(cudaStreamSynchronize(stream));
       }
       for (size_t j = 0; j < nq; j++) {
          if (!child_centroid_phi.empty()) {
@@ -513,12 +520,18 @@ extern "C" void generateRHS(double** rhs, struct _SurfaceOperator* pbesurfaceope
    try {
       FFTSVD_REQUIRE(pbesurfaceoperator && numtotalpanels > 0, "null argument");
       const int n = 2 * (int)numtotalpanels;
+      const cudaStream_t stream = dropin_stream();
       DevBuf<double> d(n);
-      d.zero();
+      d.zero(stream);
       rhs_region(reinterpret_cast<const ref::SurfaceOperator*>(pbesurfaceoperator), d.get());
       double* out = static_cast<double*>(std::calloc((size_t)n, sizeof(double)));
       FFTSVD_REQUIRE(out, "host allocation failed");
-      FFTSVD_CUDA(cudaMemcpy(out, d.get(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+      const cudaError_t e1 = cudaMemcpyAsync(out, d.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream);
+      const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamSynchronize(stream) : e1;
+      if (e2 != cudaSuccess) {
+         std::free(out);
+         throw Error(FFTSVD_ERR_CUDA, std::string("generateRHS copy: ") + cudaGetErrorString(e2));
+      }
       *rhs = out;
    } catch (const std::exception& e) {
       set_last_error(e.what());
@@ -572,11 +585,13 @@ extern "C" void collectPotentials(struct PDBentry_s* PDBcollectentries, unsigned
             dipos.upload(ipos);
             diq.upload(iq);
             dpot.upload(pot);
+            const cudaStream_t stream = dropin_stream();
             const int ncol = (int)nc;
-            coulomb_kernel<<<(ncol + 127) / 128, 128>>>(ncol, dcpos.get(), (int)iq.size(), dipos.get(), diq.get(),
-                                                         kKTConversion, eps_in, dpot.get());
+            coulomb_kernel<<<(ncol + 127) / 128, 128, 0, stream>>>(ncol, dcpos.get(), (int)iq.size(), dipos.get(),
+                                                                    diq.get(), kKTConversion, eps_in, dpot.get());
             FFTSVD_CHECK_LAUNCH();
-            FFTSVD_CUDA(cudaMemcpy(pot.data(), dpot.get(), sizeof(double) * nc, cudaMemcpyDeviceToHost));
+            FFTSVD_CUDA(cudaMemcpyAsync(pot.data(), dpot.get(), sizeof(double) * nc, cudaMemcpyDeviceToHost, stream));
+            FFTSVD_CUDA(cudaStreamSynchronize(stream));
          }
       }
       for (size_t a = 0; a < nc; a++) collect[a].potential = pot[a];

@@ -51,13 +51,33 @@ void set_charges(Surface& S, int num_charges, const double* pos, const double* q
 constexpr int kRhsThreads = 256;
 constexpr int kRhsTile = 256;
 
-// One thread per panel; charges streamed through shared memory in order, so each
-// panel accumulates over charges in the reference's order (charge-major loop).
+// Target centroids of the right-hand-side kernel: the library's flat panels, or
+// plain xyz triples (the drop-in reads them from the caller's reference panels).
+struct PanelTargets {
+   const FlatPanel* __restrict__ p;
+   __device__ void get(int i, double c[3]) const {
+      c[0] = p[i].centroid[0];
+      c[1] = p[i].centroid[1];
+      c[2] = p[i].centroid[2];
+   }
+};
+struct PointTargets {
+   const double* __restrict__ xyz;
+   __device__ void get(int i, double c[3]) const {
+      c[0] = xyz[3 * i];
+      c[1] = xyz[3 * i + 1];
+      c[2] = xyz[3 * i + 2];
+   }
+};
+
+// One thread per target; charges streamed through shared memory in order, so each
+// target accumulates over charges in the reference's order (charge-major loop,
+// SurfaceOperator.c:298-312), and rhs[row[i]] += the sum.
 // With gptr, blockIdx.y is a charge group: charges [gptr[g], gptr[g+1]) and
 // output column rhs + g * col.
-__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, const FlatPanel* __restrict__ panels,
-                                                          const int32_t* __restrict__ phi_row, int nq,
-                                                          const double* __restrict__ qpos,
+template <typename Targets>
+__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, Targets targets, const int32_t* __restrict__ row,
+                                                          int nq, const double* __restrict__ qpos,
                                                           const double* __restrict__ q, double* __restrict__ rhs,
                                                           const int32_t* __restrict__ gptr, int64_t col) {
    __shared__ double4 tile[kRhsTile];
@@ -70,7 +90,7 @@ __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, const FlatPane
    }
    const int i = blockIdx.x * blockDim.x + threadIdx.x;
    double c[3] = {0, 0, 0};
-   if (i < np) { c[0] = panels[i].centroid[0]; c[1] = panels[i].centroid[1]; c[2] = panels[i].centroid[2]; }
+   if (i < np) targets.get(i, c);
    double acc = 0.0;
    for (int base = 0; base < nq; base += kRhsTile) {
       const int cnt = min(kRhsTile, nq - base);
@@ -86,7 +106,16 @@ __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(int np, const FlatPane
             acc += t.w / sqrt(dx * dx + dy * dy + dz * dz);
          }
    }
-   if (i < np) rhs[phi_row[i]] = acc;
+   if (i < np) rhs[row[i]] += acc;
+}
+
+void rhs_points_device(int nt, const double* centroids, const int32_t* rows, int nq, const double* qpos,
+                       const double* q, double* rhs, cudaStream_t stream) {
+   FFTSVD_REQUIRE(nt >= 0 && nq >= 0, "negative target or charge count");
+   if (nt == 0) return;
+   rhs_kernel<<<(nt + kRhsThreads - 1) / kRhsThreads, kRhsThreads, 0, stream>>>(
+       nt, PointTargets{centroids}, rows, nq, qpos, q, rhs, nullptr, 0);
+   FFTSVD_CHECK_LAUNCH();
 }
 
 constexpr int kReactThreads = 128;
@@ -154,8 +183,8 @@ void rhs_device(Surface& S, double* rhs) {
    FFTSVD_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * S.n, S.stream));
    const int np = S.geom->num_panels;
    rhs_kernel<<<(np + kRhsThreads - 1) / kRhsThreads, kRhsThreads, 0, S.stream>>>(
-       np, S.geom->panels.get(), S.geom->phi_row.get(), S.num_charges, S.charge_pos.get(), S.charge_q.get(), rhs,
-       nullptr, 0);
+       np, PanelTargets{S.geom->panels.get()}, S.geom->phi_row.get(), S.num_charges, S.charge_pos.get(),
+       S.charge_q.get(), rhs, nullptr, 0);
    FFTSVD_CHECK_LAUNCH();
 }
 
@@ -225,7 +254,8 @@ void rhs_groups_device(Surface& S, int ngroups, const int32_t* gptr_host, double
    FFTSVD_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * S.n * ngroups, S.stream));
    const int np = S.geom->num_panels;
    rhs_kernel<<<dim3((np + kRhsThreads - 1) / kRhsThreads, ngroups), kRhsThreads, 0, S.stream>>>(
-       np, S.geom->panels.get(), S.geom->phi_row.get(), 0, S.charge_pos.get(), S.charge_q.get(), rhs, gptr.get(), S.n);
+       np, PanelTargets{S.geom->panels.get()}, S.geom->phi_row.get(), 0, S.charge_pos.get(), S.charge_q.get(), rhs,
+       gptr.get(), S.n);
    FFTSVD_CHECK_LAUNCH();
    FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
 }

@@ -25,6 +25,10 @@ void set_charges(Surface& S, int num_charges, const double* pos, const double* q
 
 // rhs[phi_row[i]] = sum_j q_j / |x_j - c_i|, other rows zero.  Device pointer.
 void rhs_device(Surface& S, double* rhs);
+// rhs[rows[i]] += sum_j q_j / |x_j - c_i| for nt target centroids c (xyz triples), charges in
+// order (SurfaceOperator.c:298-312).  Device pointers; asynchronous on `stream`.
+void rhs_points_device(int nt, const double* centroids, const int32_t* rows, int nq, const double* qpos,
+                       const double* q, double* rhs, cudaStream_t stream);
 // phi_j = sum_i (dphi_i SLP(x_j, i) - phi_i DLP(x_j, i)) - 4 pi phi_i [x_j == c_i].  Device pointers.
 void reaction_device(Surface& S, const double* sol, double* phi);
 // The same sum for nq points against an explicit panel set, all device arrays:

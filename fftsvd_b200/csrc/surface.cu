@@ -15,6 +15,7 @@
 namespace fftsvd {
 
 std::atomic<long long> g_kernel_launches{0};
+std::atomic<long long> g_device_allocs{0};
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -434,6 +435,7 @@ int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, d
 }
 
 long long fftsvd_b200_launch_count(void) { return g_kernel_launches.load(); }
+long long fftsvd_b200_device_alloc_count(void) { return g_device_allocs.load(); }
 
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s) { return s ? (void*)s->s.stream : nullptr; }
 

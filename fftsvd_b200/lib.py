@@ -29,7 +29,8 @@ EXPORTED = [
     "fftsvd_b200_matvec_bytes", "fftsvd_b200_surface_stats", "fftsvd_b200_host_setup",
     "fftsvd_b200_host_operator_tree", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
     "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
-    "fftsvd_b200_launch_count", "fftsvd_b200_reaction_potentials_noalloc", "solveSurfaceOperator", "generateRHS",
+    "fftsvd_b200_launch_count", "fftsvd_b200_device_alloc_count", "fftsvd_b200_reaction_potentials_noalloc",
+    "solveSurfaceOperator", "generateRHS",
     "collectPotentials",
     "fftsvd_b200_matvec_batch_device", "fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch",
     "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
@@ -89,6 +90,7 @@ def load():
     lib.fftsvd_b200_surface_stream.argtypes = [sp]
     lib.fftsvd_b200_surface_stream.restype = C.c_void_p
     lib.fftsvd_b200_launch_count.restype = C.c_longlong
+    lib.fftsvd_b200_device_alloc_count.restype = C.c_longlong
     lib.fftsvd_b200_reaction_potentials_noalloc.argtypes = [sp, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_matvec_batch_device.argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
     for name in ("fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch", "fftsvd_b200_solve_block_device",

@@ -228,15 +228,23 @@ int fftsvd_b200_reaction_potentials_device(fftsvd_surface* s, const double* sol,
    device synchronisation of cudaMalloc/cudaFree is not acceptable.  sol
    (2N doubles) and phi (one double per charge) are device pointers the caller
    allocated; the surface itself was allocated when it was created.
+   The call reads sol on the surface's own stream (fftsvd_b200_surface_stream)
+   without waiting for any other stream: every write to sol must have finished
+   before the call, for example by making the surface's stream wait on an event
+   recorded after the writes, or by synchronising the writing stream.
    The per-chunk partial sums live in one file-scope device array of
    524288 doubles (4 MiB), which every GPU that loads this library holds until
    the process exits; surfaces with more than 524288 charges are rejected with
-   FFTSVD_ERR_ARGUMENT.  The first call on a device looks up that array's
-   device address with the surface's device current; make that first call
-   before any stream capture.  All calls share the one array and every call
-   overwrites the entries it reads, so nothing carries over between calls;
-   calls that overlap on the GPU (different threads or streams) race on it.
-   The call returns after its work on the surface's stream has finished. */
+   FFTSVD_ERR_ARGUMENT before any launch.  Up to 8192 charges the panels are
+   split into the same 64 chunks as in fftsvd_b200_reaction_potentials; above
+   that into 524288 / charges chunks, so the sums are grouped differently and
+   agree with the allocating call to rounding, not bit for bit.  The first call
+   on a device looks up that array's device address with the surface's device
+   current; that first call should come before any stream capture.  All calls
+   share the one array and every call overwrites the entries it reads, so
+   nothing carries over between calls; calls that overlap on the GPU
+   (different threads or streams) race on it.  The call returns after its work
+   on the surface's stream has finished. */
 int fftsvd_b200_reaction_potentials_noalloc(fftsvd_surface* s, const double* sol, double* phi);
 /* 0.5 * sum q phi * 332.112 / eps_in (FFTSVDsalt.c:167-170). */
 int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
@@ -365,6 +373,8 @@ int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const 
                                       double* energies);
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
+/* Device allocations (cudaMalloc calls) made by this library since it was loaded. */
+long long fftsvd_b200_device_alloc_count(void);
 
 /* ---- drop-in replacements for FFTSVDpbeAPI.h (reference types are opaque here) ----
    The declarations in FFTSVDpbeAPI.h are ABI-identical.  PDBentry is an

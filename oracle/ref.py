@@ -20,6 +20,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# the reference source tree (read-only; only the oracle build and the CPU tests that
+# compile against its headers read it): FFTSVD_REFERENCE, else the Makefile's default
+REFERENCE_TREE = os.environ.get("FFTSVD_REFERENCE") or "/root/reference"
 sys.path.insert(0, os.path.dirname(HERE))
 from fftsvd_b200._abi import TreeFlat, tree_flat_to_numpy  # noqa: E402
 

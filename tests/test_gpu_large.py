@@ -1,0 +1,67 @@
+"""Parity at the benchmark sizes: the GPU solves of the 81 920-panel blob (2 500
+charges) and the 327 680-panel blob (30 000 charges) against the compiled
+reference's FP64 build on the same seeded inputs.  The reference takes minutes to
+hours on these systems, so its results were computed once by
+tests/golden/make_golden_large.py and committed (tests/golden/blob6_ref64.npz,
+blob7_ref64.npz): the energy of its GMRES solve at relative residual 1e-6, its
+reaction potentials, a strided sample of its surface solution, and its energy at
+1e-10.
+
+Bars (both solves stop at a relative preconditioned residual of 1e-6, so their
+solutions differ by about the tolerance times the conditioning of the
+preconditioned operator):
+  dG                relative 1e-6 (the plan's accuracy target)
+  phi_reac          relative 2-norm 1e-5
+  surface solution  relative 2-norm of the sampled entries 1e-4
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from fftsvd_b200.surface import Surface
+from helpers import GOLDEN, rel
+
+pytestmark = pytest.mark.gpu
+sys.path.insert(0, GOLDEN)
+
+DG_TOL = 1e-6
+PHI_TOL = 1e-5
+SOL_TOL = 1e-4
+
+
+def _load(name):
+    path = os.path.join(GOLDEN, name + "_ref64.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing fixture {path}: run tests/golden/make_golden_large.py {name}")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("name", ["blob6", "blob7"])
+def test_benchmark_size_solve_matches_reference_fp64(gpu, name):
+    import make_golden_large as mg  # tests/golden: the inputs of the fixture and their hash
+
+    g = _load(name)
+    tri, qpos, q, c = mg.make_inputs(name)
+    assert mg.inputs_hash(tri, qpos, q) == str(g["inputs_sha256"]), "the seeded generators changed"
+    s = Surface.from_problem(tri, qpos, q, c["eps_in"], c["eps_out"], c["kappa"], svd_tol=float(g["svd_tol"]))
+    rhs = s.rhs()
+    stride = int(g["sol_stride"])
+    report = {}
+    for precision in ("mixed", "fp64"):
+        r = s.solve(rhs, precision=precision, tol=float(g["gmres_tol"]))
+        phi = s.reaction_potentials(r.solution)
+        dG = s.energy(phi)
+        e_dG = abs(dG - float(g["dG"])) / abs(float(g["dG"]))
+        e_tight = abs(dG - float(g["dG_tight"])) / abs(float(g["dG_tight"]))
+        e_phi = rel(phi, g["phi"])
+        e_sol = rel(r.solution[::stride], g["sol_sample"])
+        report[precision] = (dG, e_dG, e_tight, e_phi, e_sol, r.iterations)
+        print(f"{name} {precision}: dG {dG:.9f} (reference {float(g['dG']):.9f}) rel {e_dG:.2e}, "
+              f"vs converged {e_tight:.2e}; phi {e_phi:.2e}; solution {e_sol:.2e}; {r.iterations} iterations")
+    s.close()
+    for precision, (dG, e_dG, e_tight, e_phi, e_sol, _) in report.items():
+        assert e_dG < DG_TOL, (precision, e_dG)
+        assert e_phi < PHI_TOL, (precision, e_phi)
+        assert e_sol < SOL_TOL, (precision, e_sol)

@@ -9,8 +9,10 @@ import subprocess
 
 import pytest
 
+import ref  # oracle: the reference tree location
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFERENCE = "/root/reference"
+REFERENCE = ref.REFERENCE_TREE
 
 # (reference type, mirror type, fields, compare sizeof)
 STRUCTS = [

@@ -13,10 +13,12 @@ import subprocess
 
 import pytest
 
+import ref  # oracle: the reference tree location
+
 from fftsvd_b200.lib import LIB_PATH
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFERENCE = "/root/reference"
+REFERENCE = ref.REFERENCE_TREE
 OBJ32 = os.path.join(ROOT, "oracle", "_ref", "obj32")
 DROPIN = ["solveSurfaceOperator", "generateRHS", "collectPotentials"]
 GLOBALS = ["errortolerance", "innerdielectric", "addcoulombic"]
