@@ -62,14 +62,33 @@ GMRES_TOL = 1e-6
 METRIC = "PBE solve ms & matvec GB/s, 40k-400k panels: mixed vs FP64 GPU at 1e-6 dG err"
 
 
-def make_workload(cfg):
+def make_workload(cfg, rank=0):
+    """The seeded system of a configuration.  Under torchrun every rank solves its own
+    system of the same size: rank 0 the configuration's, rank r > 0 the blob of seed
+    seed + 100 r (independent work, no replicas of one solve)."""
     from fftsvd_b200 import meshes
     if cfg["kind"] == "born":
         tri, qpos, q = meshes.born_ion(cfg["level"], cfg["radius"])
     else:
-        tri = meshes.blob(cfg["level"], cfg["radius"], seed=cfg["seed"])
-        qpos, q = meshes.blob_charges(tri, cfg["radius"], cfg["nq"], seed=cfg["seed"] + 1, surface_seed=cfg["seed"])
+        seed = cfg["seed"] + 100 * rank
+        tri = meshes.blob(cfg["level"], cfg["radius"], seed=seed)
+        qpos, q = meshes.blob_charges(tri, cfg["radius"], cfg["nq"], seed=seed + 1, surface_seed=seed)
     return tri, qpos, q
+
+
+def golden_ref64(name, tri, qpos, q):
+    """The reference FP64 build's results on this system (tests/golden/<name>_ref64.npz,
+    written by tests/golden/make_golden_large.py), or None when the fixture is absent or
+    was made from other inputs."""
+    import hashlib
+    path = os.path.join(ROOT, "tests", "golden", name + "_ref64.npz")
+    if not os.path.exists(path):
+        return None
+    g = np.load(path)
+    h = hashlib.sha256()
+    for a in (tri, qpos, q):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return g if h.hexdigest() == str(g["inputs_sha256"]) else None
 
 
 def hbm_peak():
@@ -225,6 +244,103 @@ def run_reference(args, cfg, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _time_solves(s, stream, flush, rhs, sol, precision, k, warm):
+    """k timed solves (CUDA events on the library stream, L2 flushed before each) after
+    warm untimed ones: total ms and the last solve's info."""
+    import torch
+    for _ in range(warm):
+        s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
+    total, info = 0.0, None
+    for _ in range(k):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total, info
+
+
+def _setup_stats(s):
+    from fftsvd_b200 import _abi
+    from fftsvd_b200.lib import load
+    st = _abi.SurfaceStats()
+    load().fftsvd_b200_surface_stats(s._h, C.byref(st))
+    return st
+
+
+def _ref64_errors(g, e_mixed, e64):
+    if g is None:
+        return None
+    r = float(g["dG"])
+    return {"dG_ref_fp64": r, "dG_ref_fp64_converged": float(g["dG_tight"]),
+            "mixed": abs(e_mixed - r) / abs(r), "fp64": abs(e64 - r) / abs(r),
+            "mixed_vs_converged": abs(e_mixed - float(g["dG_tight"])) / abs(float(g["dG_tight"]))}
+
+
+def run_large(flush, steps, warmup):
+    """The 327 680-panel blob (30 000 charges): mixed and FP64 solve times, their ratio and
+    their energies against the reference FP64 build (committed fixture)."""
+    import torch
+    from fftsvd_b200.lib import load
+    from fftsvd_b200.surface import Surface
+    cfg = CONFIGS["large"]
+    tri, qpos, q = make_workload(cfg)
+    t0 = time.time()
+    s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
+    setup_s = time.time() - t0
+    st = _setup_stats(s)
+    stream = torch.cuda.ExternalStream(load().fftsvd_b200_surface_stream(s._h))
+    rhs = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    s.rhs_device(rhs.data_ptr())
+    sol = torch.empty_like(rhs)
+    torch.cuda.synchronize()
+    tm, im = _time_solves(s, stream, flush, rhs, sol, "mixed", steps, warmup)
+    em = s.energy(s.reaction_potentials(sol.cpu().numpy()))
+    k64 = max(1, steps // 2)
+    t64, i64 = _time_solves(s, stream, flush, rhs, sol, "fp64", k64, 1)
+    e64 = s.energy(s.reaction_potentials(sol.cpu().numpy()))
+    out = {"workload": cfg["name"], "panels": len(tri), "charges": len(q), "steps": steps,
+           "mixed_ms": tm / steps, "fp64_ms": t64 / k64, "speedup_mixed_vs_fp64": (t64 / k64) / (tm / steps),
+           "iterations_mixed": im.iterations, "refinements_mixed": im.refinements, "iterations_fp64": i64.iterations,
+           "dG_kcal_mixed": em, "dG_kcal_fp64": e64, "dG_rel_err_mixed_vs_fp64": abs(em - e64) / abs(e64),
+           "dG_rel_err_vs_ref_fp64": _ref64_errors(golden_ref64("blob7", tri, qpos, q), em, e64),
+           "setup_s": setup_s, "setup_stage_ms": list(st.setup_ms)}
+    s.close()
+    return out
+
+
+def run_block256(s, qpos, q, cfg, flush, fp64_single_ms):
+    """The blob's charges in 256 seeded disjoint groups, one right-hand side per group,
+    solved as one block GMRES (mixed precision) on the same surface; against 256 plain
+    FP64 single solves of the headline system's size."""
+    import torch
+    from fftsvd_b200.lib import load
+    groups = 256
+    perm, gptr = charge_groups(len(q), groups, cfg["seed"])
+    s.set_charges(qpos[perm], q[perm])
+    stream = torch.cuda.ExternalStream(load().fftsvd_b200_surface_stream(s._h))
+    R = torch.empty((groups, s.n), dtype=torch.float64, device="cuda")
+    S = torch.empty_like(R)
+    s.rhs_groups_device(gptr, R.data_ptr())
+    s.solve_block_device(R.data_ptr(), S.data_ptr(), groups, "mixed", GMRES_TOL, 150)  # warm-up
+    with torch.cuda.stream(stream):
+        flush.fill_(1.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    info = s.solve_block_device(R.data_ptr(), S.data_ptr(), groups, "mixed", GMRES_TOL, 150)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.set_charges(qpos, q)
+    return {"workload": f"{cfg['name']}, charges in {groups} seeded groups", "right_hand_sides": groups,
+            "block_mixed_ms": ms, "ms_per_rhs": ms / groups, "fp64_single_solve_ms": fp64_single_ms,
+            "speedup_vs_fp64_single_solves": fp64_single_ms * groups / ms,
+            "block_steps_max": max(info[c].iterations for c in range(groups))}
+
+
 def run_ours(args, cfg, ws, rank, local):
     import torch
     from fftsvd_b200 import _abi
@@ -233,12 +349,11 @@ def run_ours(args, cfg, ws, rank, local):
 
     torch.cuda.set_device(local)
     lib = load()
-    tri, qpos, q = make_workload(cfg)
+    tri, qpos, q = make_workload(cfg, rank)
     t0 = time.time()
     s = Surface.from_problem(tri, qpos, q, cfg["eps_in"], cfg["eps_out"], cfg["kappa"], svd_tol=SVD_TOL)
     setup_s = time.time() - t0
-    st = _abi.SurfaceStats()
-    lib.fftsvd_b200_surface_stats(s._h, C.byref(st))
+    st = _setup_stats(s)
     n = s.n
     stream = torch.cuda.ExternalStream(lib.fftsvd_b200_surface_stream(s._h))
     rhs = torch.empty(n, dtype=torch.float64, device="cuda")
@@ -247,42 +362,28 @@ def run_ours(args, cfg, ws, rank, local):
     sol = torch.empty_like(rhs)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
 
-    def timed_solves(precision, k, warm):
-        for _ in range(warm):
-            s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
-        total = 0.0
-        info = None
-        for _ in range(k):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            info = s.solve_device(rhs.data_ptr(), sol.data_ptr(), precision, GMRES_TOL)
-            e1.record(stream)
-            e1.synchronize()
-            total += e0.elapsed_time(e1)
-        return total, info
-
     barrier(ws)
     torch.cuda.synchronize()
     launches0 = lib.fftsvd_b200_launch_count()
     with ClockSampler(local) as clk:
-        t_mixed, info_mixed = timed_solves("mixed", args.steps, args.warmup)
-    launches = lib.fftsvd_b200_launch_count() - launches0 - 0
+        t_mixed, info_mixed = _time_solves(s, stream, flush, rhs, sol, "mixed", args.steps, args.warmup)
+    launches = lib.fftsvd_b200_launch_count() - launches0
     torch.cuda.synchronize()
     barrier(ws)
     t_max = barrier_max(t_mixed, ws)
     ms_per_step = t_max / args.steps
-    value = t_max / (args.steps * ws)
+    value = t_max / (args.steps * ws)  # ws independent systems solved per step
     x_mixed = sol.cpu().numpy()
 
     # plain FP64 GPU solve of the same system (the comparison the target is stated against)
     k64 = max(1, args.steps // 2)
-    t64, info64 = timed_solves("fp64", k64, 1)
+    t64, info64 = _time_solves(s, stream, flush, rhs, sol, "fp64", k64, 1)
     x64 = sol.cpu().numpy()
     fp64_ms = t64 / k64
     e_mixed = s.energy(s.reaction_potentials(x_mixed))
     e64 = s.energy(s.reaction_potentials(x64))
+    ref64 = _ref64_errors(golden_ref64("blob6", tri, qpos, q) if cfg is CONFIGS["blob"] and rank == 0 else None,
+                          e_mixed, e64)
 
     # matvec: per-kernel CUDA-event times on the library stream, algorithmic bytes per kernel
     xv = torch.randn(n, dtype=torch.float64, device="cuda")
@@ -348,6 +449,11 @@ def run_ours(args, cfg, ws, rank, local):
             if len(cells) == 3 and cells[0] == key and cells[1] == dom and cells[2].isdigit():
                 traffic = float(cells[2])
 
+    # the other end of the metric's panel range and the batched solve: one GPU only
+    extras = ws == 1 and cfg is CONFIGS["blob"] and not args.no_extras
+    large = run_large(flush, max(3, args.steps // 4), 2) if extras else None
+    block = run_block256(s, qpos, q, cfg, flush, fp64_ms) if extras else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -363,7 +469,9 @@ def run_ours(args, cfg, ws, rank, local):
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": cfg["name"], "panels": len(tri), "charges": len(q), "svd_tol": SVD_TOL,
                        "gmres_tol": GMRES_TOL, "precision": "FP32 operator, FP64 Krylov + FP64 refinement",
-                       "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas x{ws}",
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": "one system per GPU" if ws == 1 else
+                                      f"{ws} independent seeded systems of this size, one per GPU",
                        "depth": list(st.depth), "leaves": list(st.num_leaves), "far_cubes": list(st.num_cubes)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
@@ -376,11 +484,13 @@ def run_ours(args, cfg, ws, rank, local):
             "iterations_mixed": info_mixed.iterations, "refinements_mixed": info_mixed.refinements,
             "iterations_fp64": info64.iterations,
             "dG_kcal_mixed": e_mixed, "dG_kcal_fp64": e64, "dG_rel_err_mixed_vs_fp64": abs(e_mixed - e64) / abs(e64),
+            "dG_rel_err_vs_ref_fp64": ref64,
             "matvec_ms_fp32": prof["fp32"]["total_ms"], "matvec_ms_fp64": prof["fp64"]["total_ms"],
             "matvec_ms_fp32_streams": mv_streams["fp32"], "matvec_ms_fp64_streams": mv_streams["fp64"],
             "matvec_gbs_fp32": mv_bytes32 / (prof["fp32"]["total_ms"] * 1e6),
             "matvec_gbs_fp64": mv_bytes64 / (prof["fp64"]["total_ms"] * 1e6),
-            "matvec_kernels": prof, "setup_s": setup_s,
+            "matvec_kernels": prof, "setup_s": setup_s, "setup_stage_ms": list(st.setup_ms),
+            "large": large, "batched_256_rhs": block,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -758,6 +868,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="blob")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the large-blob and 256-right-hand-side sections of the default line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

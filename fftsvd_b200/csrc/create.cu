@@ -1,7 +1,8 @@
 // fftsvd_b200_surface_create: the library's own replacement for the reference
 // operator construction of the single-molecule PBE problem
 // (generateSurfaceOperator + Tree_fill + generateSurfaceOperatorPreconditioner,
-// FFTSVDpbeAPI.c:1053-1739, 1853-1861): host setup (setup.cpp), then upload.
+// FFTSVDpbeAPI.c:1053-1739, 1853-1861): setup (setup.cpp) with its panel integrals
+// on the device (sampling.cu), then upload.
 #include <cmath>
 #include <vector>
 
@@ -21,9 +22,12 @@ extern "C" int fftsvd_b200_surface_create(const fftsvd_problem* pr, fftsvd_surfa
       if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(FFTSVD_ERR_NO_DEVICE, "no CUDA device visible");
       setup::HostOperator H;
       try {
-         setup::host_setup(*pr, H);
+         const setup::BatchEvaluator eval = setup::device_evaluator();
+         setup::host_setup(*pr, H, &eval);
       } catch (const std::invalid_argument& e) {
          throw Error(FFTSVD_ERR_ARGUMENT, e.what());
+      } catch (const setup::DeviceError& e) {
+         throw Error(e.code, e.what());
       }
       Surface& S = s->s;
       init_surface(S, 2 * H.n, 2, H.views, H.maps, &H.precond);

@@ -394,12 +394,48 @@ void Tree::fill_near() {
    std::vector<int> leaves;
    for (size_t i = 0; i < cubes.size(); i++)
       if (cubes[i].leaf) leaves.push_back((int)i);
+   for (int li : leaves) {
+      Cube& c = cubes[li];
+      c.dcols = c.panels;
+      for (int o : c.local) c.dcols.insert(c.dcols.end(), cubes[o].panels.begin(), cubes[o].panels.end());
+   }
+   if (eval) {
+      // every leaf block in one batch: Ds then Dd of each leaf, row-major
+      IntegralBatch B;
+      std::vector<int64_t> off(leaves.size(), -1);
+      for (size_t li = 0; li < leaves.size(); li++) {
+         const Cube& c = cubes[leaves[li]];
+         const int nr = (int)c.points.size(), nc = (int)c.dcols.size();
+         if (nr == 0 || nc == 0) continue;
+         IntegralBlock b;
+         b.npts = nr;
+         b.npan = nc;
+         b.pt_off = (int64_t)B.points.size() / 3;
+         for (int pt : c.points) B.points.insert(B.points.end(), &(*points)[3 * (size_t)pt], &(*points)[3 * (size_t)pt + 3]);
+         b.pan_off = (int64_t)B.panels.size();
+         B.panels.insert(B.panels.end(), c.dcols.begin(), c.dcols.end());
+         off[li] = B.out_elems;
+         b.out_s = B.out_elems;
+         b.out_d = B.out_elems + (int64_t)nr * nc;
+         b.ld_s = b.ld_d = nc;
+         B.out_elems += 2 * (int64_t)nr * nc;
+         B.blocks.push_back(b);
+      }
+      std::vector<double> out((size_t)B.out_elems);
+      (*eval)(kernel, *panels, B, out.data());
+#pragma omp parallel for schedule(static)
+      for (size_t li = 0; li < leaves.size(); li++) {
+         if (off[li] < 0) continue;
+         Cube& c = cubes[leaves[li]];
+         const size_t e = c.points.size() * c.dcols.size();
+         c.Ds.assign(out.begin() + off[li], out.begin() + off[li] + e);
+         c.Dd.assign(out.begin() + off[li] + e, out.begin() + off[li] + 2 * e);
+      }
+      return;
+   }
 #pragma omp parallel for schedule(dynamic, 4)
    for (size_t li = 0; li < leaves.size(); li++) {
       Cube& c = cubes[leaves[li]];
-      c.dcols.clear();
-      c.dcols = c.panels;
-      for (int o : c.local) c.dcols.insert(c.dcols.end(), cubes[o].panels.begin(), cubes[o].panels.end());
       const int nr = (int)c.points.size(), nc = (int)c.dcols.size();
       if (nr == 0 || nc == 0) continue;
       c.Ds.assign((size_t)nr * nc, 0.0);
@@ -473,18 +509,112 @@ void Tree::fill_T() {
    }
 }
 
+void Tree::row_samples(const Cube& c, const std::vector<int>& withpoints, int pass, std::vector<double>& R) const {
+   const int m = (int)c.panels.size(), nwp = (int)withpoints.size(), rows = 2 * nwp * pass;
+   R.assign((size_t)rows * m, 0.0);
+   for (int p = 0; p < pass; p++)
+      for (int r = 0; r < nwp; r++) {
+         const Cube& pc = cubes[withpoints[r]];
+         const int pi = (int)((unsigned)p * (unsigned)pc.points.size() / (unsigned)pass);
+         const double* pt = &(*points)[3 * (size_t)pc.points[pi]];
+         for (int k = 0; k < m; k++)
+            kernel.panel(pt, (*panels)[c.panels[k]], &R[(size_t)(p * nwp + r) * m + k],
+                         &R[(size_t)(p * nwp + r + nwp * pass) * m + k]);
+      }
+}
+
+void Tree::col_samples(const Cube& c, const std::vector<int>& withpanels, int pass, std::vector<double>& Cm) const {
+   const int np = (int)c.points.size(), nwq = (int)withpanels.size(), cols = 2 * nwq * pass;
+   Cm.assign((size_t)np * cols, 0.0);
+   for (int p = 0; p < pass; p++)
+      for (int q = 0; q < nwq; q++) {
+         const Cube& qc = cubes[withpanels[q]];
+         const int pi = (int)((unsigned)p * (unsigned)qc.panels.size() / (unsigned)pass);
+         const FlatPanel& pan = (*panels)[qc.panels[pi]];
+         for (int r = 0; r < np; r++) {
+            const double* pt = &(*points)[3 * (size_t)c.points[r]];
+            kernel.panel(pt, pan, &Cm[(size_t)r * cols + p * nwq + q], &Cm[(size_t)r * cols + p * nwq + q + nwq * pass]);
+         }
+      }
+}
+
+void Tree::sphere_points(const Cube& c, double (*sphere)[3]) const {
+   const double box = c.b1[0] - c.b0[0];
+   for (int q = 0; q < kNumSphere; q++)
+      for (int k = 0; k < 3; k++) sphere[q][k] = kSphere49[q][k] * (box * 1.5) + c.center[k];
+}
+
 void Tree::fill_bases() {
    std::vector<int> work;
    for (size_t i = 0; i < cubes.size(); i++)
       if (!cubes[i].inter.empty()) work.push_back((int)i);
+   // interacting cubes with panels (column samples) and with points (row samples)
+   std::vector<std::vector<int>> wpan(work.size()), wpts(work.size());
+   for (size_t wi = 0; wi < work.size(); wi++)
+      for (int o : cubes[work[wi]].inter) {
+         if (!cubes[o].panels.empty()) wpan[wi].push_back(o);
+         if (!cubes[o].points.empty()) wpts[wi].push_back(o);
+      }
+   // With an evaluator the first sampling pass of every cube and its sphere fits are
+   // integrated in one batch; a cube whose first pass does not settle its rank samples its
+   // further passes on the host as before.
+   std::vector<double> pre;
+   std::vector<int64_t> roff(work.size(), -1), coff(work.size(), -1), soff(work.size(), -1);
+   if (eval) {
+      IntegralBatch B;
+      auto add_point = [&](const double* p) { B.points.insert(B.points.end(), p, p + 3); };
+      for (size_t wi = 0; wi < work.size(); wi++) {
+         const Cube& c = cubes[work[wi]];
+         const int m = (int)c.panels.size(), np = (int)c.points.size();
+         const int nwp = (int)wpts[wi].size(), nwq = (int)wpan[wi].size();
+         if (m > 0 && nwp > 0) {
+            IntegralBlock b;
+            b.pan_off = (int64_t)B.panels.size();
+            B.panels.insert(B.panels.end(), c.panels.begin(), c.panels.end());
+            b.npan = m;
+            b.npts = nwp;
+            b.pt_off = (int64_t)B.points.size() / 3;
+            for (int o : wpts[wi]) add_point(&(*points)[3 * (size_t)cubes[o].points[0]]);
+            roff[wi] = b.out_s = B.out_elems;
+            b.out_d = B.out_elems + (int64_t)nwp * m;
+            b.ld_s = b.ld_d = m;
+            B.out_elems += 2 * (int64_t)nwp * m;
+            B.blocks.push_back(b);
+            // sphere fits of the same panels
+            IntegralBlock sb = b;
+            double sphere[kNumSphere][3];
+            sphere_points(c, sphere);
+            sb.npts = kNumSphere;
+            sb.pt_off = (int64_t)B.points.size() / 3;
+            for (int q = 0; q < kNumSphere; q++) add_point(sphere[q]);
+            soff[wi] = sb.out_s = B.out_elems;
+            sb.out_d = B.out_elems + (int64_t)kNumSphere * m;
+            B.out_elems += 2 * (int64_t)kNumSphere * m;
+            B.blocks.push_back(sb);
+         }
+         if (np > 0 && nwq > 0) {
+            IntegralBlock b;
+            b.pan_off = (int64_t)B.panels.size();
+            for (int o : wpan[wi]) B.panels.push_back(cubes[o].panels[0]);
+            b.npan = nwq;
+            b.npts = np;
+            b.pt_off = (int64_t)B.points.size() / 3;
+            for (int pt : c.points) add_point(&(*points)[3 * (size_t)pt]);
+            coff[wi] = b.out_s = B.out_elems;
+            b.out_d = B.out_elems + nwq;
+            b.ld_s = b.ld_d = 2 * nwq;
+            B.out_elems += (int64_t)np * 2 * nwq;
+            B.blocks.push_back(b);
+         }
+      }
+      pre.resize((size_t)B.out_elems);
+      (*eval)(kernel, *panels, B, pre.data());
+   }
 #pragma omp parallel for schedule(dynamic, 1)
    for (size_t wi = 0; wi < work.size(); wi++) {
       Cube& c = cubes[work[wi]];
-      std::vector<int> withpanels, withpoints;
-      for (int o : c.inter) {
-         if (!cubes[o].panels.empty()) withpanels.push_back(o);
-         if (!cubes[o].points.empty()) withpoints.push_back(o);
-      }
+      const std::vector<int>& withpanels = wpan[wi];
+      const std::vector<int>& withpoints = wpts[wi];
       const int m = (int)c.panels.size(), np = (int)c.points.size();
       const int nwp = (int)withpoints.size(), nwq = (int)withpanels.size();
       c.rowrank = 0;
@@ -492,16 +622,11 @@ void Tree::fill_bases() {
       if (m > 0 && nwp > 0) {
          for (int pass = 1;; pass++) {
             const int rows = 2 * nwp * pass;
-            std::vector<double> R((size_t)rows * m);
-            for (int p = 0; p < pass; p++)
-               for (int r = 0; r < nwp; r++) {
-                  const Cube& pc = cubes[withpoints[r]];
-                  const int pi = (int)((unsigned)p * (unsigned)pc.points.size() / (unsigned)pass);
-                  const double* pt = &(*points)[3 * (size_t)pc.points[pi]];
-                  for (int k = 0; k < m; k++)
-                     kernel.panel(pt, (*panels)[c.panels[k]], &R[(size_t)(p * nwp + r) * m + k],
-                                  &R[(size_t)(p * nwp + r + nwp * pass) * m + k]);
-               }
+            std::vector<double> R;
+            if (pass == 1 && roff[wi] >= 0)
+               R.assign(pre.begin() + roff[wi], pre.begin() + roff[wi] + (int64_t)rows * m);
+            else
+               row_samples(c, withpoints, pass, R);
             std::vector<double> VT;
             const int rank = row_basis(R, rows, m, eps, VT);
             if (rank < rows / 2) {
@@ -514,17 +639,11 @@ void Tree::fill_bases() {
       if (np > 0 && nwq > 0) {
          for (int pass = 1;; pass++) {
             const int cols = 2 * nwq * pass;
-            std::vector<double> Cm((size_t)np * cols);
-            for (int p = 0; p < pass; p++)
-               for (int q = 0; q < nwq; q++) {
-                  const Cube& qc = cubes[withpanels[q]];
-                  const int pi = (int)((unsigned)p * (unsigned)qc.panels.size() / (unsigned)pass);
-                  const FlatPanel& pan = (*panels)[qc.panels[pi]];
-                  for (int r = 0; r < np; r++) {
-                     const double* pt = &(*points)[3 * (size_t)c.points[r]];
-                     kernel.panel(pt, pan, &Cm[(size_t)r * cols + p * nwq + q], &Cm[(size_t)r * cols + p * nwq + q + nwq * pass]);
-                  }
-               }
+            std::vector<double> Cm;
+            if (pass == 1 && coff[wi] >= 0)
+               Cm.assign(pre.begin() + coff[wi], pre.begin() + coff[wi] + (int64_t)np * cols);
+            else
+               col_samples(c, withpanels, pass, Cm);
             std::vector<double> U;
             const int rank = column_basis(Cm, np, cols, eps, U);
             if (rank < cols / 2) {
@@ -536,16 +655,20 @@ void Tree::fill_bases() {
       }
       // projection (P) and interpolation (I) on the equivalent-density grid, then PV and UTI
       const int n = grid[c.level], gp3 = n * n * n;
-      const double box = c.b1[0] - c.b0[0];
       const std::vector<double>& Pi = pinv[c.level];  // gp3 x 49
       double sphere[kNumSphere][3];
-      for (int q = 0; q < kNumSphere; q++)
-         for (int k = 0; k < 3; k++) sphere[q][k] = kSphere49[q][k] * (box * 1.5) + c.center[k];
+      sphere_points(c, sphere);
       if (m > 0 && c.rowrank > 0) {
          std::vector<double> Qs((size_t)kNumSphere * m), Qd((size_t)kNumSphere * m);
-         for (int q = 0; q < kNumSphere; q++)
-            for (int k = 0; k < m; k++)
-               kernel.panel(sphere[q], (*panels)[c.panels[k]], &Qs[(size_t)q * m + k], &Qd[(size_t)q * m + k]);
+         if (soff[wi] >= 0) {
+            const int64_t e = (int64_t)kNumSphere * m;
+            std::copy(pre.begin() + soff[wi], pre.begin() + soff[wi] + e, Qs.begin());
+            std::copy(pre.begin() + soff[wi] + e, pre.begin() + soff[wi] + 2 * e, Qd.begin());
+         } else {
+            for (int q = 0; q < kNumSphere; q++)
+               for (int k = 0; k < m; k++)
+                  kernel.panel(sphere[q], (*panels)[c.panels[k]], &Qs[(size_t)q * m + k], &Qd[(size_t)q * m + k]);
+         }
          // P = pinv Q2S (gp3 x m); PV = P VT^T (gp3 x r)
          const int r = c.rowrank;
          std::vector<double> Ps((size_t)gp3 * m, 0.0), Pd((size_t)gp3 * m, 0.0);
@@ -724,6 +847,22 @@ void FlatTree::view(fftsvd_tree_flat& t) const {
    t.t_level_ptr = t_level_ptr.data(); t.t_ops = t_ops.data();
 }
 
+BatchEvaluator host_evaluator() {
+   return [](const Kernel& k, const std::vector<FlatPanel>& pl, const IntegralBatch& B, double* out) {
+      const int64_t nb = (int64_t)B.blocks.size();
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int64_t bi = 0; bi < nb; bi++) {
+         const IntegralBlock& b = B.blocks[bi];
+         for (int i = 0; i < b.npts; i++) {
+            const double* p = &B.points[3 * (size_t)(b.pt_off + i)];
+            for (int j = 0; j < b.npan; j++)
+               k.panel(p, pl[B.panels[b.pan_off + j]], &out[b.out_s + (int64_t)i * b.ld_s + j],
+                       &out[b.out_d + (int64_t)i * b.ld_d + j]);
+         }
+      }
+   };
+}
+
 Timings build_tree(Tree& T, int max_panels) {
    Timings tm;
    auto now = [] { return std::chrono::steady_clock::now(); };
@@ -746,7 +885,7 @@ Timings build_tree(Tree& T, int max_panels) {
    return tm;
 }
 
-void host_setup(const fftsvd_problem& pr, HostOperator& H) {
+void host_setup(const fftsvd_problem& pr, HostOperator& H, const BatchEvaluator* eval) {
    if (pr.num_panels <= 0 || !pr.vertices) throw std::invalid_argument("no panels");
    if (!(pr.eps_in > 0 && pr.eps_out > 0)) throw std::invalid_argument("dielectric constants must be positive");
    if (!(pr.kappa >= 0 && std::isfinite(pr.kappa))) throw std::invalid_argument("kappa must be non-negative");
@@ -782,6 +921,7 @@ void host_setup(const fftsvd_problem& pr, HostOperator& H) {
       T.grid_points = pr.grid_points;
       T.kernel.yukawa = (t == 0) && pr.kappa > 0.0;
       T.kernel.kappa = (t == 0) ? pr.kappa : 0.0;
+      T.eval = eval;
       H.tm[t] = build_tree(T, pr.max_panels_per_leaf);
       H.depth[t] = T.depth;
       T.flatten(H.flat[t]);
@@ -854,6 +994,44 @@ extern "C" int fftsvd_b200_host_setup(const fftsvd_problem* problem, fftsvd_host
    if (!op) return FFTSVD_ERR_ARGUMENT;
    try {
       fftsvd::setup::host_setup(*problem, op->h);
+   } catch (const std::exception& e) {
+      fftsvd::set_last_error(e.what());
+      delete op;
+      return FFTSVD_ERR_ARGUMENT;
+   }
+   *out = op;
+   return FFTSVD_OK;
+}
+
+extern "C" int fftsvd_b200_host_setup_batched(const fftsvd_problem* problem, fftsvd_host_operator** out) {
+   if (!problem || !out) return FFTSVD_ERR_ARGUMENT;
+   *out = nullptr;
+   auto* op = new (std::nothrow) fftsvd_host_operator();
+   if (!op) return FFTSVD_ERR_ARGUMENT;
+   try {
+      const fftsvd::setup::BatchEvaluator eval = fftsvd::setup::host_evaluator();
+      fftsvd::setup::host_setup(*problem, op->h, &eval);
+   } catch (const std::exception& e) {
+      fftsvd::set_last_error(e.what());
+      delete op;
+      return FFTSVD_ERR_ARGUMENT;
+   }
+   *out = op;
+   return FFTSVD_OK;
+}
+
+extern "C" int fftsvd_b200_device_setup(const fftsvd_problem* problem, fftsvd_host_operator** out) {
+   if (!problem || !out) return FFTSVD_ERR_ARGUMENT;
+   *out = nullptr;
+   auto* op = new (std::nothrow) fftsvd_host_operator();
+   if (!op) return FFTSVD_ERR_ARGUMENT;
+   try {
+      const fftsvd::setup::BatchEvaluator eval = fftsvd::setup::device_evaluator();
+      fftsvd::setup::host_setup(*problem, op->h, &eval);
+   } catch (const fftsvd::setup::DeviceError& e) {
+      fftsvd::set_last_error(e.what());
+      delete op;
+      return e.code;
    } catch (const std::exception& e) {
       fftsvd::set_last_error(e.what());
       delete op;

@@ -2,6 +2,9 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "../../include/fftsvd_b200.h"
@@ -16,6 +19,29 @@ struct Kernel {
    void panel(const double* point, const FlatPanel& p, double* slp, double* dlp) const;
    double point(const double* dest, const double* src) const;
 };
+
+// A block of panel integrals: the single- and double-layer integrals of every panel of a
+// panel list at every point of a point list, written row by row into one output array
+// (point i, panel k: slp at out_s + i * ld_s + k, dlp at out_d + i * ld_d + k).
+struct IntegralBlock {
+   int32_t npts = 0, npan = 0;
+   int64_t pt_off = 0;   // first point (xyz triple) in IntegralBatch::points
+   int64_t pan_off = 0;  // first panel index in IntegralBatch::panels
+   int64_t out_s = 0, out_d = 0;
+   int32_t ld_s = 0, ld_d = 0;
+};
+struct IntegralBatch {
+   std::vector<double> points;   // 3 per point
+   std::vector<int32_t> panels;  // indices into the tree's panels
+   std::vector<IntegralBlock> blocks;
+   int64_t out_elems = 0;        // size of the output array
+};
+
+// Evaluates every block of a batch with one kernel over the tree's panels into out
+// (out_elems doubles).  Trees without an evaluator integrate on the host, panel by
+// panel; the device evaluator (sampling.cu) runs the same integrals on the GPU.
+using BatchEvaluator =
+    std::function<void(const Kernel& k, const std::vector<FlatPanel>& panels, const IntegralBatch& b, double* out)>;
 
 struct Cube {
    int level = 0;
@@ -58,6 +84,7 @@ struct Tree {
    std::vector<Cube> cubes;                  // cubes[0] is the root
    std::vector<std::vector<double>> pinv;    // per level, n^3 x 49
    std::vector<std::vector<double>> tops;    // per level, 343 slots x padded grid complex (re, im)
+   const BatchEvaluator* eval = nullptr;     // near-field blocks and first-pass samples in batches
 
    void build_cubes(int depth);
    void choose_depth(int max_panels);
@@ -66,6 +93,12 @@ struct Tree {
    void fill_pinv();
    void fill_T();
    void fill_bases();
+   // sampled matrices of one cube (Cube.c:1104-1281): row samples of `pass` passes
+   // (2 nwp pass x m), column samples (np x 2 nwq pass), and the 49-point sphere fits
+   // of its panels (49 x m each layer)
+   void row_samples(const Cube& c, const std::vector<int>& withpoints, int pass, std::vector<double>& R) const;
+   void col_samples(const Cube& c, const std::vector<int>& withpanels, int pass, std::vector<double>& Cm) const;
+   void sphere_points(const Cube& c, double (*sphere)[3]) const;
    void flatten(FlatTree& F) const;
 };
 
@@ -94,8 +127,22 @@ struct HostOperator {
    fftsvd_precond_csc precond;
 };
 
-// Build the two-region operator on the host (no GPU involved).
-void host_setup(const fftsvd_problem& pr, HostOperator& H);
+// Build the two-region operator on the host.  With an evaluator the near-field blocks,
+// the first-pass basis samples and the sphere fits are integrated in batches through it
+// (the GPU with device_evaluator()); without one everything runs on the host.
+void host_setup(const fftsvd_problem& pr, HostOperator& H, const BatchEvaluator* eval = nullptr);
+
+// The same batches evaluated on the host, block by block (the batch layout without the
+// device's rounding).
+BatchEvaluator host_evaluator();
+
+// The panel-integral evaluator on the current CUDA device (sampling.cu).  It keeps a
+// device copy of the panel list between calls and throws DeviceError on a CUDA failure.
+BatchEvaluator device_evaluator();
+struct DeviceError : std::runtime_error {
+   int code;
+   DeviceError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
 
 int column_basis(const std::vector<double>& A, int rows, int cols, double eps, std::vector<double>& Q);
 int row_basis(const std::vector<double>& A, int rows, int cols, double eps, std::vector<double>& VT);

@@ -355,15 +355,20 @@ def solve_many(surfaces, rhs_ptrs, sol_ptrs, precision="mixed", tol=1e-6, max_it
 
 
 def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4,
-                  num_threads=0):
-    """Run only the host setup (no GPU): returns ([exterior tree, interior tree], preconditioner) as numpy."""
+                  num_threads=0, integrals="host"):
+    """Run only the setup: returns ([exterior tree, interior tree], preconditioner) as numpy.
+    integrals: "host" (fftsvd_b200_host_setup), "device" (the panel integrals in batches
+    on the current CUDA device, fftsvd_b200_device_setup) or "batched" (the device path's
+    batches evaluated on the host, fftsvd_b200_host_setup_batched)."""
     lib = load()
     vv = f64(vertices)
     zero3, zero1 = np.zeros(3), np.zeros(1)
     p = Problem(len(vv), ptr(vv), 0, ptr(zero3), ptr(zero1), float(eps_in), float(eps_out), float(kappa),
                 float(svd_tol), int(max_panels_per_leaf), int(grid_points), int(num_threads))
     h = C.c_void_p()
-    check(lib.fftsvd_b200_host_setup(C.byref(p), C.byref(h)))
+    setup = {"host": lib.fftsvd_b200_host_setup, "device": lib.fftsvd_b200_device_setup,
+             "batched": lib.fftsvd_b200_host_setup_batched}[integrals]
+    check(setup(C.byref(p), C.byref(h)))
     try:
         trees = []
         for t in range(2):

@@ -178,6 +178,18 @@ int fftsvd_b200_surface_create(const fftsvd_problem* problem, fftsvd_surface** o
 typedef struct fftsvd_host_operator fftsvd_host_operator;
 int fftsvd_b200_host_setup(const fftsvd_problem* problem, fftsvd_host_operator** out);
 int fftsvd_b200_host_operator_tree(const fftsvd_host_operator* op, int32_t tree, fftsvd_tree_flat* view);
+/* The same setup with its panel integrals on the current CUDA device: the near-field
+   blocks (Cube.c:715-793), the first sampling pass of every cube's row and column bases
+   and the 49-point sphere fits (Cube.c:1104-1281, 795-1002) are integrated in FP64 in one
+   batched launch per tree; the rank-revealing factorisations, projections and
+   translation operators stay on the host.  The integrals agree with the host ones to
+   rounding (the device's FP64 sqrt, log, exp and atan2 against the host's).
+   fftsvd_b200_surface_create uses this path. */
+int fftsvd_b200_device_setup(const fftsvd_problem* problem, fftsvd_host_operator** out);
+/* The device setup's batches of panel integrals evaluated on the host instead: the
+   same operator as fftsvd_b200_host_setup, bit for bit (a check of the batch layout
+   that needs no GPU). */
+int fftsvd_b200_host_setup_batched(const fftsvd_problem* problem, fftsvd_host_operator** out);
 int fftsvd_b200_host_operator_precond(const fftsvd_host_operator* op, fftsvd_precond_csc* out);
 void fftsvd_b200_host_operator_free(fftsvd_host_operator* op);
 

@@ -7,12 +7,16 @@ blob7_ref64.npz): the energy of its GMRES solve at relative residual 1e-6, its
 reaction potentials, a strided sample of its surface solution, and its energy at
 1e-10.
 
-Bars (both solves stop at a relative preconditioned residual of 1e-6, so their
-solutions differ by about the tolerance times the conditioning of the
-preconditioned operator):
-  dG                relative 1e-6 (the plan's accuracy target)
-  phi_reac          relative 2-norm 1e-5
-  surface solution  relative 2-norm of the sampled entries 1e-4
+Bars.  The FP64 solve runs the reference's iteration on the same FP64 operator, so it
+lands on the reference's iterate up to rounding (measured on the 81 920-panel blob:
+dG 3e-13, phi 3e-13, solution 2e-12).  The mixed solve stops at the same relative
+preconditioned residual of 1e-6 from FP32-operator iterations refined in FP64, so it
+differs from the reference's iterate by about the tolerance times the conditioning
+of the preconditioned operator (measured: dG 4.0e-7, phi 2.9e-6, solution 3.2e-5):
+                    fp64     mixed
+  dG                1e-10    1e-6 (the plan's accuracy target)
+  phi_reac          1e-10    1e-5   (relative 2-norm)
+  surface solution  1e-10    1e-4   (relative 2-norm of the sampled entries)
 """
 import os
 import sys
@@ -26,9 +30,7 @@ from helpers import GOLDEN, rel
 pytestmark = pytest.mark.gpu
 sys.path.insert(0, GOLDEN)
 
-DG_TOL = 1e-6
-PHI_TOL = 1e-5
-SOL_TOL = 1e-4
+BARS = {"fp64": (1e-10, 1e-10, 1e-10), "mixed": (1e-6, 1e-5, 1e-4)}  # dG, phi, solution
 
 
 def _load(name):
@@ -62,6 +64,7 @@ def test_benchmark_size_solve_matches_reference_fp64(gpu, name):
               f"vs converged {e_tight:.2e}; phi {e_phi:.2e}; solution {e_sol:.2e}; {r.iterations} iterations")
     s.close()
     for precision, (dG, e_dG, e_tight, e_phi, e_sol, _) in report.items():
-        assert e_dG < DG_TOL, (precision, e_dG)
-        assert e_phi < PHI_TOL, (precision, e_phi)
-        assert e_sol < SOL_TOL, (precision, e_sol)
+        dg_tol, phi_tol, sol_tol = BARS[precision]
+        assert e_dG < dg_tol, (precision, e_dG)
+        assert e_phi < phi_tol, (precision, e_phi)
+        assert e_sol < sol_tol, (precision, e_sol)

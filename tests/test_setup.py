@@ -59,3 +59,23 @@ def test_host_setup_rejects_bad_input():
         host_operator(tri, 1.0, 80.0, 0.0)  # degenerate panels
     with pytest.raises(FFTSVDError):
         host_operator(np.full((4, 9), np.nan), 1.0, 80.0, 0.0)
+
+
+_FLAT_ARRAYS = ["leaf_row_ptr", "leaf_rows", "leaf_col_ptr", "leaf_cols", "leaf_d_ptr", "d_single", "d_double",
+                "cube_level", "cube_index", "cube_panel_ptr", "cube_panels", "cube_point_ptr", "cube_points",
+                "cube_row_rank", "cube_col_rank", "cube_vt_ptr", "vt", "cube_pv_ptr", "pv_single", "pv_double",
+                "cube_uti_ptr", "uti", "cube_u_ptr", "u", "inter_ptr", "inter_cubes", "t_level_ptr", "t_ops"]
+
+
+@pytest.mark.parametrize("name", ["born3", "blob3"])
+def test_batched_integrals_reproduce_host_setup_bit_for_bit(name):
+    """The device setup's batch layout (near-field blocks, first-pass samples, sphere fits),
+    evaluated on the host: the same operator as the per-cube host setup, bit for bit."""
+    from helpers import make_case
+    tri, _, _, c = make_case(name)
+    a, pa = host_operator(tri, c["eps_in"], c["eps_out"], c["kappa"], svd_tol=1e-4)
+    b, pb = host_operator(tri, c["eps_in"], c["eps_out"], c["kappa"], svd_tol=1e-4, integrals="batched")
+    for t in range(2):
+        for key in _FLAT_ARRAYS:
+            assert np.array_equal(a[t][key], b[t][key]), (t, key)
+    assert np.array_equal(pa["value"], pb["value"])
