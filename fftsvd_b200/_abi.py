@@ -72,7 +72,7 @@ class SolveInfo(C.Structure):
 
 class SurfaceStats(C.Structure):
     _fields_ = [("depth", C.c_int32 * 2), ("num_leaves", C.c_int32 * 2), ("num_cubes", C.c_int32 * 2),
-                ("setup_ms", C.c_double * 4), ("device_bytes", C.c_double), ("matvec_bytes_fp32", C.c_double),
+                ("setup_ms", C.c_double * 8), ("device_bytes", C.c_double), ("matvec_bytes_fp32", C.c_double),
                 ("matvec_bytes_fp64", C.c_double)]
 
 

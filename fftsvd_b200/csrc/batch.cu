@@ -269,7 +269,7 @@ int Surface::solve_batch(int precision, int k, const double* rhs, double* x, dou
                   iters, status);
    } else if (precision == FFTSVD_PREC_MIXED) {
       // FP64 iterative refinement around FP32-operator GMRES, column by column as in
-      // the single solve: x += A32^-1 (b - A64 x), inner targets 0.3 tol / residual
+      // the single solve: x += A32^-1 (b - A64 x), inner targets kInnerTarget tol / residual
       const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
       precond_batch(B.b0.get(), B.t0.get(), ncols);
       std::vector<double> bn;
@@ -288,7 +288,7 @@ int Surface::solve_batch(int precision, int k, const double* rhs, double* x, dou
          for (int c = 0; c < ncols; c++)
             if (run[c] && status[c] == FFTSVD_OK && res[c] >= tol) {
                act[c] = 1;
-               itol[c] = std::min(0.1, std::max(0.3 * tol / res[c], 1e-13));
+               itol[c] = std::min(0.1, std::max(kInnerTarget * tol / res[c], 1e-13));
                refinements[c]++;
                any = true;
             }

@@ -3,6 +3,7 @@
 // (generateSurfaceOperator + Tree_fill + generateSurfaceOperatorPreconditioner,
 // FFTSVDpbeAPI.c:1053-1739, 1853-1861): setup (setup.cpp) with its panel integrals
 // on the device (sampling.cu), then upload.
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -17,6 +18,10 @@ extern "C" int fftsvd_b200_surface_create(const fftsvd_problem* pr, fftsvd_surfa
    *out = nullptr;
    fftsvd_surface* s = new (std::nothrow) fftsvd_surface();
    if (!s) return FFTSVD_ERR_ARGUMENT;
+   const auto c0 = std::chrono::steady_clock::now();
+   auto ms_since = [](std::chrono::steady_clock::time_point t) {
+      return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+   };
    try {
       int ndev = 0;
       if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(FFTSVD_ERR_NO_DEVICE, "no CUDA device visible");
@@ -30,7 +35,9 @@ extern "C" int fftsvd_b200_surface_create(const fftsvd_problem* pr, fftsvd_surfa
          throw Error(e.code, e.what());
       }
       Surface& S = s->s;
+      const auto u0 = std::chrono::steady_clock::now();
       init_surface(S, 2 * H.n, 2, H.views, H.maps, &H.precond);
+      S.stats.setup_ms[6] = ms_since(u0);
       S.eps_in = pr->eps_in;
       std::vector<int32_t> dphi_rows(H.n);
       for (int i = 0; i < H.n; i++) dphi_rows[i] = H.n + i;
@@ -45,6 +52,9 @@ extern "C" int fftsvd_b200_surface_create(const fftsvd_problem* pr, fftsvd_surfa
       S.stats.setup_ms[1] = H.tm[0].near_ms + H.tm[1].near_ms;
       S.stats.setup_ms[2] = H.tm[0].pinv_t_ms + H.tm[1].pinv_t_ms;
       S.stats.setup_ms[3] = H.tm[0].bases_ms + H.tm[1].bases_ms;
+      S.stats.setup_ms[4] = H.tm[0].flatten_ms + H.tm[1].flatten_ms;
+      S.stats.setup_ms[5] = H.tm[0].integrals_ms + H.tm[1].integrals_ms;
+      S.stats.setup_ms[7] = ms_since(c0);
    } catch (const Error& e) {
       set_last_error(e.what());
       delete s;

@@ -158,7 +158,7 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
                               const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                               GivensState* __restrict__ st, int64_t hcol, int64_t pcol,
-                              const int32_t* __restrict__ active) {
+                              const int32_t* __restrict__ active, double2* __restrict__ hist) {
    extern __shared__ double gsh[];  // the new column (i + 2), then the previous rotations cs[i], sn[i]
    __shared__ double red[256];
    // column blockIdx.x of a batch: its own Hessenberg (ldh x ldh), rotations, g and state
@@ -220,6 +220,7 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
       st->residual = fabs(g[i + 1]) / st->normr;
       st->inv_beta = beta > 0.0 ? 1.0 / beta : 0.0;
       st->flag = !finite ? 2 : (beta == 0.0 ? 1 : 0);
+      if (hist) hist[i] = make_double2(st->residual, (double)st->flag);
    }
    __syncthreads();
    double* colh = H + (int64_t)i * ldh;
@@ -227,12 +228,16 @@ __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const doub
 }
 
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
-                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol) {
+                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol,
+                             double* __restrict__ dst2) {
    src += blockIdx.z * col;
    dst += blockIdx.z * col;
    const double f = factor_ptr ? factor_ptr[blockIdx.z * fcol] : factor;
-   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-      dst[k] = src[k] * f;
+   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+      const double v = src[k] * f;
+      dst[k] = v;
+      if (dst2) dst2[k] = v;
+   }
 }
 
 __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,

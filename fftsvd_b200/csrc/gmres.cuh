@@ -55,15 +55,19 @@ struct GivensState {
 // norm partials, applies the previous rotations, forms the new one, updates g
 // (GMRES.c:485-503).  One block per column with givens_smem(i) bytes of dynamic shared
 // memory; a column whose active flag is 0 (active may be null: all active) only zeroes
-// its inv_beta.
+// its inv_beta.  With hist (single column), hist[i] = {residual, flag} as well: the
+// residual history the host reads after several steps.
 __global__ void givens_kernel(int i, int ldh, double* __restrict__ H, const double* __restrict__ h1,
                               const double* __restrict__ h2, const double* __restrict__ norm_partial, int nblk,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                               GivensState* __restrict__ st, int64_t hcol, int64_t pcol,
-                              const int32_t* __restrict__ active);
+                              const int32_t* __restrict__ active, double2* __restrict__ hist = nullptr);
 
+// dst = src * (factor_ptr ? *factor_ptr : factor); dst2, if given (single column), receives
+// the same values.
 __global__ void scale_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ factor_ptr,
-                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol);
+                             double factor, double* __restrict__ dst, int64_t col, int64_t fcol,
+                             double* __restrict__ dst2 = nullptr);
 
 // x += V y  (y on device)
 __global__ void combine_kernel(int64_t n, int nvec, const double* __restrict__ V, int64_t ldv,

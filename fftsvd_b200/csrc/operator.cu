@@ -1699,11 +1699,36 @@ __device__ inline typename Vec2<T>::type shfl_c(typename Vec2<T>::type v, int sr
    return v;
 }
 
+// Bulk asynchronous prefetch (the TMA engine's cp.async.bulk.prefetch.L2) of bytes
+// [off, off + len) of a buffer of buf_bytes into L2: 16-byte aligned pieces of at most
+// 32 KiB that stay inside the buffer.  A prefetch only warms L2: it writes nothing, and
+// nothing waits for it.
+__device__ inline void prefetch_l2(const void* base, int64_t buf_bytes, int64_t off, int64_t len) {
+   int64_t a = off & ~int64_t(15);
+   const int64_t e = min((off + len + 15) & ~int64_t(15), buf_bytes & ~int64_t(15));
+   const char* p = static_cast<const char*>(base);
+   while (a < e) {
+      const unsigned n = (unsigned)min(e - a, int64_t(32768));
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + a), "r"(n) : "memory");
+      a += n;
+   }
+}
+
+// Bytes of the operator buffers the streaming kernels prefetch from, and how far ahead:
+// a warp about to work on unit u (a cube, or a leaf) prefetches the blocks of unit
+// u + ahead, the unit the same warp slot of the next wave of resident blocks will take
+// (ahead = resident warps of the launch; 0 disables the prefetch).
+struct Prefetch {
+   int64_t ahead = 0;
+   int64_t a_bytes = 0, b_bytes = 0, c_bytes = 0;  // VT, PV | UTI, U, translated | D
+};
+
 template <typename T>
 __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forward_n4_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
-    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
+    const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs,
+    Prefetch pre) {
    using T2 = typename Vec2<T>::type;
    const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
    xsd += rhs * bs.panels;
@@ -1721,6 +1746,11 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forw
    const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const SrcDesc c = cubes[cube];
+   if (pre.ahead > 0 && rhs == 0 && lane == 0 && cube + pre.ahead < count) {
+      const SrcDesc nc = cubes[cube + pre.ahead];
+      prefetch_l2(vt, pre.a_bytes, nc.vt_off * (int64_t)sizeof(T), (int64_t)nc.r * nc.m * (int64_t)sizeof(T));
+      prefetch_l2(pv, pre.b_bytes, nc.pv_off * (int64_t)sizeof(T2), (int64_t)nc.r * 64 * (int64_t)sizeof(T2));
+   }
    const int m = c.m, r = c.r;  // r <= 32: lane j owns row j of VT
    const int kq = lane & 3, jp = (lane >> 2) & 3, hi = lane >> 4;
    // per-lane twiddles: stage k (kf = kq) and stage j (jf = jp, jp + 4)
@@ -1834,7 +1864,7 @@ template <typename T>
 __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_backward_n4_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
-    T* __restrict__ staging, int64_t total_points, BatchStrides bs) {
+    T* __restrict__ staging, int64_t total_points, BatchStrides bs, Prefetch pre) {
    using T2 = typename Vec2<T>::type;
    const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
    translated += rhs * bs.translated;
@@ -1853,6 +1883,11 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_back
    const int cube = unit * kWarpCubes + warp;
    if (cube >= count) return;
    const DstDesc c = cubes[cube];
+   if (pre.ahead > 0 && rhs == 0 && lane == 0 && cube + pre.ahead < count) {
+      const DstDesc nc = cubes[cube + pre.ahead];
+      prefetch_l2(uti, pre.a_bytes, nc.uti_off * (int64_t)sizeof(T), (int64_t)nc.r * N3 * (int64_t)sizeof(T));
+      prefetch_l2(ucm, pre.b_bytes, nc.u_off * (int64_t)sizeof(T), (int64_t)nc.r * nc.p * (int64_t)sizeof(T));
+   }
    const int kq = lane & 3, jp = (lane >> 2) & 3;
    T2 W[Np], w2[Np], w3[N];
 #pragma unroll
@@ -2164,7 +2199,7 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
     const typename Vec2<T>::type* __restrict__ xsd, const int32_t* __restrict__ point_out,
     const int32_t* __restrict__ point_panel, const double* __restrict__ point_jump,
     const int32_t* __restrict__ phi_idx, const double* __restrict__ phi_scale, const double* __restrict__ x,
-    double* __restrict__ y, BatchStrides bs) {
+    double* __restrict__ y, BatchStrides bs, Prefetch pre) {
    using T2 = typename Vec2<T>::type;
    extern __shared__ __align__(16) char smem_raw[];
    const int rhs = blockIdx.x % bs.nrhs, unit = blockIdx.x / bs.nrhs;  // right-hand side fastest
@@ -2175,6 +2210,10 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
    const int leaf = unit * (blockDim.x >> 5) + warp;
    if (leaf >= n_leaf) return;
    const LeafDesc L = leaves[leaf];
+   if (pre.ahead > 0 && rhs == 0 && lane == 0 && leaf + pre.ahead < n_leaf) {
+      const LeafDesc nl = leaves[leaf + pre.ahead];
+      prefetch_l2(d, pre.c_bytes, nl.d_off * (int64_t)sizeof(T2), (int64_t)nl.nrows * nl.ncols * (int64_t)sizeof(T2));
+   }
    T2* xl = reinterpret_cast<T2*>(smem_raw) + (size_t)warp * xl_stride;
    for (int i = lane; i < L.ncols; i += 32) xl[i] = xsd[cols[L.col_off + i]];
    __syncwarp();
@@ -2400,10 +2439,29 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    raise_smem_limit(far_forward_kernel<T, far_rb<T>()>, src_b);
    raise_smem_limit(far_backward_kernel<T, far_rb<T>()>, dst_b);
    raise_smem_limit(near_kernel<T>, leaf_smem_max_);
+   {
+      int nb = 0;
+      FFTSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_forward_n4_kernel<T>, kWarpThreads, 0));
+      fwd_n4_wave_ = (int64_t)nb * sm_count_ * kWarpCubes;
+      FFTSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_backward_n4_kernel<T>, kWarpThreads, 0));
+      bwd_n4_wave_ = (int64_t)nb * sm_count_ * kWarpCubes;
+      FFTSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, near_kernel<T>, 32 * near_warps_, leaf_smem_max_));
+      near_wave_ = (int64_t)nb * sm_count_ * near_warps_;
+   }
    raise_smem_limit(far_forward_t_kernel<T>, std::max(src_smem_t_, 1));
    raise_smem_limit(far_backward_t_kernel<T>, std::max(dst_smem_t_, 1));
    build_chains();
    FFTSVD_CUDA(cudaDeviceSynchronize());
+}
+
+template <typename T>
+Prefetch DeviceOperator<T>::prefetch(int64_t wave, int nrhs, int64_t a_bytes, int64_t b_bytes, int64_t c_bytes) const {
+   Prefetch p;
+   p.ahead = wave / std::max(nrhs, 1);  // the blocks of one unit for all right-hand sides are adjacent
+   p.a_bytes = a_bytes;
+   p.b_bytes = b_bytes;
+   p.c_bytes = c_bytes;
+   return p;
 }
 
 template <typename T>
@@ -2480,7 +2538,9 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
                                                                          vt_.get(), pv_.get(), b.spectra, b.bs);
       else if (g.n == 4)
          far_forward_n4_kernel<T><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd, vt_.get(),
-                                                                     pv_.get(), b.spectra, b.bs);
+                                                                     pv_.get(), b.spectra, b.bs,
+                                                                     prefetch(fwd_n4_wave_, b.nrhs, vt_.bytes(),
+                                                                              pv_.bytes(), 0));
       else
          far_forward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(c, g.count, src_panels_.get(), b.xsd,
                                                                          vt_.get(), pv_.get(), b.spectra, b.bs);
@@ -2619,7 +2679,8 @@ void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cud
              c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
       else if (g.n == 4)
          far_backward_n4_kernel<T><<<grid, kWarpThreads, 0, stream>>>(
-             c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
+             c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs,
+             prefetch(bwd_n4_wave_, b.nrhs, uti_.bytes(), u_.bytes(), 0));
       else
          far_backward_warp_kernel<T, 5><<<grid, kWarpThreads, 0, stream>>>(
              c, g.count, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_, b.bs);
@@ -2751,7 +2812,7 @@ void DeviceOperator<T>::launch_near(const double* x, double* y, const Bufs& b, c
    near_kernel<T><<<(n_leaf_ + near_warps_ - 1) / near_warps_ * b.nrhs, 32 * near_warps_, leaf_smem_max_,
                     stream>>>(leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), b.xsd,
                               point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(),
-                              join_phi_scale_.get(), x, y, b.bs);
+                              join_phi_scale_.get(), x, y, b.bs, prefetch(near_wave_, b.nrhs, 0, 0, d_.bytes()));
    FFTSVD_CHECK_LAUNCH();
 }
 

@@ -287,6 +287,10 @@ class DeviceOperator {
    void launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream);
    bool warp_path(const LaunchGroup& g) const;
    int warp_min_cubes_ = kWarpMinCubes;
+   // resident warps of one wave of the 4^3 forward/backward and the near-field launches:
+   // how far ahead their warps prefetch operator blocks into L2
+   int64_t fwd_n4_wave_ = 0, bwd_n4_wave_ = 0, near_wave_ = 0;
+   struct Prefetch prefetch(int64_t wave, int nrhs, int64_t a_bytes, int64_t b_bytes, int64_t c_bytes) const;
    int sm_count_ = 148;
    int smem_optin_ = 0;  // largest dynamic shared memory a block may opt into
    int64_t spectra_elems_ = 1, translated_elems_ = 1;

@@ -422,7 +422,9 @@ void Tree::fill_near() {
          B.blocks.push_back(b);
       }
       std::vector<double> out((size_t)B.out_elems);
+      const auto e0 = std::chrono::steady_clock::now();
       (*eval)(kernel, *panels, B, out.data());
+      eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - e0).count();
 #pragma omp parallel for schedule(static)
       for (size_t li = 0; li < leaves.size(); li++) {
          if (off[li] < 0) continue;
@@ -608,7 +610,9 @@ void Tree::fill_bases() {
          }
       }
       pre.resize((size_t)B.out_elems);
+      const auto e0 = std::chrono::steady_clock::now();
       (*eval)(kernel, *panels, B, pre.data());
+      eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - e0).count();
    }
 #pragma omp parallel for schedule(dynamic, 1)
    for (size_t wi = 0; wi < work.size(); wi++) {
@@ -882,6 +886,7 @@ Timings build_tree(Tree& T, int max_panels) {
    tm.near_ms = ms(t1, t2);
    tm.pinv_t_ms = ms(t2, t3);
    tm.bases_ms = ms(t3, t4);
+   tm.integrals_ms = T.eval_ms;
    return tm;
 }
 
@@ -924,7 +929,9 @@ void host_setup(const fftsvd_problem& pr, HostOperator& H, const BatchEvaluator*
       T.eval = eval;
       H.tm[t] = build_tree(T, pr.max_panels_per_leaf);
       H.depth[t] = T.depth;
+      const auto f0 = std::chrono::steady_clock::now();
       T.flatten(H.flat[t]);
+      H.tm[t].flatten_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - f0).count();
       if (t == 1)  // interior self terms for the preconditioner (Cube.c:2349-2390)
          for (const auto& c : T.cubes) {
             if (!c.leaf || c.points.empty() || c.dcols.empty()) continue;
@@ -1050,6 +1057,18 @@ extern "C" int fftsvd_b200_host_operator_tree(const fftsvd_host_operator* op, in
 extern "C" int fftsvd_b200_host_operator_precond(const fftsvd_host_operator* op, fftsvd_precond_csc* out) {
    if (!op || !out) return FFTSVD_ERR_ARGUMENT;
    *out = op->h.precond;
+   return FFTSVD_OK;
+}
+
+extern "C" int fftsvd_b200_host_operator_timings(const fftsvd_host_operator* op, double* ms6) {
+   if (!op || !ms6) return FFTSVD_ERR_ARGUMENT;
+   const fftsvd::setup::Timings* t = op->h.tm;
+   ms6[0] = t[0].partition_ms + t[1].partition_ms;
+   ms6[1] = t[0].near_ms + t[1].near_ms;
+   ms6[2] = t[0].pinv_t_ms + t[1].pinv_t_ms;
+   ms6[3] = t[0].bases_ms + t[1].bases_ms;
+   ms6[4] = t[0].flatten_ms + t[1].flatten_ms;
+   ms6[5] = t[0].integrals_ms + t[1].integrals_ms;
    return FFTSVD_OK;
 }
 

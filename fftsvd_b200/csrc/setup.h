@@ -85,6 +85,7 @@ struct Tree {
    std::vector<std::vector<double>> pinv;    // per level, n^3 x 49
    std::vector<std::vector<double>> tops;    // per level, 343 slots x padded grid complex (re, im)
    const BatchEvaluator* eval = nullptr;     // near-field blocks and first-pass samples in batches
+   double eval_ms = 0.0;                     // wall time inside eval
 
    void build_cubes(int depth);
    void choose_depth(int max_panels);
@@ -103,7 +104,8 @@ struct Tree {
 };
 
 struct Timings {
-   double partition_ms = 0, near_ms = 0, pinv_t_ms = 0, bases_ms = 0;
+   double partition_ms = 0, near_ms = 0, pinv_t_ms = 0, bases_ms = 0, flatten_ms = 0;
+   double integrals_ms = 0;  // inside the evaluator (part of near_ms and bases_ms)
 };
 
 Timings build_tree(Tree& T, int max_panels);

@@ -127,8 +127,56 @@ void Preconditioner::apply(const double* r, double* z, cudaStream_t s, bool tran
 
 Surface::~Surface() {
    blk.reset();  // its cuBLAS handle is bound to the stream
+   release_step_graphs();
    if (st_host) cudaFreeHost(st_host);
+   if (hist_host) cudaFreeHost(hist_host);
    if (stream) cudaStreamDestroy(stream);
+}
+
+void Surface::release_step_graphs() {
+   for (auto& byprec : step_graphs)
+      for (StepGraph& g : byprec) {
+         if (g.exec) cudaGraphExecDestroy(g.exec);
+         g.exec = nullptr;
+         g.kernels = 0;
+      }
+}
+
+void Surface::step_apply(int precision) {
+   StepGraph& g = step_graphs[precision == FFTSVD_PREC_FP64 ? 1 : 0][transposed ? 1 : 0];
+   if (!g.exec) {
+      // capture on the surface's stream: the operator's chain and near-field streams fork
+      // from it and join back into it, so the graph holds the whole concurrent matvec
+      FFTSVD_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      cudaGraph_t graph = nullptr;
+      try {
+         apply(precision, krylov_in.get(), w.get());
+         pinv(w.get(), w.get());
+      } catch (...) {
+         cudaStreamEndCapture(stream, &graph);
+         if (graph) cudaGraphDestroy(graph);
+         throw;
+      }
+      FFTSVD_CUDA(cudaStreamEndCapture(stream, &graph));
+      // kernel nodes of the graph: the launch count is charged when the graph runs
+      size_t nodes = 0;
+      cudaError_t e = cudaGraphGetNodes(graph, nullptr, &nodes);
+      std::vector<cudaGraphNode_t> list(nodes);
+      if (e == cudaSuccess && nodes) e = cudaGraphGetNodes(graph, list.data(), &nodes);
+      long long kernels = 0;
+      for (size_t k = 0; e == cudaSuccess && k < nodes; k++) {
+         cudaGraphNodeType type;
+         e = cudaGraphNodeGetType(list[k], &type);
+         if (type == cudaGraphNodeTypeKernel) kernels++;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      FFTSVD_CUDA(e);
+      g.kernels = kernels;
+      g_kernel_launches.fetch_sub(kernels);  // the captured launches did not run
+   }
+   FFTSVD_CUDA(cudaGraphLaunch(g.exec, stream));
+   g_kernel_launches.fetch_add(g.kernels);
 }
 
 void Surface::ensure_capacity(int nvec) {
@@ -143,6 +191,10 @@ void Surface::ensure_capacity(int nvec) {
    h2.alloc(nvec);
    y.alloc(nvec);
    partial.alloc((size_t)nvec * nb);
+   hist.alloc(nvec);
+   if (hist_host) cudaFreeHost(hist_host);
+   hist_host = nullptr;
+   FFTSVD_CUDA(cudaMallocHost(&hist_host, sizeof(double2) * nvec));
    capacity = nvec;
 }
 
@@ -194,7 +246,8 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
    }
    double* Vp = V.get();
    const int64_t ldv = n;
-   scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, r.get(), nullptr, 1.0 / normr, Vp, 0, 0);
+   // v0 = r / |r|, also into the operator's input buffer
+   scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, r.get(), nullptr, 1.0 / normr, Vp, 0, 0, krylov_in.get());
    FFTSVD_CHECK_LAUNCH();
    FFTSVD_CUDA(cudaMemsetAsync(g.get(), 0, sizeof(double) * capacity, stream));
    FFTSVD_CUDA(cudaMemcpyAsync(g.get(), &normr, sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -203,14 +256,13 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
    st_host->flag = 0;
    FFTSVD_CUDA(cudaMemcpyAsync(st.get(), st_host, sizeof(GivensState), cudaMemcpyHostToDevice, stream));
 
-   int i = 0;
-   double resid = 1.0;
-   for (i = 0; i < maxit; i++) {
+   // Arnoldi step i (GMRES.c:470-503): w = P^-1 A v_i (one graph launch), CGS2 against
+   // v_0..v_i, the Givens update on the device, v_{i+1} = w / beta (also into the
+   // operator's input buffer for step i + 1).  The residual of every step lands in hist.
+   auto step = [&](int i) {
       const int nvec = i + 1;
-      const double* vi = Vp + (int64_t)i * ldv;
       double* vnext = Vp + (int64_t)(i + 1) * ldv;
-      apply(precision, vi, w.get());
-      pinv(w.get(), w.get());
+      step_apply(precision);
       // CGS2: h1 = V^T w, w -= V h1, h2 = V^T w, vnext = w - V h2 with its norm partials
       const size_t sh = sizeof(double) * nvec;
       dots_partial_kernel<<<dim3(nd, nvec), kVecThreads, 0, stream>>>(n, nvec, Vp, ldv, w.get(), partial.get(), 0, 0);
@@ -224,21 +276,53 @@ int Surface::gmres(int precision, const double* rhs, double* x, double tol, int 
                                                      normpart.get(), 0, 0, 0, 0);
       FFTSVD_CHECK_LAUNCH();
       givens_kernel<<<1, 256, givens_smem(i), stream>>>(i, capacity, H.get(), h1.get(), h2.get(), normpart.get(), nb,
-                                                        cs.get(), sn.get(), g.get(), st.get(), 0, 0, nullptr);
+                                                        cs.get(), sn.get(), g.get(), st.get(), 0, 0, nullptr,
+                                                        hist.get());
       FFTSVD_CHECK_LAUNCH();
-      scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext, 0, 0);
+      scale_kernel<<<ew_blocks, 256, 0, stream>>>(n, vnext, &st.get()->inv_beta, 0.0, vnext, 0, 0, krylov_in.get());
       FFTSVD_CHECK_LAUNCH();
-      FFTSVD_CUDA(cudaMemcpyAsync(st_host, st.get(), sizeof(GivensState), cudaMemcpyDeviceToHost, stream));
-      FFTSVD_CUDA(cudaStreamSynchronize(stream));
-      resid = st_host->residual;
-      if (st_host->flag == 2) {
-         *status = FFTSVD_ERR_NONFINITE;
-         break;
+   };
+
+   // Steps are issued in runs without waiting in between: the host reads the residual
+   // history only after each run.  A run is as long as the residual's recent rate of decrease
+   // predicts the solve to stay above tol (at most kMaxRun steps, one step near the end).
+   // Steps issued past the converged one add basis vectors and Hessenberg columns that the
+   // solution never uses: GMRES's least-squares problem of the first k steps does not
+   // depend on later ones.
+   constexpr int kMaxRun = 8;
+   int i = 0, last = -1;
+   double resid = 1.0;
+   while (i < maxit && last < 0) {
+      int run = 1;
+      if (i >= 4) {
+         const double r_now = hist_host[i - 1].x, r_past = hist_host[i - 4].x;
+         if (r_now > 0.0 && r_past > r_now) {
+            const double per_step = std::log(r_now / r_past) / 3.0;  // < 0
+            const double left = std::log(tol / r_now) / per_step;     // steps still predicted above tol
+            run = (int)std::max(1.0, std::min((double)kMaxRun, std::floor(0.6 * left)));
+         }
       }
-      if (resid < tol || st_host->flag == 1) break;
+      run = std::min(run, maxit - i);
+      for (int j = 0; j < run; j++) step(i + j);
+      FFTSVD_CUDA(cudaMemcpyAsync(hist_host + i, hist.get() + i, sizeof(double2) * run, cudaMemcpyDeviceToHost,
+                                  stream));
+      FFTSVD_CUDA(cudaStreamSynchronize(stream));
+      for (int j = 0; j < run; j++) {
+         const int flag = (int)hist_host[i + j].y;
+         resid = hist_host[i + j].x;
+         if (flag == 2) {
+            *status = FFTSVD_ERR_NONFINITE;
+            last = i + j;
+            break;
+         }
+         if (resid < tol || flag == 1) {
+            last = i + j;
+            break;
+         }
+      }
+      i += run;
    }
-   int last = i;
-   if (i == maxit) {
+   if (last < 0) {
       last = maxit - 1;
       *status = FFTSVD_ERR_NOT_CONVERGED;
    }
@@ -278,14 +362,16 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
       res = 1.0;
       if (!std::isfinite(bn)) status = FFTSVD_ERR_NONFINITE;
       else if (bn < tol) res = 0.0;
-      // Each inner solve targets an absolute preconditioned error of 0.3 tol ||P^-1 b||: the
-      // first one therefore runs to 0.3 tol, a correction to 0.3 tol / (current residual).
-      // The FP32 operator differs from the FP64 one by ~1e-7 relative, so one correction is
-      // rarely needed and the FP64 operator is applied once per refinement only.
+      // Each inner solve targets an absolute preconditioned error of kInnerTarget tol
+      // ||P^-1 b||: the first one therefore runs to kInnerTarget tol, a correction to
+      // kInnerTarget tol / (current residual).  The FP32 operator differs from the FP64 one
+      // by ~1e-7 relative, far below the remaining 1 - kInnerTarget of the tolerance, so
+      // one correction is rarely needed and the FP64 operator is applied once per
+      // refinement only.
       for (refinements = 0; status == FFTSVD_OK && res >= tol && refinements < 8; refinements++) {
          double inner_res = 0.0;
          int st2 = FFTSVD_OK;
-         const double inner_tol = std::min(0.1, std::max(0.3 * tol / res, 1e-13));
+         const double inner_tol = std::min(0.1, std::max(kInnerTarget * tol / res, 1e-13));
          iters += gmres(FFTSVD_PREC_FP32, t1.get(), xout.get(), inner_tol, maxit, &inner_res, &st2, false);
          if (st2 == FFTSVD_ERR_NONFINITE) { status = st2; break; }
          add_kernel<<<ew_blocks, 256, 0, stream>>>(n, xout.get(), x, 0);
@@ -339,6 +425,7 @@ void init_surface(Surface& S, int num_unknowns, int num_trees, const fftsvd_tree
    S.xin.alloc(num_unknowns);
    S.xout.alloc(num_unknowns);
    S.sold.alloc(num_unknowns);
+   S.krylov_in.alloc(num_unknowns);
    S.scal.alloc(8);
    S.normpart.alloc(nb);
    S.st.alloc(1);

@@ -19,6 +19,11 @@ namespace fftsvd {
 
 struct PanelGeometry;  // nbody.h
 
+// Share of the tolerance the FP32-operator inner solves of the mixed mode aim at (single
+// and lockstep-batch solves): the FP64 refinement residual then stays below the tolerance
+// by the FP32 operator's ~1e-7 relative error.
+constexpr double kInnerTarget = 0.8;
+
 struct Preconditioner {
    int nblocks = 0;
    DevBuf<int32_t> blk_ptr, blk_idx;
@@ -52,9 +57,23 @@ struct Surface {
    // GMRES workspace
    int capacity = 0;  // basis vectors
    DevBuf<double> V, H, cs, sn, g, h1, h2, partial, normpart, y;
-   DevBuf<double> w, r, t0, t1, t2, xin, xout, sold, scal;
+   DevBuf<double> w, r, t0, t1, t2, xin, xout, sold, scal, krylov_in;
    DevBuf<GivensState> st;
    GivensState* st_host = nullptr;
+   DevBuf<double2> hist;           // per Arnoldi step {residual, flag}
+   double2* hist_host = nullptr;   // pinned copy, capacity entries
+
+   // One Arnoldi step's operator application, krylov_in -> w = P^-1 A krylov_in, captured
+   // once per (operator precision, direction) as a CUDA graph: one launch replays the
+   // join, the concurrent grid-size chains and near field, the far-field add and the
+   // preconditioner.  Rebuilt after the translation tiles change.
+   struct StepGraph {
+      cudaGraphExec_t exec = nullptr;
+      long long kernels = 0;  // kernel nodes, for fftsvd_b200_launch_count
+   };
+   StepGraph step_graphs[2][2];   // [FP64 operator][transposed]
+   void step_apply(int precision);
+   void release_step_graphs();
 
    ~Surface();
    void ensure_capacity(int nvec);

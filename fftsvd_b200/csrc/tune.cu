@@ -64,12 +64,14 @@ void Surface::set_tile_limits(int max_groups, int max_src, int max_entries) {
    lim.max_entries = max_entries;
    TileSet fwd, adj;
    make_tiles(*tile_problems, lim, fwd, adj);
+   release_step_graphs();  // they hold the old tiles' buffers
    op32.set_tiles(fwd, adj);
    op64.set_tiles(fwd, adj);
 }
 
 void Surface::autotune(fftsvd_tune_info* info) {
    FFTSVD_REQUIRE(tile_problems != nullptr, "surface without translation problems");
+   release_step_graphs();  // they hold the current tiles' buffers
    std::vector<TileSet> fwd(kNumCandidates), adj(kNumCandidates);
    for (int c = 0; c < kNumCandidates; c++) make_tiles(*tile_problems, kCandidates[c], fwd[c], adj[c]);
    // timing input: zeros (the kernels' speed does not depend on the values)

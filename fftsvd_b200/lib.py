@@ -27,7 +27,8 @@ EXPORTED = [
     "fftsvd_b200_solve_device", "fftsvd_b200_set_geometry", "fftsvd_b200_rhs", "fftsvd_b200_rhs_device",
     "fftsvd_b200_reaction_potentials", "fftsvd_b200_reaction_potentials_device", "fftsvd_b200_energy",
     "fftsvd_b200_matvec_bytes", "fftsvd_b200_surface_stats", "fftsvd_b200_host_setup",
-    "fftsvd_b200_host_operator_tree", "fftsvd_b200_device_setup", "fftsvd_b200_host_setup_batched", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
+    "fftsvd_b200_host_operator_tree", "fftsvd_b200_device_setup", "fftsvd_b200_host_setup_batched",
+    "fftsvd_b200_host_operator_timings", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
     "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
     "fftsvd_b200_launch_count", "fftsvd_b200_device_alloc_count", "fftsvd_b200_reaction_potentials_noalloc",
     "solveSurfaceOperator", "generateRHS",
@@ -84,6 +85,7 @@ def load():
     lib.fftsvd_b200_host_setup.argtypes = [C.POINTER(Problem), C.POINTER(sp)]
     lib.fftsvd_b200_device_setup.argtypes = [C.POINTER(Problem), C.POINTER(sp)]
     lib.fftsvd_b200_host_setup_batched.argtypes = [C.POINTER(Problem), C.POINTER(sp)]
+    lib.fftsvd_b200_host_operator_timings.argtypes = [sp, _f64p]
     lib.fftsvd_b200_host_operator_tree.argtypes = [sp, C.c_int32, C.POINTER(TreeFlat)]
     lib.fftsvd_b200_host_operator_precond.argtypes = [sp, C.POINTER(PrecondCSC)]
     lib.fftsvd_b200_host_operator_free.argtypes = [sp]

@@ -355,11 +355,12 @@ def solve_many(surfaces, rhs_ptrs, sol_ptrs, precision="mixed", tol=1e-6, max_it
 
 
 def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per_leaf=32, grid_points=4,
-                  num_threads=0, integrals="host"):
+                  num_threads=0, integrals="host", timings=None):
     """Run only the setup: returns ([exterior tree, interior tree], preconditioner) as numpy.
     integrals: "host" (fftsvd_b200_host_setup), "device" (the panel integrals in batches
     on the current CUDA device, fftsvd_b200_device_setup) or "batched" (the device path's
-    batches evaluated on the host, fftsvd_b200_host_setup_batched)."""
+    batches evaluated on the host, fftsvd_b200_host_setup_batched).  A dict passed as
+    timings receives the wall milliseconds of the setup stages."""
     lib = load()
     vv = f64(vertices)
     zero3, zero1 = np.zeros(3), np.zeros(1)
@@ -370,6 +371,10 @@ def host_operator(vertices, eps_in, eps_out, kappa, svd_tol=1e-5, max_panels_per
              "batched": lib.fftsvd_b200_host_setup_batched}[integrals]
     check(setup(C.byref(p), C.byref(h)))
     try:
+        if timings is not None:
+            ms = np.zeros(6)
+            check(lib.fftsvd_b200_host_operator_timings(h, ptr(ms)))
+            timings.update(zip(["partition", "near", "pinv_t", "bases", "flatten", "integrals"], ms.tolist()))
         trees = []
         for t in range(2):
             tf = _abi.TreeFlat()

@@ -147,7 +147,10 @@ typedef struct {
    int32_t depth[2];              /* partitioning levels of the exterior and interior trees */
    int32_t num_leaves[2];
    int32_t num_cubes[2];          /* cubes with a non-empty interaction list */
-   double setup_ms[4];            /* partition + lists, near field, pinv + translation operators, bases */
+   double setup_ms[8];            /* wall ms of the setup stages: [0] partition + lists, [1] near field,
+                                     [2] pinv + translation operators, [3] bases, [4] flattening,
+                                     [5] panel integrals in batches (device; inside [1] and [3]),
+                                     [6] device layout and upload, [7] the whole surface creation */
    double device_bytes;           /* resident operator bytes, both precisions */
    double matvec_bytes_fp32;      /* algorithmic bytes of one matvec, FP32 operator */
    double matvec_bytes_fp64;      /* algorithmic bytes of one matvec, FP64 operator */
@@ -191,6 +194,9 @@ int fftsvd_b200_device_setup(const fftsvd_problem* problem, fftsvd_host_operator
    that needs no GPU). */
 int fftsvd_b200_host_setup_batched(const fftsvd_problem* problem, fftsvd_host_operator** out);
 int fftsvd_b200_host_operator_precond(const fftsvd_host_operator* op, fftsvd_precond_csc* out);
+/* Wall milliseconds of the setup stages, as the first six entries of
+   fftsvd_surface_stats.setup_ms. */
+int fftsvd_b200_host_operator_timings(const fftsvd_host_operator* op, double* ms6);
 void fftsvd_b200_host_operator_free(fftsvd_host_operator* op);
 
 /* Upload an operator given in flat form (one tree per region). */
