@@ -388,6 +388,25 @@ int fftsvd_b200_matvec_batch_device(fftsvd_surface* s, int32_t precision, int32_
    });
 }
 
+int fftsvd_b200_matvec_batch_tensor_device(fftsvd_surface* s, int32_t nrhs, const double* x, double* y) {
+   if (!s || !x || !y || nrhs <= 0 || nrhs % kBatchGroup != 0) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      Surface& S = s->s;
+      if (!S.op32.tensor_near_available())
+         throw Error(FFTSVD_ERR_UNSUPPORTED, "a leaf has more rows than the tensor-core near field takes (256)");
+      S.op32.set_tensor_near(true);
+      try {
+         S.apply_batch(FFTSVD_PREC_FP32, x, y, nrhs);
+      } catch (...) {
+         S.op32.set_tensor_near(false);
+         throw;
+      }
+      S.op32.set_tensor_near(false);
+      FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+      if (S.op32.tensor_status(true)) throw Error(FFTSVD_ERR_TIMEOUT, "a tensor-core near-field wait gave up");
+   });
+}
+
 }  // extern "C"
 
 // ---- many surfaces at once

@@ -383,6 +383,12 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
    const bool mixed = precision == FFTSVD_PREC_MIXED;
    const int inner = mixed ? FFTSVD_PREC_FP32 : precision, outer = mixed ? FFTSVD_PREC_FP64 : precision;
    if (!blk) blk = std::make_unique<BlockWorkspace>();
+   // the FP32 multi-vector matvecs of the block solve take the tensor-core near field
+   struct TensorNear {
+      DeviceOperator<float>& op;
+      explicit TensorNear(DeviceOperator<float>& o) : op(o) { op.set_tensor_near(true); }
+      ~TensorNear() { op.set_tensor_near(false); }
+   } tensor_near(op32);
    const int ew_blocks = std::max(1, std::min((n + 255) / 256, 148 * 8));
    const int nb = vec_blocks(n);
    std::vector<int> iters(k, 0), refinements(k, 0), status(k, FFTSVD_OK);
@@ -525,6 +531,8 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
    }
    const auto clock_end = std::chrono::steady_clock::now();
    const double ms = std::chrono::duration<double, std::milli>(clock_end - clock_start).count();
+   if (op32.tensor_status(true))
+      throw Error(FFTSVD_ERR_TIMEOUT, "a tensor-core near-field wait gave up (results discarded)");
    int first_bad = FFTSVD_OK;
    for (int c = 0; c < k; c++) {
       if (first_bad == FFTSVD_OK && status[c] != FFTSVD_OK) first_bad = status[c];

@@ -20,6 +20,7 @@
 #include <array>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <numeric>
 #include <string>
 
@@ -2439,6 +2440,17 @@ void DeviceOperator<T>::upload(const OperatorLayout& L) {
    raise_smem_limit(far_forward_kernel<T, far_rb<T>()>, src_b);
    raise_smem_limit(far_backward_kernel<T, far_rb<T>()>, dst_b);
    raise_smem_limit(near_kernel<T>, leaf_smem_max_);
+   near_np_max_ = 0;
+   if (std::is_same<T, float>::value) {
+      int rmax = 8;
+      for (const auto& l : L.leaves) rmax = std::max(rmax, (l.nrows + 7) & ~7);
+      if (rmax <= 256 && near_tc_smem(rmax) <= optin) {
+         near_np_max_ = rmax;
+         prepare_near_tc(rmax);
+         tc_status_.alloc(1);
+         tc_status_.zero();
+      }
+   }
    {
       int nb = 0;
       FFTSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_forward_n4_kernel<T>, kWarpThreads, 0));
@@ -2807,8 +2819,28 @@ void DeviceOperator<T>::apply_bufs(const double* x, double* y, const Bufs& b, cu
 }
 
 template <typename T>
+int DeviceOperator<T>::tensor_status(bool reset) {
+   if (!tc_status_.get()) return 0;
+   int v = 0;
+   FFTSVD_CUDA(cudaMemcpy(&v, tc_status_.get(), sizeof(int), cudaMemcpyDeviceToHost));
+   if (reset && v) tc_status_.zero();
+   return v;
+}
+
+template <typename T>
 void DeviceOperator<T>::launch_near(const double* x, double* y, const Bufs& b, cudaStream_t stream) {
    if (n_leaf_ == 0) return;
+   if constexpr (std::is_same<T, float>::value) {
+      if (tensor_near_ && b.nrhs >= kBatchGroup && near_np_max_ > 0) {
+         const int64_t ld = (b.nrhs + 31) / 32 * 32;
+         if (xsd_t_.size() < (size_t)(total_panels_ * ld)) xsd_t_.alloc((size_t)(total_panels_ * ld));
+         launch_near_tc(leaves_.get(), n_leaf_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), b.xsd, b.bs.panels,
+                        (int)total_panels_, xsd_t_.get(), ld, point_out_.get(), point_panel_.get(), point_jump_.get(),
+                        join_phi_idx_.get(), join_phi_scale_.get(), x, y, b.nrhs, b.bs.n, near_np_max_,
+                        tc_status_.get(), stream);
+         return;
+      }
+   }
    near_kernel<T><<<(n_leaf_ + near_warps_ - 1) / near_warps_ * b.nrhs, 32 * near_warps_, leaf_smem_max_,
                     stream>>>(leaves_.get(), n_leaf_, near_stride_, leaf_rows_.get(), leaf_cols_.get(), d_.get(), b.xsd,
                               point_out_.get(), point_panel_.get(), point_jump_.get(), join_phi_idx_.get(),

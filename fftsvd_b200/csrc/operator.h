@@ -229,6 +229,19 @@ struct OperatorLayout {
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
                             const fftsvd_region_map* maps);
 
+// Near field of a multi-vector FP32 matvec on the tensor cores (near_tc.cu): the joined
+// panel values are transposed to [panel][rhs] (xsd_t, ld >= nrhs) and each leaf's block
+// product runs as kind::tf32 MMAs with three-product splitting, 128 right-hand sides per
+// CTA.  np_max: the largest leaf row count padded to 8 (at most 256).  A bounded wait that
+// gives up sets *status.
+int near_tc_smem(int np_max);
+void prepare_near_tc(int np_max);
+void launch_near_tc(const LeafDesc* leaves, int n_leaf, const int32_t* rows, const int32_t* cols, const float2* d,
+                    const float2* xsd, int64_t panels, int np_panels, float2* xsd_t, int64_t ld,
+                    const int32_t* point_out, const int32_t* point_panel, const double* point_jump,
+                    const int32_t* phi_idx, const double* phi_scale, const double* x, double* y, int nrhs, int64_t ldn,
+                    int np_max, int* status, cudaStream_t stream);
+
 template <typename T>
 class DeviceOperator {
  public:
@@ -252,6 +265,13 @@ class DeviceOperator {
    // y = A^T x (the transposed operator), x and y device vectors of num_unknowns doubles.
    // Column sums are accumulated with FP64 atomics: not bitwise reproducible run to run.
    void apply_transpose(const double* x, double* y, cudaStream_t stream);
+   // Multi-vector FP32 matvecs take the tensor-core near field (near_tc.cu) while this is
+   // set; the columns then differ from single matvecs at FP32 rounding level (the block
+   // solve sets it; the lockstep batch keeps the single-matvec arithmetic).
+   void set_tensor_near(bool on) { tensor_near_ = on; }
+   bool tensor_near_available() const { return near_np_max_ > 0; }
+   // nonzero when a tensor-core near-field wait gave up since the last reset
+   int tensor_status(bool reset);
    // per-stage events for timing (recorded when enabled)
    void enable_timing(bool on);
    // milliseconds of [join, far_forward, translate, far_backward, near] of the last timed apply
@@ -290,6 +310,11 @@ class DeviceOperator {
    // resident warps of one wave of the 4^3 forward/backward and the near-field launches:
    // how far ahead their warps prefetch operator blocks into L2
    int64_t fwd_n4_wave_ = 0, bwd_n4_wave_ = 0, near_wave_ = 0;
+   bool tensor_near_ = false;
+   int near_np_max_ = 0;               // 0: some leaf has more than 256 rows (no tensor path)
+   DevBuf<float2> xsd_t_;              // joined values [panel][rhs] of the tensor-core near field
+   int64_t xsd_t_ld_ = 0;
+   DevBuf<int> tc_status_;
    struct Prefetch prefetch(int64_t wave, int nrhs, int64_t a_bytes, int64_t b_bytes, int64_t c_bytes) const;
    int sm_count_ = 148;
    int smem_optin_ = 0;  // largest dynamic shared memory a block may opt into

@@ -33,7 +33,8 @@ EXPORTED = [
     "fftsvd_b200_launch_count", "fftsvd_b200_device_alloc_count", "fftsvd_b200_reaction_potentials_noalloc",
     "solveSurfaceOperator", "generateRHS",
     "collectPotentials",
-    "fftsvd_b200_matvec_batch_device", "fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch",
+    "fftsvd_b200_matvec_batch_device", "fftsvd_b200_matvec_batch_tensor_device", "fftsvd_b200_solve_batch_device",
+    "fftsvd_b200_solve_batch",
     "fftsvd_b200_rhs_groups_device", "fftsvd_b200_group_energies_device",
     "fftsvd_b200_set_charges", "fftsvd_b200_matvec_transpose", "fftsvd_b200_matvec_transpose_device",
     "fftsvd_b200_adjoint", "fftsvd_b200_solve_many", "fftsvd_b200_surface_autotune",
@@ -97,6 +98,7 @@ def load():
     lib.fftsvd_b200_device_alloc_count.restype = C.c_longlong
     lib.fftsvd_b200_reaction_potentials_noalloc.argtypes = [sp, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_matvec_batch_device.argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.fftsvd_b200_matvec_batch_tensor_device.argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p]
     for name in ("fftsvd_b200_solve_batch_device", "fftsvd_b200_solve_batch", "fftsvd_b200_solve_block_device",
                  "fftsvd_b200_solve_block"):
         getattr(lib, name).argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,

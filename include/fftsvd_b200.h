@@ -337,6 +337,12 @@ int fftsvd_b200_adjoint(fftsvd_surface* s, int32_t precision, double tol, int32_
    Like that call it is issued on the surface's stream and returns before it
    finishes (when nrhs is not a multiple of 8 it waits for a padded copy). */
 int fftsvd_b200_matvec_batch_device(fftsvd_surface* s, int32_t precision, int32_t nrhs, const double* x, double* y);
+/* Y = A X with the FP32 operator for nrhs vectors (a multiple of 8), device pointers, the
+   near field on the tensor cores: per leaf and 128 right-hand sides one kind::tf32 GEMM with
+   three-product splitting (FP32-level accuracy; the columns differ from
+   fftsvd_b200_matvec_batch_device at FP32 rounding level).  The block solve's inner
+   matvecs take this path.  Synchronous.  No counterpart in the reference. */
+int fftsvd_b200_matvec_batch_tensor_device(fftsvd_surface* s, int32_t nrhs, const double* x, double* y);
 /* Solves A x_c = rhs_c for nrhs columns at once: lockstep GMRES in which every
    column keeps its own Krylov basis, Hessenberg matrix, Givens rotations and
    stopping test (as fftsvd_b200_solve), over the multi-vector matvec.  For
