@@ -388,6 +388,8 @@ int Surface::solve(int precision, const double* rhs, double* x, double tol, int 
       throw Error(FFTSVD_ERR_ARGUMENT, "unknown precision mode");
    }
    FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   if (op32.tensor_status(true) | op64.tensor_status(true))
+      throw Error(FFTSVD_ERR_TIMEOUT, "a bounded device wait of the matvec gave up (results discarded)");
    const auto clock_end = std::chrono::steady_clock::now();
    if (info) {
       info->iterations = iters;
@@ -480,6 +482,8 @@ int fftsvd_b200_matvec(fftsvd_surface* s, int32_t precision, const double* x, do
       S.apply(precision == FFTSVD_PREC_FP64 ? FFTSVD_PREC_FP64 : FFTSVD_PREC_FP32, S.xin.get(), S.w.get());
       FFTSVD_CUDA(cudaMemcpyAsync(y, S.w.get(), sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
       FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
+      if (S.op32.tensor_status(true) | S.op64.tensor_status(true))
+         throw Error(FFTSVD_ERR_TIMEOUT, "a bounded device wait of the matvec gave up (results discarded)");
    });
 }
 
