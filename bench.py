@@ -271,6 +271,16 @@ def _setup_stats(s):
     return st
 
 
+def smem_roofline(smem_bytes, ms, sm_count, sm_mhz):
+    """The translation stage against the shared-memory bandwidth of the SMs."""
+    mhz = sm_mhz or 1965.0
+    peak = sm_count * 128.0 * mhz * 1e6 / 1e9  # GB/s
+    ach = smem_bytes / (ms * 1e6) if ms > 0 else None
+    return {"kernel": "translate", "bytes_per_launch": smem_bytes, "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak if ach else None,
+            "peak_kind": f"nominal: 128 bytes per clock per SM x {sm_count} SMs at {mhz:.0f} MHz"}
+
+
 def _ref64_errors(g, e_mixed, e64):
     if g is None:
         return None
@@ -439,6 +449,11 @@ def run_ours(args, cfg, ws, rank, local):
     peak, peak_kind = hbm_peak()
     dom = max(kernels, key=lambda k: prof["fp32"][k]["ms"])
     ach = prof["fp32"][dom]["gbs"]
+    # the translation's own bound: shared-memory bytes it moves over the SMs' shared-memory
+    # bandwidth (128 bytes per clock per SM, at the SM clock sampled during the timed region)
+    smem_b = C.c_double()
+    lib.fftsvd_b200_translate_smem_bytes(s._h, _abi.PREC_FP32, C.byref(smem_b))
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     # DRAM traffic of that stage per matvec, from the ncu capture summarised in profiles/
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "translate_dram_blob_l6.md")
@@ -475,7 +490,9 @@ def run_ours(args, cfg, ws, rank, local):
                        "depth": list(st.depth), "leaves": list(st.num_leaves), "far_cubes": list(st.num_cubes)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak if ach else None, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": prof["fp32"][dom]["bytes"]},
+                         "algorithmic_bytes_per_launch": prof["fp32"][dom]["bytes"],
+                         "smem": smem_roofline(smem_b.value, prof["fp32"]["translate"]["ms"], sm_count,
+                                               clk.summary().get("sm_mhz"))},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
             "gpu_launches": int(launches),

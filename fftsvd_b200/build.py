@@ -63,7 +63,7 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr):
-            cmd = [nvcc, *ARCH, "-lineinfo", *opt, "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+            cmd = [nvcc, *ARCH, "-lineinfo", *opt, "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr",
                    "-ccbin", cxx, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")

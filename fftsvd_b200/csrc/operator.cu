@@ -20,6 +20,8 @@
 #include <array>
 #include <map>
 #include <mutex>
+#include <unordered_map>
+#include <exception>
 #include <type_traits>
 #include <numeric>
 #include <string>
@@ -83,7 +85,8 @@ bool make_group(const TileProblem& P, const std::vector<int>& ids, size_t first,
       morton_decode(P.morton[ids[i]], c);
       pos.push_back({c[0], c[1], c[2]});
    }
-   std::map<int64_t, int> where;
+   std::unordered_map<int64_t, int> where;
+   where.reserve(256);
    std::vector<std::array<int, 3>> v0;  // offset of member 0 to each source
    for (size_t m = 0; m < pos.size(); m++) {
       const int o = ids[first + m];
@@ -163,7 +166,8 @@ static void build_tiles(const TileProblem& P, const TileLimits& lim, TileSet& S)
          tile.mem_off = (int64_t)S.tile_dst.size();
          tile.src_off = (int64_t)S.tile_src.size();
          tile.ent_off = (int64_t)S.tile_entries.size();
-         std::map<int64_t, int> halo;
+         std::unordered_map<int64_t, int> halo;
+         halo.reserve(2 * kTileMaxSrc);
          std::vector<int> tg;
          while (pos < groups.size()) {
             const MemberGroup& G = groups[pos];
@@ -281,10 +285,25 @@ void make_tiles(const TileProblems& P, const TileLimits& lim, TileSet& fwd, Tile
                   "tile limits out of range");
    fwd = TileSet();
    adj = TileSet();
-   build_tiles(P.fwd, lim, fwd);
-   build_tiles(P.adj, lim, adj);
-   check_tiles(fwd, P.nt, P.spectra_elems, P.translated_elems);  // spectra -> translated
-   check_tiles(adj, P.nt, P.translated_elems, P.spectra_elems);  // transposed: translated -> spectra
+   // the two directions are independent: built side by side (an exception in either is
+   // carried out of the parallel region and rethrown here)
+   std::exception_ptr err[2];
+#pragma omp parallel for num_threads(2) schedule(static, 1)
+   for (int d = 0; d < 2; d++) {
+      try {
+         if (d == 0) {
+            build_tiles(P.fwd, lim, fwd);
+            check_tiles(fwd, P.nt, P.spectra_elems, P.translated_elems);  // spectra -> translated
+         } else {
+            build_tiles(P.adj, lim, adj);
+            check_tiles(adj, P.nt, P.translated_elems, P.spectra_elems);  // transposed: translated -> spectra
+         }
+      } catch (...) {
+         err[d] = std::current_exception();
+      }
+   }
+   for (auto& e : err)
+      if (e) std::rethrow_exception(e);
 }
 
 OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_flat* trees,
@@ -354,8 +373,13 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          }
       }
 
-      // ---- near field
+      // ---- near field: a serial pass checks every leaf and places it, then the rows,
+      // columns and {D_single, D_double} pairs are filled in parallel
       std::vector<char> covered(T.num_points, 0);
+      std::vector<int> near_leaf;  // leaves with rows, in order
+      const size_t lr0 = L.leaf_rows.size(), lc0 = L.leaf_cols.size(), ld0 = L.leaves.size();
+      const size_t dp0 = L.d_pairs.size();
+      size_t nrows_all = 0, ncols_all = 0, npairs_all = 0;
       for (int l = 0; l < T.num_leaves; l++) {
          const int r0 = T.leaf_row_ptr[l], r1 = T.leaf_row_ptr[l + 1];
          const int c0 = T.leaf_col_ptr[l], c1 = T.leaf_col_ptr[l + 1];
@@ -363,35 +387,52 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          FFTSVD_REQUIRE(nr >= 0 && nc >= 0, "bad leaf extents");
          if (nr == 0) continue;
          FFTSVD_REQUIRE(T.leaf_d_ptr[l + 1] - T.leaf_d_ptr[l] == (int64_t)nr * nc, "leaf D size mismatch");
-         LeafDesc d;
-         d.row_off = (int32_t)L.leaf_rows.size();
-         d.nrows = nr;
-         d.col_off = (int32_t)L.leaf_cols.size();
-         d.ncols = ncp;
-         d.d_off = (int64_t)(L.d_pairs.size() / 2);
          for (int r = r0; r < r1; r++) {
-            int p = T.leaf_rows[r];
-            FFTSVD_REQUIRE(p >= 0 && p < T.num_points, "leaf row out of range");
-            FFTSVD_REQUIRE(!covered[p], "point in two leaves");
-            covered[p] = 1;
-            L.leaf_rows.push_back((int32_t)(qo + p));
+            const int pt = T.leaf_rows[r];
+            FFTSVD_REQUIRE(pt >= 0 && pt < T.num_points, "leaf row out of range");
+            FFTSVD_REQUIRE(!covered[pt], "point in two leaves");
+            covered[pt] = 1;
          }
-         for (int c = c0; c < c1; c++) {
-            int k = T.leaf_cols[c];
-            FFTSVD_REQUIRE(k >= 0 && k < T.num_panels, "leaf column out of range");
-            L.leaf_cols.push_back((int32_t)(po + k));
-         }
-         for (int c = nc; c < ncp; c++) L.leaf_cols.push_back(zero_slot);
-         const int64_t db = T.leaf_d_ptr[l];
-         for (int r = 0; r < nr; r++) {
-            for (int c = 0; c < nc; c++) {
-               L.d_pairs.push_back(T.d_single[db + (int64_t)r * nc + c]);
-               L.d_pairs.push_back(T.d_double[db + (int64_t)r * nc + c]);
-            }
-            for (int c = nc; c < ncp; c++) { L.d_pairs.push_back(0.0); L.d_pairs.push_back(0.0); }
-         }
+         for (int c = c0; c < c1; c++)
+            FFTSVD_REQUIRE(T.leaf_cols[c] >= 0 && T.leaf_cols[c] < T.num_panels, "leaf column out of range");
+         LeafDesc d;
+         d.row_off = (int32_t)(lr0 + nrows_all);
+         d.nrows = nr;
+         d.col_off = (int32_t)(lc0 + ncols_all);
+         d.ncols = ncp;
+         d.d_off = (int64_t)((dp0 / 2) + npairs_all);
+         nrows_all += nr;
+         ncols_all += ncp;
+         npairs_all += (size_t)nr * ncp;
          L.operator_elems += 2LL * nr * nc;
          L.leaves.push_back(d);
+         near_leaf.push_back(l);
+      }
+      L.leaf_rows.resize(lr0 + nrows_all);
+      L.leaf_cols.resize(lc0 + ncols_all);
+      L.d_pairs.resize(dp0 + 2 * npairs_all);
+      const int nleaf_here = (int)near_leaf.size();
+#pragma omp parallel for schedule(dynamic, 16)
+      for (int i = 0; i < nleaf_here; i++) {
+         const int l = near_leaf[i];
+         const LeafDesc& d = L.leaves[ld0 + i];
+         const int r0 = T.leaf_row_ptr[l], c0 = T.leaf_col_ptr[l];
+         const int nr = d.nrows, nc = T.leaf_col_ptr[l + 1] - c0, ncp = d.ncols;
+         for (int r = 0; r < nr; r++) L.leaf_rows[d.row_off + r] = (int32_t)(qo + T.leaf_rows[r0 + r]);
+         for (int c = 0; c < nc; c++) L.leaf_cols[d.col_off + c] = (int32_t)(po + T.leaf_cols[c0 + c]);
+         for (int c = nc; c < ncp; c++) L.leaf_cols[d.col_off + c] = zero_slot;
+         const int64_t db = T.leaf_d_ptr[l];
+         double* out = &L.d_pairs[2 * (size_t)d.d_off];
+         for (int r = 0; r < nr; r++) {
+            for (int c = 0; c < nc; c++) {
+               *out++ = T.d_single[db + (int64_t)r * nc + c];
+               *out++ = T.d_double[db + (int64_t)r * nc + c];
+            }
+            for (int c = nc; c < ncp; c++) {
+               *out++ = 0.0;
+               *out++ = 0.0;
+            }
+         }
       }
       // points of no leaf still receive their far field and jump term
       std::vector<int32_t> rest;
@@ -418,6 +459,11 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          FFTSVD_REQUIRE(nl >= 2 && nl <= 12, "grid size out of range");
          tlev[l + 1] = tlev[l] + 343LL * pad16(Npl * Npl * nl);
       }
+      // source cubes: a serial pass checks and places them, the panel lists, VT and the
+      // transposed {PV_single, PV_double} pairs are copied in parallel
+      std::vector<int> src_cube;  // parallel to the SrcDesc appended for this tree
+      const size_t s0 = L.src.size(), sp0 = L.src_panels.size(), vt0 = L.vt.size(), pv0 = L.pv_pairs.size();
+      size_t sp_all = 0, vt_all = 0, pv_all = 0;
       for (int c = 0; c < T.num_cubes; c++) {
          const int lvl = T.cube_level[c];
          FFTSVD_REQUIRE(lvl >= 0 && lvl < T.depth, "cube level out of range");
@@ -431,42 +477,62 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          FFTSVD_REQUIRE(T.cube_vt_ptr[c + 1] - T.cube_vt_ptr[c] == (int64_t)r * m, "VT size mismatch");
          FFTSVD_REQUIRE(T.cube_pv_ptr[c + 1] - T.cube_pv_ptr[c] == (int64_t)r * n3, "PV size mismatch");
          FFTSVD_REQUIRE(r <= 1024, "row rank too large");
-         SrcDesc s;
-         s.n = n; s.m = m; s.r = r;
-         s.panel_off = (int32_t)L.src_panels.size();
-         s.vt_off = (int64_t)L.vt.size();
-         s.pv_off = (int64_t)(L.pv_pairs.size() / 2);
-         s.spec_off = L.spectra_elems;
+         for (int i = T.cube_panel_ptr[c]; i < T.cube_panel_ptr[c + 1]; i++)
+            FFTSVD_REQUIRE(T.cube_panels[i] >= 0 && T.cube_panels[i] < T.num_panels, "cube panel out of range");
+         SrcDesc sd;
+         sd.n = n; sd.m = m; sd.r = r;
+         sd.panel_off = (int32_t)(sp0 + sp_all);
+         sd.vt_off = (int64_t)(vt0 + vt_all);
+         sd.pv_off = (int64_t)((pv0 / 2) + pv_all / 2);
+         sd.spec_off = L.spectra_elems;
          spec_of_cube[c] = L.spectra_elems;
          L.spectra_elems += pad16(pg);
-         for (int i = T.cube_panel_ptr[c]; i < T.cube_panel_ptr[c + 1]; i++) {
-            FFTSVD_REQUIRE(T.cube_panels[i] >= 0 && T.cube_panels[i] < T.num_panels, "cube panel out of range");
-            L.src_panels.push_back((int32_t)(po + T.cube_panels[i]));
-         }
-         const int64_t vb = T.cube_vt_ptr[c];
-         L.vt.insert(L.vt.end(), T.vt + vb, T.vt + vb + (int64_t)r * m);
-         const int64_t pb = T.cube_pv_ptr[c];
-         for (int j = 0; j < r; j++)
-            for (int p = 0; p < n3; p++) {
-               L.pv_pairs.push_back(T.pv_single[pb + (int64_t)p * r + j]);
-               L.pv_pairs.push_back(T.pv_double[pb + (int64_t)p * r + j]);
-            }
+         sp_all += m;
+         vt_all += (size_t)r * m;
+         pv_all += 2 * (size_t)r * n3;
          L.operator_elems += (int64_t)r * m + 2LL * r * n3;
          const int ch = std::min(m, 1024);
          const int H = n;
          int need = 2 * ch + 2 * r + n3 + 2 * Np + 2 * (n * n * H) + 2 * (n * Np * H) + 16;
          L.max_src_smem_elems = std::max(L.max_src_smem_elems, need);
-         s.level = lvl;
-         s.pad = 0;
-         L.src.push_back(s);
+         sd.level = lvl;
+         sd.pad = 0;
+         L.src.push_back(sd);
+         src_cube.push_back(c);
          {
             const int32_t* ci = &T.cube_index[3 * c];
             uint64_t code = 0;  // Morton order of the cube coordinates
-            for (int b = 0; b < 21; b++)
-               for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> b) & 1) << (3 * b + k);
+            for (int bb = 0; bb < 21; bb++)
+               for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> bb) & 1) << (3 * bb + k);
             src_extra.push_back({t * 64 + lvl, code, tlev[lvl], pad16(pg)});
          }
       }
+      L.src_panels.resize(sp0 + sp_all);
+      L.vt.resize(vt0 + vt_all);
+      L.pv_pairs.resize(pv0 + pv_all);
+      const int nsrc_here = (int)src_cube.size();
+#pragma omp parallel for schedule(dynamic, 16)
+      for (int i = 0; i < nsrc_here; i++) {
+         const int c = src_cube[i];
+         const SrcDesc& sd = L.src[s0 + i];
+         const int m = sd.m, r = sd.r, n3 = sd.n * sd.n * sd.n;
+         for (int k = 0; k < m; k++) L.src_panels[sd.panel_off + k] = (int32_t)(po + T.cube_panels[T.cube_panel_ptr[c] + k]);
+         std::copy(T.vt + T.cube_vt_ptr[c], T.vt + T.cube_vt_ptr[c] + (int64_t)r * m, L.vt.begin() + sd.vt_off);
+         const int64_t pb = T.cube_pv_ptr[c];
+         double* out = &L.pv_pairs[2 * (size_t)sd.pv_off];
+         for (int j = 0; j < r; j++)
+            for (int q = 0; q < n3; q++) {
+               *out++ = T.pv_single[pb + (int64_t)q * r + j];
+               *out++ = T.pv_double[pb + (int64_t)q * r + j];
+            }
+      }
+      // destination cubes: a serial pass checks them, counts their interactions with
+      // source spectra and places them, then points, UTI, the transposed U and the
+      // interaction pairs are filled in parallel
+      std::vector<int> dst_cube;
+      const size_t d0 = L.dst.size(), dp_0 = L.dst_points.size(), uti0 = L.uti.size(), u0 = L.u_cm.size();
+      const size_t ip0 = L.inter_pairs.size();
+      size_t dp_all = 0, uti_all = 0, u_all = 0, ip_all = 0;
       for (int c = 0; c < T.num_cubes; c++) {
          const int lvl = T.cube_level[c];
          const int n = T.grid[lvl];
@@ -477,56 +543,77 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
          FFTSVD_REQUIRE(T.cube_uti_ptr[c + 1] - T.cube_uti_ptr[c] == (int64_t)r * n3, "UTI size mismatch");
          FFTSVD_REQUIRE(T.cube_u_ptr[c + 1] - T.cube_u_ptr[c] == (int64_t)r * p, "U size mismatch");
          FFTSVD_REQUIRE(r <= 1024, "column rank too large");
-         DstDesc d;
-         d.n = n; d.p = p; d.r = r;
-         d.point_off = (int32_t)L.dst_points.size();
-         d.uti_off = (int64_t)L.uti.size();
-         d.u_off = (int64_t)L.u_cm.size();
-         d.inter_off = (int32_t)(L.inter_pairs.size() / 2);
-         d.stage = lvl;
-         d.pad = 0;
-         for (int i = T.cube_point_ptr[c]; i < T.cube_point_ptr[c + 1]; i++) {
+         for (int i = T.cube_point_ptr[c]; i < T.cube_point_ptr[c + 1]; i++)
             FFTSVD_REQUIRE(T.cube_points[i] >= 0 && T.cube_points[i] < T.num_points, "cube point out of range");
-            L.dst_points.push_back((int32_t)(qo + T.cube_points[i]));
-         }
-         const int64_t ub = T.cube_uti_ptr[c];
-         L.uti.insert(L.uti.end(), T.uti + ub, T.uti + ub + (int64_t)r * n3);
-         const int64_t uub = T.cube_u_ptr[c];
-         for (int j = 0; j < r; j++)
-            for (int q = 0; q < p; q++) L.u_cm.push_back(T.u[uub + (int64_t)q * r + j]);
-         L.operator_elems += (int64_t)r * n3 + (int64_t)p * r;
          int cnt = 0;
          for (int i = T.inter_ptr[c]; i < T.inter_ptr[c + 1]; i++) {
-            const int s = T.inter_cubes[i];
-            FFTSVD_REQUIRE(s >= 0 && s < T.num_cubes, "interacting cube out of range");
-            if (spec_of_cube[s] < 0) continue;  // source without panels or rank: contributes zero
-            FFTSVD_REQUIRE(T.cube_level[s] == lvl, "interaction across levels");
-            const int dx = T.cube_index[3 * c] - T.cube_index[3 * s];
-            const int dy = T.cube_index[3 * c + 1] - T.cube_index[3 * s + 1];
-            const int dz = T.cube_index[3 * c + 2] - T.cube_index[3 * s + 2];
+            const int sc = T.inter_cubes[i];
+            FFTSVD_REQUIRE(sc >= 0 && sc < T.num_cubes, "interacting cube out of range");
+            if (spec_of_cube[sc] < 0) continue;  // source without panels or rank: contributes zero
+            FFTSVD_REQUIRE(T.cube_level[sc] == lvl, "interaction across levels");
+            const int dx = T.cube_index[3 * c] - T.cube_index[3 * sc];
+            const int dy = T.cube_index[3 * c + 1] - T.cube_index[3 * sc + 1];
+            const int dz = T.cube_index[3 * c + 2] - T.cube_index[3 * sc + 2];
             FFTSVD_REQUIRE(std::abs(dx) <= 3 && std::abs(dy) <= 3 && std::abs(dz) <= 3, "interaction offset too large");
             FFTSVD_REQUIRE(std::abs(dx) > 1 || std::abs(dy) > 1 || std::abs(dz) > 1, "local cube in interaction list");
-            const int slot = ((dx + 3) * 7 + (dy + 3)) * 7 + (dz + 3);
-            const int64_t toff = tlev[lvl] + (int64_t)slot * pad16(pg);
             FFTSVD_REQUIRE(T.t_level_ptr[lvl + 1] - T.t_level_ptr[lvl] == 343LL * pg, "translation table size mismatch");
-            L.inter_pairs.push_back(spec_of_cube[s]);
-            L.inter_pairs.push_back(toff);
             cnt++;
          }
-         d.inter_cnt = cnt;
+         L.operator_elems += (int64_t)r * n3 + (int64_t)p * r;
          int need = 2 * pg + 2 * (n * Np * H) + 2 * (n * n * H) + n3 + r + 2 * Np + 16;
          L.max_dst_smem_elems = std::max(L.max_dst_smem_elems, need);
-         if (cnt > 0) {
-            d.s_off = L.translated_elems;
-            L.translated_elems += pad16(pg);
-            L.dst.push_back(d);
-            const int32_t* ci = &T.cube_index[3 * c];
-            uint64_t code = 0;  // Morton order of the cube coordinates
-            for (int b = 0; b < 21; b++)
-               for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> b) & 1) << (3 * b + k);
-            dst_extra.push_back({t * 64 + lvl, code, tlev[lvl], pad16(pg)});
-         } else {
-            L.uti.resize(d.uti_off), L.u_cm.resize(d.u_off), L.dst_points.resize(d.point_off);
+         if (cnt == 0) continue;  // no interaction with any source spectrum: no far field to add
+         DstDesc dd;
+         dd.n = n; dd.p = p; dd.r = r;
+         dd.point_off = (int32_t)(dp_0 + dp_all);
+         dd.uti_off = (int64_t)(uti0 + uti_all);
+         dd.u_off = (int64_t)(u0 + u_all);
+         dd.inter_off = (int32_t)((ip0 + ip_all) / 2);
+         dd.inter_cnt = cnt;
+         dd.stage = lvl;
+         dd.pad = 0;
+         dd.s_off = L.translated_elems;
+         L.translated_elems += pad16(pg);
+         dp_all += p;
+         uti_all += (size_t)r * n3;
+         u_all += (size_t)r * p;
+         ip_all += 2 * (size_t)cnt;
+         L.dst.push_back(dd);
+         dst_cube.push_back(c);
+         const int32_t* ci = &T.cube_index[3 * c];
+         uint64_t code = 0;  // Morton order of the cube coordinates
+         for (int bb = 0; bb < 21; bb++)
+            for (int k = 0; k < 3; k++) code |= (uint64_t)((ci[k] >> bb) & 1) << (3 * bb + k);
+         dst_extra.push_back({t * 64 + lvl, code, tlev[lvl], pad16(pg)});
+      }
+      L.dst_points.resize(dp_0 + dp_all);
+      L.uti.resize(uti0 + uti_all);
+      L.u_cm.resize(u0 + u_all);
+      L.inter_pairs.resize(ip0 + ip_all);
+      const int ndst_here = (int)dst_cube.size();
+#pragma omp parallel for schedule(dynamic, 16)
+      for (int i = 0; i < ndst_here; i++) {
+         const int c = dst_cube[i];
+         const DstDesc& dd = L.dst[d0 + i];
+         const int p = dd.p, r = dd.r, n = dd.n, n3 = n * n * n, pg = (2 * n - 1) * (2 * n - 1) * n;
+         const int lvl = T.cube_level[c];
+         for (int k = 0; k < p; k++)
+            L.dst_points[dd.point_off + k] = (int32_t)(qo + T.cube_points[T.cube_point_ptr[c] + k]);
+         std::copy(T.uti + T.cube_uti_ptr[c], T.uti + T.cube_uti_ptr[c] + (int64_t)r * n3, L.uti.begin() + dd.uti_off);
+         const int64_t uub = T.cube_u_ptr[c];
+         double* uo = &L.u_cm[dd.u_off];
+         for (int j = 0; j < r; j++)
+            for (int q = 0; q < p; q++) *uo++ = T.u[uub + (int64_t)q * r + j];
+         int64_t* io = &L.inter_pairs[2 * (size_t)dd.inter_off];
+         for (int ii = T.inter_ptr[c]; ii < T.inter_ptr[c + 1]; ii++) {
+            const int sc = T.inter_cubes[ii];
+            if (spec_of_cube[sc] < 0) continue;
+            const int dx = T.cube_index[3 * c] - T.cube_index[3 * sc];
+            const int dy = T.cube_index[3 * c + 1] - T.cube_index[3 * sc + 1];
+            const int dz = T.cube_index[3 * c + 2] - T.cube_index[3 * sc + 2];
+            const int slot = ((dx + 3) * 7 + (dy + 3)) * 7 + (dz + 3);
+            *io++ = spec_of_cube[sc];
+            *io++ = tlev[lvl] + (int64_t)slot * pad16(pg);
          }
       }
       // translation operators of this tree (unique tables: 316 non-local offsets per level),
@@ -563,7 +650,8 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
    {
       TileProblem& fwd = L.problems->fwd;
       TileProblem& adj = L.problems->adj;
-      std::map<int64_t, int> src_of_spec;
+      std::unordered_map<int64_t, int> src_of_spec;
+      src_of_spec.reserve(2 * L.src.size());
       for (int i = 0; i < (int)L.src.size(); i++) src_of_spec[L.src[i].spec_off] = i;
       std::vector<std::vector<std::pair<int64_t, int>>> adj_lists(L.src.size());
       for (int i = 0; i < (int)L.dst.size(); i++) {
@@ -2306,19 +2394,24 @@ __global__ void far_add_kernel(int64_t nrows, const int32_t* __restrict__ rows, 
 
 template <typename T>
 static void upload_cast(DevBuf<T>& dst, const std::vector<double>& src) {
-   std::vector<T> tmp(src.begin(), src.end());
-   dst.upload(tmp);
+   std::vector<T, FillLater<T>> tmp(src.size());
+   const int64_t n = (int64_t)tmp.size();
+#pragma omp parallel for schedule(static)
+   for (int64_t i = 0; i < n; i++) tmp[i] = (T)src[i];
+   dst.upload(tmp.data(), tmp.size());
 }
 
-template <typename T>
-static void upload_pairs(DevBuf<typename Vec2<T>::type>& dst, const std::vector<double>& src) {
+template <typename T, typename Vec>
+static void upload_pairs(DevBuf<typename Vec2<T>::type>& dst, const Vec& src) {
    using T2 = typename Vec2<T>::type;
-   std::vector<T2> tmp(src.size() / 2);
-   for (size_t i = 0; i < tmp.size(); i++) {
+   std::vector<T2, FillLater<T2>> tmp(src.size() / 2);
+   const int64_t np = (int64_t)tmp.size();
+#pragma omp parallel for schedule(static)
+   for (int64_t i = 0; i < np; i++) {
       tmp[i].x = (T)src[2 * i];
       tmp[i].y = (T)src[2 * i + 1];
    }
-   dst.upload(tmp);
+   dst.upload(tmp.data(), tmp.size());
 }
 
 // The dynamic shared-memory limit of a kernel is one device-wide setting shared by
@@ -2573,6 +2666,20 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
 
 template <typename T>
 void DeviceOperator<T>::DevTiles::upload(const TileSet& S) {
+   // shared-memory bytes one single-vector translation moves: per tile and frequency
+   // chunk, the staged rows (343 table slots and the halo spectra) are written once, and
+   // each (group, entry) reads its source row once and one table row per member; rows are
+   // kTileRowBytes wide
+   smem_bytes = 0.0;
+   for (const TileDesc& t : S.tiles) {
+      const double chunks = (double)t.pg / (kTileRowBytes / (double)sizeof(typename Vec2<T>::type));
+      double reads = 0.0;
+      for (int gi = 0; gi < t.ngroups; gi++) {
+         const int4 g = S.tile_grp[t.grp_off + gi];
+         reads += (double)g.y * (1.0 + g.w);
+      }
+      smem_bytes += chunks * kTileRowBytes * ((343.0 + t.nsrc) + reads);
+   }
    tiles.upload(S.tiles);
    src.upload(S.tile_src);
    dst.upload(S.tile_dst);
@@ -2816,6 +2923,11 @@ void DeviceOperator<T>::apply_bufs(const double* x, double* y, const Bufs& b, cu
       FFTSVD_CHECK_LAUNCH();
    }
    if (timing_) FFTSVD_CUDA(cudaEventRecord(ev_[5], stream));
+}
+
+template <typename T>
+double DeviceOperator<T>::translate_smem_bytes() const {
+   return fwd_.smem_bytes;
 }
 
 template <typename T>

@@ -15,9 +15,11 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "common.h"
+#include "fill_later.h"
 
 namespace fftsvd {
 
@@ -183,6 +185,8 @@ struct KernelBytes {
    double fixed[kNumKernels] = {0, 0, 0, 0, 0};
 };
 
+using LayoutDoubles = std::vector<double, FillLater<double>>;
+
 // Host-side relayout product, independent of the element type.
 struct OperatorLayout {
    int num_unknowns = 0;
@@ -201,12 +205,12 @@ struct OperatorLayout {
    // near field
    std::vector<LeafDesc> leaves;
    std::vector<int32_t> leaf_rows, leaf_cols;
-   std::vector<double> d_pairs;        // interleaved {Ds, Dd}
+   LayoutDoubles d_pairs;              // interleaved {Ds, Dd}
    // far field
    std::vector<SrcDesc> src;
    std::vector<int32_t> src_panels;
    std::vector<double> vt;
-   std::vector<double> pv_pairs;       // interleaved {PVs, PVd}, r x n^3
+   LayoutDoubles pv_pairs;             // interleaved {PVs, PVd}, r x n^3
    std::vector<DstDesc> dst;
    std::vector<int32_t> dst_points;
    std::vector<double> uti, u_cm;
@@ -270,6 +274,9 @@ class DeviceOperator {
    // solve sets it; the lockstep batch keeps the single-matvec arithmetic).
    void set_tensor_near(bool on) { tensor_near_ = on; }
    bool tensor_near_available() const { return near_np_max_ > 0; }
+   // Shared-memory bytes one single-vector translation moves (staged rows written, source
+   // and table rows read): the translation's bound is the SMs' shared-memory bandwidth.
+   double translate_smem_bytes() const;
    // nonzero when a tensor-core near-field wait gave up since the last reset
    int tensor_status(bool reset);
    // per-stage events for timing (recorded when enabled)
@@ -345,6 +352,7 @@ class DeviceOperator {
       DevBuf<int4> grp;
       DevBuf<uint32_t> entries;
       std::vector<TileGroup> groups;
+      double smem_bytes = 0.0;  // shared-memory traffic of one single-vector translation
       void upload(const TileSet& S);
    };
    DevTiles fwd_, adj_;

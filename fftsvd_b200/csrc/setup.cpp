@@ -29,6 +29,7 @@
 
 #include "../../include/fftsvd_b200.h"
 #include "integrals.h"
+#include "fill_later.h"
 #include "setup.h"
 
 namespace fftsvd {
@@ -421,7 +422,7 @@ void Tree::fill_near() {
          B.out_elems += 2 * (int64_t)nr * nc;
          B.blocks.push_back(b);
       }
-      std::vector<double> out((size_t)B.out_elems);
+      std::vector<double, FillLater<double>> out((size_t)B.out_elems);  // every entry is written
       const auto e0 = std::chrono::steady_clock::now();
       (*eval)(kernel, *panels, B, out.data());
       eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - e0).count();
@@ -560,7 +561,7 @@ void Tree::fill_bases() {
    // With an evaluator the first sampling pass of every cube and its sphere fits are
    // integrated in one batch; a cube whose first pass does not settle its rank samples its
    // further passes on the host as before.
-   std::vector<double> pre;
+   std::vector<double, FillLater<double>> pre;  // every entry is written by the batch
    std::vector<int64_t> roff(work.size(), -1), coff(work.size(), -1), soff(work.size(), -1);
    if (eval) {
       IntegralBatch B;

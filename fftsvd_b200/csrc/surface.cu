@@ -563,6 +563,12 @@ int fftsvd_b200_profile_matvec(fftsvd_surface* s, int32_t precision, const doubl
    });
 }
 
+int fftsvd_b200_translate_smem_bytes(const fftsvd_surface* s, int32_t precision, double* bytes) {
+   if (!s || !bytes) return FFTSVD_ERR_ARGUMENT;
+   *bytes = precision == FFTSVD_PREC_FP64 ? s->s.op64.translate_smem_bytes() : s->s.op32.translate_smem_bytes();
+   return FFTSVD_OK;
+}
+
 int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes) {
    if (!s || !bytes) return FFTSVD_ERR_ARGUMENT;
    const double es = precision == FFTSVD_PREC_FP64 ? 8.0 : 4.0;

@@ -29,7 +29,7 @@ EXPORTED = [
     "fftsvd_b200_matvec_bytes", "fftsvd_b200_surface_stats", "fftsvd_b200_host_setup",
     "fftsvd_b200_host_operator_tree", "fftsvd_b200_device_setup", "fftsvd_b200_host_setup_batched",
     "fftsvd_b200_host_operator_timings", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
-    "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
+    "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_translate_smem_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
     "fftsvd_b200_launch_count", "fftsvd_b200_device_alloc_count", "fftsvd_b200_reaction_potentials_noalloc",
     "solveSurfaceOperator", "generateRHS",
     "collectPotentials",
@@ -91,6 +91,7 @@ def load():
     lib.fftsvd_b200_host_operator_precond.argtypes = [sp, C.POINTER(PrecondCSC)]
     lib.fftsvd_b200_host_operator_free.argtypes = [sp]
     lib.fftsvd_b200_matvec_kernel_bytes.argtypes = [sp, C.c_int32, _f64p]
+    lib.fftsvd_b200_translate_smem_bytes.argtypes = [sp, C.c_int32, _f64p]
     lib.fftsvd_b200_profile_matvec.argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, _f64p]
     lib.fftsvd_b200_surface_stream.argtypes = [sp]
     lib.fftsvd_b200_surface_stream.restype = C.c_void_p

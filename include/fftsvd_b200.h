@@ -272,6 +272,10 @@ int fftsvd_b200_energy(fftsvd_surface* s, const double* phi, double* energy);
    and the FP64 input and output vectors. */
 int fftsvd_b200_matvec_bytes(const fftsvd_surface* s, int32_t precision, double* bytes);
 
+/* Shared-memory bytes one matvec's translation stage moves (staged table and halo rows
+   written, source and table rows read): the translation is bound by the SMs' shared-memory
+   bandwidth rather than by HBM. */
+int fftsvd_b200_translate_smem_bytes(const fftsvd_surface* s, int32_t precision, double* bytes);
 /* Algorithmic bytes of each matvec kernel: [join, far_forward, translate, far_backward, near]. */
 int fftsvd_b200_matvec_kernel_bytes(const fftsvd_surface* s, int32_t precision, double* bytes5);
 /* Run `reps` matvecs on device vectors with CUDA events around each kernel on
