@@ -318,6 +318,9 @@ def run_large(flush, steps, warmup):
            "dG_kcal_mixed": em, "dG_kcal_fp64": e64, "dG_rel_err_mixed_vs_fp64": abs(em - e64) / abs(e64),
            "dG_rel_err_vs_ref_fp64": _ref64_errors(golden_ref64("blob7", tri, qpos, q), em, e64),
            "setup_s": setup_s, "setup_stage_ms": list(st.setup_ms)}
+    # the batched solve at this end of the panel range: 256 charge groups as one block GMRES
+    del rhs, sol
+    out["batched_256_rhs"] = run_block256(s, qpos, q, cfg, flush, t64 / k64)
     s.close()
     return out
 
@@ -358,6 +361,7 @@ def run_ours(args, cfg, ws, rank, local):
     from fftsvd_b200.surface import Surface
 
     torch.cuda.set_device(local)
+    torch.zeros(1, device="cuda")  # the CUDA context exists before the setup is timed
     lib = load()
     tri, qpos, q = make_workload(cfg, rank)
     t0 = time.time()
@@ -828,7 +832,8 @@ def run_capture(args, cfg, local):
     `gmres` = right-hand side, 12 steps of an FP64 GMRES solve and the reaction potentials;
     `transpose` = one FP32 transposed matvec (the adjoint's operator);
     `block` = one mixed-precision block GMRES solve of the charge groups' right-hand sides
-    (configurations with groups)."""
+    (configurations with groups);
+    `near_tc` = two 128-column FP32 multi-vector matvecs with the tensor-core near field."""
     import ctypes as C
 
     import torch
@@ -858,6 +863,20 @@ def run_capture(args, cfg, local):
                           "residual_max": max(info[c].residual for c in range(k))}))
         s.close()
         return
+    if args.capture == "near_tc":
+        k = 128
+        X = torch.randn((k, s.n), dtype=torch.float64, device="cuda")
+        Y = torch.empty_like(X)
+        lib = load()
+        for _ in range(2):
+            rc = lib.fftsvd_b200_matvec_batch_tensor_device(s._h, k, C.c_void_p(X.data_ptr()),
+                                                            C.c_void_p(Y.data_ptr()))
+            if rc != 0:
+                raise RuntimeError(lib.fftsvd_b200_last_error().decode())
+        torch.cuda.synchronize()
+        print(json.dumps({"capture": "near_tc", "workload": cfg["name"], "nrhs": k, "norm": float(Y.norm())}))
+        s.close()
+        return
     if args.capture == "gmres":
         s.rhs_device(x.data_ptr())
         info = _abi.SolveInfo()
@@ -876,7 +895,7 @@ def run_capture(args, cfg, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--matvec-only", action="store_true", help="only run --reps matvecs (profiling)")
-    ap.add_argument("--capture", choices=["gmres", "transpose", "block"], default=None,
+    ap.add_argument("--capture", choices=["gmres", "transpose", "block", "near_tc"], default=None,
                     help="only run one part of the workload (profiling)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)

@@ -65,14 +65,12 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
     double* __restrict__ y, int nrhs, int64_t ldn, int np_max, int* __restrict__ status) {
    extern __shared__ __align__(1024) char smem[];
    const int np_cap = np_max;                    // B operand rows the buffers hold
-   char* const Ah = smem;                        // kTcRhs x kTcK, heads
-   char* const Al = Ah + kTcRhs * kTcK * 4;      // tails
-   char* const Bh = Al + kTcRhs * kTcK * 4;      // np_cap x kTcK
-   char* const Bl = Bh + np_cap * kTcK * 4;
-   int* const row_out = reinterpret_cast<int*>(Bl + np_cap * kTcK * 4);  // per leaf row
+   // two stages, each: A heads, A tails (kTcRhs x kTcK), B heads, B tails (np_cap x kTcK)
+   const int a_bytes = kTcRhs * kTcK * 4, b_bytes = np_cap * kTcK * 4, stage_bytes = 2 * a_bytes + 2 * b_bytes;
+   int* const row_out = reinterpret_cast<int*>(smem + 2 * stage_bytes);  // per leaf row
    int* const row_jk = row_out + np_cap;
    double* const row_jump = reinterpret_cast<double*>(row_jk + np_cap);
-   __shared__ __align__(8) uint64_t mbar;
+   __shared__ __align__(8) uint64_t mbar[2];     // one per stage: its chunk's MMAs completed
    __shared__ uint32_t tslot;
    const int t = threadIdx.x, warp = t >> 5;
    const LeafDesc L = leaves[blockIdx.x];
@@ -81,7 +79,10 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
    uint32_t ncols_tmem = 32;
    while ((int)ncols_tmem < np) ncols_tmem <<= 1;
    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tslot), ncols_tmem);
-   if (t == 0) tc::mbar_init(tc::smem_addr(&mbar), 1);
+   if (t == 0) {
+      tc::mbar_init(tc::smem_addr(&mbar[0]), 1);
+      tc::mbar_init(tc::smem_addr(&mbar[1]), 1);
+   }
    for (int i = t; i < nr; i += kTcRhs) {
       const int pnt = rows[L.row_off + i];
       const int k = point_panel[pnt];
@@ -95,18 +96,38 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
    const uint32_t tmem = tslot;
    const uint32_t idesc = tc::idesc_tf32(kTcRhs, np);
    const float2* drow = d + L.d_off;
+   const int nchunks = (kdim + kTcK - 1) / kTcK;
    bool ok = true;
-   int chunk = 0;
-   for (int k0 = 0; k0 < kdim; k0 += kTcK, chunk++) {
-      // X chunk: thread t is right-hand side t; K value 2 c + layer of column c
-#pragma unroll 4
+   int committed = -1;  // last chunk whose MMAs were committed
+   // Chunk k is staged into stage k & 1 while the MMAs of chunk k - 1 run on the other stage;
+   // a stage is refilled once the MMAs of the chunk two back, which read it, have completed.
+   for (int chunk = 0; chunk < nchunks; chunk++) {
+      const int st = chunk & 1, k0 = chunk * kTcK;
+      char* const Ah = smem + st * stage_bytes;
+      char* const Al = Ah + a_bytes;
+      char* const Bh = Al + a_bytes;
+      char* const Bl = Bh + b_bytes;
+      // X chunk: thread t is right-hand side t; K value 2 c + layer of column c.  All loads
+      // are issued before any split and store.
+      float2 xv[kTcK / 2];
+#pragma unroll
       for (int c = 0; c < kTcK / 2; c++) {
          const int col = (k0 >> 1) + c;
-         float2 v = make_float2(0.f, 0.f);
-         if (rhs < nrhs && 2 * col < kdim) v = xsd_t[(int64_t)cols[L.col_off + col] * ld + rhs];
+         xv[c] = make_float2(0.f, 0.f);
+         if (rhs < nrhs && 2 * col < kdim) xv[c] = xsd_t[(int64_t)cols[L.col_off + col] * ld + rhs];
+      }
+      constexpr int kDPer = 4;  // D pairs per thread and pass
+      float2 dv[kDPer];
+      const int dcount = np * (kTcK / 2);
+      if (chunk >= 2 && !tc::mbar_wait(tc::smem_addr(&mbar[st]), (uint32_t)(((chunk - 2) >> 1) & 1), kTcPolls))
+         ok = false;
+      tc::fence_after_sync();
+      if (__syncthreads_or(!ok)) break;  // the stage is free: the MMAs that read it completed
+#pragma unroll
+      for (int c = 0; c < kTcK / 2; c++) {
          float h0, l0, h1, l1;
-         tc::split_tf32(v.x, h0, l0);
-         tc::split_tf32(v.y, h1, l1);
+         tc::split_tf32(xv[c].x, h0, l0);
+         tc::split_tf32(xv[c].y, h1, l1);
          const uint32_t o0 = tc_off(t, 2 * c, kTcRhs), o1 = tc_off(t, 2 * c + 1, kTcRhs);
          *reinterpret_cast<float*>(Ah + o0) = h0;
          *reinterpret_cast<float*>(Al + o0) = l0;
@@ -114,18 +135,28 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
          *reinterpret_cast<float*>(Al + o1) = l1;
       }
       // D chunk: np rows (rows past nr are zero) x 16 columns of pairs
-      for (int i = t; i < np * (kTcK / 2); i += kTcRhs) {
-         const int row = i / (kTcK / 2), c = i % (kTcK / 2), col = (k0 >> 1) + c;
-         float2 v = make_float2(0.f, 0.f);
-         if (row < nr && 2 * col < kdim) v = drow[(int64_t)row * L.ncols + col];
-         float h0, l0, h1, l1;
-         tc::split_tf32(v.x, h0, l0);
-         tc::split_tf32(v.y, h1, l1);
-         const uint32_t o0 = tc_off(row, 2 * c, np), o1 = tc_off(row, 2 * c + 1, np);
-         *reinterpret_cast<float*>(Bh + o0) = h0;
-         *reinterpret_cast<float*>(Bl + o0) = l0;
-         *reinterpret_cast<float*>(Bh + o1) = h1;
-         *reinterpret_cast<float*>(Bl + o1) = l1;
+      for (int i0 = t; i0 < dcount; i0 += kTcRhs * kDPer) {
+#pragma unroll
+         for (int q = 0; q < kDPer; q++) {
+            const int i = i0 + q * kTcRhs;
+            const int row = i / (kTcK / 2), col = (k0 >> 1) + i % (kTcK / 2);
+            dv[q] = make_float2(0.f, 0.f);
+            if (i < dcount && row < nr && 2 * col < kdim) dv[q] = drow[(int64_t)row * L.ncols + col];
+         }
+#pragma unroll
+         for (int q = 0; q < kDPer; q++) {
+            const int i = i0 + q * kTcRhs;
+            if (i >= dcount) break;
+            const int row = i / (kTcK / 2), c = i % (kTcK / 2);
+            float h0, l0, h1, l1;
+            tc::split_tf32(dv[q].x, h0, l0);
+            tc::split_tf32(dv[q].y, h1, l1);
+            const uint32_t o0 = tc_off(row, 2 * c, np), o1 = tc_off(row, 2 * c + 1, np);
+            *reinterpret_cast<float*>(Bh + o0) = h0;
+            *reinterpret_cast<float*>(Bl + o0) = l0;
+            *reinterpret_cast<float*>(Bh + o1) = h1;
+            *reinterpret_cast<float*>(Bl + o1) = l1;
+         }
       }
       tc::fence_proxy_async();
       __syncthreads();
@@ -142,14 +173,22 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
             tc::mma_tf32(tmem, ah, bl, idesc, 1u);
             tc::mma_tf32(tmem, al, bh, idesc, 1u);
          }
-         tc::commit(tc::smem_addr(&mbar));
+         tc::commit(tc::smem_addr(&mbar[st]));  // arrives when every MMA issued so far completed
       }
-      if (!tc::mbar_wait(tc::smem_addr(&mbar), (uint32_t)(chunk & 1), kTcPolls)) ok = false;
+      committed = chunk;
+   }
+   // the last chunk's commit covers every MMA before it: the accumulator is complete
+   if (ok && nchunks > 0) {
+      const int last = nchunks - 1;
+      if (!tc::mbar_wait(tc::smem_addr(&mbar[last & 1]), (uint32_t)((last >> 1) & 1), kTcPolls)) ok = false;
       tc::fence_after_sync();
-      if (__syncthreads_or(!ok)) break;  // the buffers are refilled only after the MMAs read them
+      if (__syncthreads_or(!ok)) ok = false;
    }
    if (!ok) {
       if (t == 0) atomicExch(status, 1);
+      // one more bounded wait for the MMAs still in flight before the TMEM is released
+      if (committed >= 0)
+         tc::mbar_wait(tc::smem_addr(&mbar[committed & 1]), (uint32_t)((committed >> 1) & 1), kTcPolls);
    } else {
       // every lane takes part in the warp-wide TMEM loads; lanes past nrhs only skip the stores
       const double* xr = x + (int64_t)rhs * ldn;
@@ -176,10 +215,34 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
    if (warp == 0) tc::tmem_free(tmem, ncols_tmem);
 }
 
+// A wait that must give up: an mbarrier expecting one arrival that never comes, polled at
+// most `polls` times.  Sets *status to 1 when the wait gave up, 2 when it (wrongly) completed.
+__global__ void bounded_wait_selftest_kernel(uint32_t polls, int* __restrict__ status) {
+   __shared__ __align__(8) uint64_t bar;
+   if (threadIdx.x == 0) tc::mbar_init(tc::smem_addr(&bar), 1);
+   __syncthreads();
+   const bool done = tc::mbar_wait(tc::smem_addr(&bar), 0u, polls);
+   if (__syncthreads_or(!done)) {
+      if (threadIdx.x == 0) *status = 1;
+   } else if (threadIdx.x == 0) {
+      *status = 2;
+   }
+}
+
 }  // namespace
 
+int bounded_wait_selftest(int polls) {
+   DevBuf<int> status(1);
+   status.zero();
+   bounded_wait_selftest_kernel<<<1, 32>>>((uint32_t)polls, status.get());
+   FFTSVD_CHECK_LAUNCH();
+   int v = 0;
+   FFTSVD_CUDA(cudaMemcpy(&v, status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+   return v;
+}
+
 int near_tc_smem(int np_max) {
-   return 2 * kTcRhs * kTcK * 4 + 2 * np_max * kTcK * 4 + np_max * (4 + 4 + 8);
+   return 2 * (2 * kTcRhs * kTcK * 4 + 2 * np_max * kTcK * 4) + np_max * (4 + 4 + 8);
 }
 
 void launch_near_tc(const LeafDesc* leaves, int n_leaf, const int32_t* rows, const int32_t* cols, const float2* d,

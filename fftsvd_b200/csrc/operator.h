@@ -239,6 +239,10 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
 // CTA.  np_max: the largest leaf row count padded to 8 (at most 256).  A bounded wait that
 // gives up sets *status.
 int near_tc_smem(int np_max);
+// Runs one wait on an mbarrier that nothing arrives at, bounded by `polls` polls, as the
+// tensor-core kernels bound theirs: 1 when the wait gave up (the expected result), 2 when
+// it completed.  Synchronous.
+int bounded_wait_selftest(int polls);
 void prepare_near_tc(int np_max);
 void launch_near_tc(const LeafDesc* leaves, int n_leaf, const int32_t* rows, const int32_t* cols, const float2* d,
                     const float2* xsd, int64_t panels, int np_panels, float2* xsd_t, int64_t ld,

@@ -95,13 +95,35 @@ struct DeviceSampler {
    Buf<FlatPanel> panels;
    const FlatPanel* host_panels = nullptr;  // the panel list the device copy was made from
    size_t host_count = 0;
+   // Pinned host copy of the last batch's output, grown to the largest batch: the results
+   // come back at full link speed and the setup's several batches reuse one allocation.
+   double* pinned = nullptr;
+   size_t pinned_elems = 0;
    ~DeviceSampler() {
       if (stream) cudaStreamDestroy(stream);
+      if (pinned) cudaFreeHost(pinned);
    }
 
-   void operator()(const Kernel& kern, const std::vector<FlatPanel>& pl, const IntegralBatch& B, double* out) {
-      if (B.out_elems == 0 || B.blocks.empty()) return;
+   double* host_output(size_t elems) {
+      if (elems > pinned_elems) {
+         if (pinned) cudaFreeHost(pinned);
+         pinned = nullptr;
+         pinned_elems = 0;
+         cuda_check(cudaHostAlloc((void**)&pinned, elems * sizeof(double), cudaHostAllocDefault),
+                    "cudaHostAlloc (setup integrals)");
+         pinned_elems = elems;
+      }
+      return pinned;
+   }
+
+   const double* operator()(const Kernel& kern, const std::vector<FlatPanel>& pl, const IntegralBatch& B) {
+      if (B.out_elems == 0) return nullptr;
       if (!stream) cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      double* out = host_output((size_t)B.out_elems);
+      if (B.blocks.empty()) {
+         std::fill(out, out + B.out_elems, 0.0);
+         return out;
+      }
       if (host_panels != pl.data() || host_count != pl.size()) {
          panels.upload(pl.data(), pl.size(), stream);
          host_panels = pl.data();
@@ -130,7 +152,10 @@ struct DeviceSampler {
          blocks[bi] = DevBlock{b.npts, b.npan, b.pt_off, b.pan_off, b.out_s, b.out_d, b.ld_s, b.ld_d};
          for (int64_t f = 0; f < pairs; f += kTilePairs) tiles.push_back(PairTile{(int32_t)bi, (int32_t)f});
       }
-      if (tiles.empty()) return;
+      if (tiles.empty()) {
+         std::fill(out, out + B.out_elems, 0.0);
+         return out;
+      }
       Buf<DevBlock> d_blocks;
       Buf<PairTile> d_tiles;
       Buf<double> d_pts, d_out;
@@ -161,6 +186,7 @@ struct DeviceSampler {
                  "copy to host");
       cuda_check(cudaStreamSynchronize(stream), "setup integrals");
       if (bad) throw std::runtime_error("Yukawa panel integration did not converge");
+      return out;
    }
 };
 
@@ -171,8 +197,8 @@ BatchEvaluator device_evaluator() {
    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
       throw DeviceError(FFTSVD_ERR_NO_DEVICE, "no CUDA device visible");
    auto sampler = std::make_shared<DeviceSampler>();
-   return [sampler](const Kernel& k, const std::vector<FlatPanel>& pl, const IntegralBatch& b, double* out) {
-      (*sampler)(k, pl, b, out);
+   return [sampler](const Kernel& k, const std::vector<FlatPanel>& pl, const IntegralBatch& b) {
+      return (*sampler)(k, pl, b);
    };
 }
 

@@ -422,17 +422,16 @@ void Tree::fill_near() {
          B.out_elems += 2 * (int64_t)nr * nc;
          B.blocks.push_back(b);
       }
-      std::vector<double, FillLater<double>> out((size_t)B.out_elems);  // every entry is written
       const auto e0 = std::chrono::steady_clock::now();
-      (*eval)(kernel, *panels, B, out.data());
+      const double* out = (*eval)(kernel, *panels, B);
       eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - e0).count();
 #pragma omp parallel for schedule(static)
       for (size_t li = 0; li < leaves.size(); li++) {
          if (off[li] < 0) continue;
          Cube& c = cubes[leaves[li]];
          const size_t e = c.points.size() * c.dcols.size();
-         c.Ds.assign(out.begin() + off[li], out.begin() + off[li] + e);
-         c.Dd.assign(out.begin() + off[li] + e, out.begin() + off[li] + 2 * e);
+         c.Ds.assign(out + off[li], out + off[li] + e);
+         c.Dd.assign(out + off[li] + e, out + off[li] + 2 * e);
       }
       return;
    }
@@ -561,7 +560,7 @@ void Tree::fill_bases() {
    // With an evaluator the first sampling pass of every cube and its sphere fits are
    // integrated in one batch; a cube whose first pass does not settle its rank samples its
    // further passes on the host as before.
-   std::vector<double, FillLater<double>> pre;  // every entry is written by the batch
+   const double* pre = nullptr;  // the batch's output, owned by the evaluator
    std::vector<int64_t> roff(work.size(), -1), coff(work.size(), -1), soff(work.size(), -1);
    if (eval) {
       IntegralBatch B;
@@ -610,9 +609,8 @@ void Tree::fill_bases() {
             B.blocks.push_back(b);
          }
       }
-      pre.resize((size_t)B.out_elems);
       const auto e0 = std::chrono::steady_clock::now();
-      (*eval)(kernel, *panels, B, pre.data());
+      pre = (*eval)(kernel, *panels, B);
       eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - e0).count();
    }
 #pragma omp parallel for schedule(dynamic, 1)
@@ -629,7 +627,7 @@ void Tree::fill_bases() {
             const int rows = 2 * nwp * pass;
             std::vector<double> R;
             if (pass == 1 && roff[wi] >= 0)
-               R.assign(pre.begin() + roff[wi], pre.begin() + roff[wi] + (int64_t)rows * m);
+               R.assign(pre + roff[wi], pre + roff[wi] + (int64_t)rows * m);
             else
                row_samples(c, withpoints, pass, R);
             std::vector<double> VT;
@@ -646,7 +644,7 @@ void Tree::fill_bases() {
             const int cols = 2 * nwq * pass;
             std::vector<double> Cm;
             if (pass == 1 && coff[wi] >= 0)
-               Cm.assign(pre.begin() + coff[wi], pre.begin() + coff[wi] + (int64_t)np * cols);
+               Cm.assign(pre + coff[wi], pre + coff[wi] + (int64_t)np * cols);
             else
                col_samples(c, withpanels, pass, Cm);
             std::vector<double> U;
@@ -667,8 +665,8 @@ void Tree::fill_bases() {
          std::vector<double> Qs((size_t)kNumSphere * m), Qd((size_t)kNumSphere * m);
          if (soff[wi] >= 0) {
             const int64_t e = (int64_t)kNumSphere * m;
-            std::copy(pre.begin() + soff[wi], pre.begin() + soff[wi] + e, Qs.begin());
-            std::copy(pre.begin() + soff[wi] + e, pre.begin() + soff[wi] + 2 * e, Qd.begin());
+            std::copy(pre + soff[wi], pre + soff[wi] + e, Qs.begin());
+            std::copy(pre + soff[wi] + e, pre + soff[wi] + 2 * e, Qd.begin());
          } else {
             for (int q = 0; q < kNumSphere; q++)
                for (int k = 0; k < m; k++)
@@ -853,7 +851,10 @@ void FlatTree::view(fftsvd_tree_flat& t) const {
 }
 
 BatchEvaluator host_evaluator() {
-   return [](const Kernel& k, const std::vector<FlatPanel>& pl, const IntegralBatch& B, double* out) {
+   auto store = std::make_shared<std::vector<double, FillLater<double>>>();
+   return [store](const Kernel& k, const std::vector<FlatPanel>& pl, const IntegralBatch& B) -> const double* {
+      store->resize((size_t)B.out_elems);  // every entry is written below
+      double* out = store->data();
       const int64_t nb = (int64_t)B.blocks.size();
 #pragma omp parallel for schedule(dynamic, 4)
       for (int64_t bi = 0; bi < nb; bi++) {
@@ -865,6 +866,7 @@ BatchEvaluator host_evaluator() {
                        &out[b.out_d + (int64_t)i * b.ld_d + j]);
          }
       }
+      return out;
    };
 }
 

@@ -37,11 +37,12 @@ struct IntegralBatch {
    int64_t out_elems = 0;        // size of the output array
 };
 
-// Evaluates every block of a batch with one kernel over the tree's panels into out
-// (out_elems doubles).  Trees without an evaluator integrate on the host, panel by
-// panel; the device evaluator (sampling.cu) runs the same integrals on the GPU.
+// Evaluates every block of a batch with one kernel over the tree's panels and returns the
+// output array (out_elems doubles), valid until the evaluator's next call.  Trees without an
+// evaluator integrate on the host, panel by panel; the device evaluator (sampling.cu) runs
+// the same integrals on the GPU and returns them in pinned host memory.
 using BatchEvaluator =
-    std::function<void(const Kernel& k, const std::vector<FlatPanel>& panels, const IntegralBatch& b, double* out)>;
+    std::function<const double*(const Kernel& k, const std::vector<FlatPanel>& panels, const IntegralBatch& b)>;
 
 struct Cube {
    int level = 0;

@@ -526,6 +526,19 @@ int fftsvd_b200_solve(fftsvd_surface* s, int32_t precision, const double* rhs, d
 }
 
 long long fftsvd_b200_launch_count(void) { return g_kernel_launches.load(); }
+
+int fftsvd_b200_bounded_wait_selftest(int32_t polls) {
+   if (polls <= 0) return FFTSVD_ERR_ARGUMENT;
+   int result = 0;
+   const int rc = guarded([&] { result = bounded_wait_selftest(polls); });
+   if (rc != FFTSVD_OK) return rc;
+   if (result == 1) {
+      set_last_error("bounded device wait gave up as expected");
+      return FFTSVD_ERR_TIMEOUT;
+   }
+   set_last_error("bounded device wait completed without an arrival");
+   return FFTSVD_ERR_CUDA;
+}
 long long fftsvd_b200_device_alloc_count(void) { return g_device_allocs.load(); }
 
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s) { return s ? (void*)s->s.stream : nullptr; }

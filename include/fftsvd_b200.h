@@ -399,6 +399,11 @@ int fftsvd_b200_rhs_groups_device(fftsvd_surface* s, int32_t ngroups, const int3
    phi_reac from that column only.  energies is a host array of ngroups. */
 int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const int32_t* group_ptr, const double* sol,
                                       double* energies);
+/* Failure-detection self-test (no counterpart in the reference): one device wait on an
+   mbarrier that nothing arrives at, bounded by `polls` polls exactly as the library's
+   tensor-core kernels bound their waits.  Returns FFTSVD_ERR_TIMEOUT when the wait gave
+   up (the expected outcome; the context stays usable), FFTSVD_ERR_CUDA when it completed. */
+int fftsvd_b200_bounded_wait_selftest(int32_t polls);
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
 /* Device allocations (cudaMalloc calls) made by this library since it was loaded. */
