@@ -78,8 +78,7 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
                   "-I", "/usr/local/cuda/include", "-c", src, "-o", obj])
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         _run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-Xcompiler", "-fopenmp", "-o", LIB, *objs,
-              "-lgomp", "-cudart", "static", "-L/usr/local/cuda/lib64", "-lcublas",
-              "-Xlinker", "-rpath=/usr/local/cuda/lib64"])
+              "-lgomp", "-cudart", "static"])
     return LIB
 
 

@@ -10,9 +10,9 @@
 // solves', so the columns agree with single solves to the tolerance, not bit for bit.
 //
 // Device: the multi-vector matvec and preconditioner of the batch, the block
-// Gram-Schmidt and the products with the basis as FP64 GEMMs (cuBLAS), the block QR as
-// CholQR2 (Gram matrix, Cholesky factor in a one-block kernel, triangular solve; twice),
-// the final triangular solve (cuBLAS).  Gram-Schmidt is one classical pass while no
+// Gram-Schmidt and the products with the basis as FP64 tensor-core GEMMs (dense.cu), the
+// block QR as CholQR2 (Gram matrix, Cholesky factor in a one-block kernel, product with
+// the factor's inverse; twice), the final block triangular solve (dense.cu).  Gram-Schmidt is one classical pass while no
 // column of a new block loses more than five digits in it (the new block is then
 // orthogonal to the basis to about 1e-11, far below what a solve to 1e-6 needs), two
 // passes from the first step where one does.  Host: the block
@@ -24,7 +24,6 @@
 // (which keep the block full rank and are not monitored), runs one block GMRES cycle
 // and adds the scaled corrections back; the residual is then recomputed with the outer
 // operator (FP64 for the mixed mode, as the single solve's refinement).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,15 +34,8 @@
 
 #include "block.h"
 #include "block_ls.h"
+#include "dense.h"
 #include "surface.h"
-
-#define FFTSVD_BLAS(call)                                                                     \
-   do {                                                                                      \
-      cublasStatus_t st_ = (call);                                                           \
-      if (st_ != CUBLAS_STATUS_SUCCESS)                                                      \
-         throw ::fftsvd::Error(FFTSVD_ERR_CUDA,                                              \
-                               std::string(#call) + ": cuBLAS status " + std::to_string((int)st_)); \
-   } while (0)
 
 namespace fftsvd {
 
@@ -188,7 +180,6 @@ int pad8(int k) { return (k + kBatchGroup - 1) / kBatchGroup * kBatchGroup; }
 }  // namespace
 
 BlockWorkspace::~BlockWorkspace() {
-   if (blas) cublasDestroy((cublasHandle_t)blas);
    for (auto& e : done)
       if (e) cudaEventDestroy(e);
    for (auto& p : hbuf)
@@ -199,16 +190,13 @@ BlockWorkspace::~BlockWorkspace() {
 }
 
 void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) {
-   if (!blas) {
-      cublasHandle_t h;
-      FFTSVD_BLAS(cublasCreate(&h));
-      blas = h;
+   (void)stream;
+   if (!flag_h) {
       for (auto& e : done) FFTSVD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       FFTSVD_CUDA(cudaMallocHost(&flag_h, 2 * sizeof(int)));
       FFTSVD_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)chol_smem(kBlockMax)));
    }
-   FFTSVD_BLAS(cublasSetStream((cublasHandle_t)blas, stream));
    if (n_ == n && K_ <= K && mmax_ <= mmax) return;
    if (n_ != n) K = mmax = 0;
    n = n_;
@@ -216,11 +204,17 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
    mmax = std::max(mmax, mmax_);
    const size_t kn = (size_t)K * n, kk = (size_t)K * K;
    V.alloc((size_t)(mmax + 1) * kn);
-   for (DevBuf<double>* b : {&W, &R0, &T, &Bc, &Xc, &Rc, &Tc}) b->alloc(kn);
+   for (DevBuf<double>* b : {&W, &R0, &T, &Bc, &Xc, &Rc, &Tc, &Qs}) b->alloc(kn);
    H.alloc((size_t)(mmax + 1) * kk);
    H2.alloc((size_t)(mmax + 1) * kk);
-   for (DevBuf<double>* b : {&G, &R1, &R2, &R}) b->alloc(kk);
+   for (DevBuf<double>* b : {&G, &R1, &R2, &R, &Rinv}) b->alloc(kk);
    Y.alloc((size_t)mmax * kk);
+   Yo.alloc((size_t)mmax * kk);
+   Dinv.alloc((size_t)mmax * kk);
+   // split-K partials of the Gram matrices (K x K) and of the projections on up to mmax blocks
+   int64_t wmax = dense::gemm_tn_work(K, K, n);
+   for (int j = 1; j <= mmax; j++) wmax = std::max(wmax, dense::gemm_tn_work(j * K, K, n));
+   gwork.alloc((size_t)std::max<int64_t>(wmax, 1));
    Rd.alloc((size_t)mmax * K * (size_t)mmax * K);
    scal.alloc(K);
    part.alloc((size_t)K * vec_blocks(n));
@@ -240,23 +234,23 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
 }
 
 // Q R = X (n x K, both column-major with ld n; X may be Q) by CholQR2: twice the Gram
-// matrix, its Cholesky factor and a triangular solve in place.  R (K x K) is left in
-// blk->R and a rank deficiency raises blk->flag.
+// matrix, its Cholesky factor R_p and the product with R_p^-1 (out of place, through the
+// scratch block Qs).  R = R_2 R_1 (K x K) is left in blk->R and a rank deficiency raises
+// blk->flag.
 void Surface::block_qr(const double* X, double* Q, int K) {
    BlockWorkspace& B = *blk;
-   cublasHandle_t h = (cublasHandle_t)B.blas;
-   const double one = 1.0, zero = 0.0;
-   if (X != Q)
-      FFTSVD_CUDA(cudaMemcpyAsync(Q, X, sizeof(double) * (size_t)K * n, cudaMemcpyDeviceToDevice, stream));
-   for (double* Rp : {B.R1.get(), B.R2.get()}) {
-      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, K, n, &one, Q, n, Q, n, &zero, B.G.get(), K));
+   const double* src = X;
+   for (int pass = 0; pass < 2; pass++) {
+      double* Rp = pass ? B.R2.get() : B.R1.get();
+      double* dst = pass ? Q : B.Qs.get();
+      dense::gemm_tn(K, K, n, 1.0, src, n, src, n, 0.0, B.G.get(), K, B.gwork.get(), stream);
       chol_kernel<<<1, kCholThreads, chol_smem(K), stream>>>(K, B.G.get(), Rp, B.flag.get());
       FFTSVD_CHECK_LAUNCH();
-      FFTSVD_BLAS(cublasDtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, K,
-                              &one, Rp, K, Q, n));
+      dense::trinv_upper(K, 1, Rp, K, 0, B.Rinv.get(), K, 0, stream);
+      dense::gemm_nn(n, K, K, 1.0, src, n, B.Rinv.get(), K, 0.0, dst, n, stream);
+      src = dst;
    }
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &one, B.R2.get(), K, B.R1.get(), K, &zero, B.R.get(),
-                           K));
+   dense::gemm_nn(K, K, K, 1.0, B.R2.get(), K, B.R1.get(), K, 0.0, B.R.get(), K, stream);
 }
 
 // One cycle of block GMRES on P^-1 A T = R0 (K columns, A the operator `precision`),
@@ -268,8 +262,6 @@ void Surface::block_qr(const double* X, double* Q, int K) {
 int Surface::gmres_block(int precision, int K, const double* R0, double* T, int nmon, const std::vector<double>& target,
                          int mmax, std::vector<double>& res) {
    BlockWorkspace& B = *blk;
-   cublasHandle_t h = (cublasHandle_t)B.blas;
-   const double one = 1.0, zero = 0.0, minus = -1.0;
    const int64_t vblk = (int64_t)K * n;
    double* V = B.V.get();
    res.assign(K, 0.0);
@@ -291,17 +283,12 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
       const int rows = (j + 1) * K;
       apply_batch(precision, V + j * vblk, B.W.get(), K);
       precond_batch(B.W.get(), B.W.get(), K);
-      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero, B.H.get(),
-                              rows));
-      FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H.get(), rows, &one,
-                              B.W.get(), n));
+      dense::gemm_tn(rows, K, n, 1.0, V, n, B.W.get(), n, 0.0, B.H.get(), rows, B.gwork.get(), stream);
+      dense::gemm_nn(n, K, rows, -1.0, V, n, B.H.get(), rows, 1.0, B.W.get(), n, stream);
       if (reorth) {
-         FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, K, n, &one, V, n, B.W.get(), n, &zero,
-                                 B.H2.get(), rows));
-         FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &minus, V, n, B.H2.get(), rows, &one,
-                                 B.W.get(), n));
-         FFTSVD_BLAS(cublasDgeam(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, K, &one, B.H.get(), rows, &one, B.H2.get(), rows,
-                                 B.H.get(), rows));
+         dense::gemm_tn(rows, K, n, 1.0, V, n, B.W.get(), n, 0.0, B.H2.get(), rows, B.gwork.get(), stream);
+         dense::gemm_nn(n, K, rows, -1.0, V, n, B.H2.get(), rows, 1.0, B.W.get(), n, stream);
+         dense::add(rows, K, B.H.get(), rows, B.H2.get(), rows, B.H.get(), rows, stream);
       }
       FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
       block_qr(B.W.get(), V + (j + 1) * vblk, K);
@@ -366,9 +353,8 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
                                     cudaMemcpyHostToDevice, stream));
    FFTSVD_CUDA(cudaMemcpy2DAsync(B.Y.get(), sizeof(double) * rows, ls.g(), sizeof(double) * ls.ldg(),
                                  sizeof(double) * rows, K, cudaMemcpyHostToDevice, stream));
-   FFTSVD_BLAS(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, K,
-                           &one, B.Rd.get(), ldr, B.Y.get(), rows));
-   FFTSVD_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, K, rows, &one, V, n, B.Y.get(), rows, &one, T, n));
+   dense::trsm_upper_left(rows, K, K, B.Rd.get(), ldr, B.Y.get(), B.Dinv.get(), B.Yo.get(), stream);
+   dense::gemm_nn(n, K, rows, 1.0, V, n, B.Yo.get(), rows, 1.0, T, n, stream);
    FFTSVD_CUDA(cudaStreamSynchronize(stream));  // ls is released with this frame
    return m;
 }

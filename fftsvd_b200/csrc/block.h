@@ -13,13 +13,15 @@ struct BlockWorkspace {
    int64_t n = 0;
    int K = 0;     // columns of a block (a multiple of 8)
    int mmax = 0;  // block steps the basis holds
-   void* blas = nullptr;  // cublasHandle_t
    DevBuf<double> V;                    // mmax + 1 blocks of K x n
    DevBuf<double> W, R0, T;             // K x n
    DevBuf<double> Bc, Xc, Rc, Tc;       // K x n: right-hand sides, iterate, residual, scratch
+   DevBuf<double> Qs;                   // K x n: the block between the two CholQR passes
    DevBuf<double> H, H2;                // (mmax + 1) K x K Gram-Schmidt coefficients
-   DevBuf<double> G, R1, R2, R;         // K x K
-   DevBuf<double> Y;                    // mmax K x K least-squares solution
+   DevBuf<double> G, R1, R2, R, Rinv;   // K x K
+   DevBuf<double> Y, Yo;                // mmax K x K least-squares right-hand side and solution
+   DevBuf<double> Dinv;                 // mmax blocks K x K: inverted diagonal blocks of Rd
+   DevBuf<double> gwork;                // split-K partial products (dense::gemm_tn)
    DevBuf<double> Rd;                   // (mmax K)^2: dense triangular factor of the least squares
    DevBuf<double> scal, part, fac;      // column norms and partial sums, column factors
    DevBuf<int32_t> idx, flag;

@@ -10,6 +10,7 @@
 
 #include "batch.h"
 #include "nbody.h"
+#include "dense.h"
 #include "surface.h"
 
 namespace fftsvd {
@@ -540,6 +541,34 @@ int fftsvd_b200_bounded_wait_selftest(int32_t polls) {
    return FFTSVD_ERR_CUDA;
 }
 long long fftsvd_b200_device_alloc_count(void) { return g_device_allocs.load(); }
+
+int fftsvd_b200_dense_gemm_device(int transpose_a, int64_t m, int32_t n, int64_t k, double alpha, const double* a,
+                                  int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc) {
+   if (m < 0 || n < 0 || k < 0 || !a || !b || !c) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      FFTSVD_REQUIRE(ldc >= m && ldb >= k && lda >= (transpose_a ? k : m), "leading dimensions");
+      if (transpose_a) {
+         FFTSVD_REQUIRE(m <= INT32_MAX, "rows");
+         DevBuf<double> work((size_t)std::max<int64_t>(1, dense::gemm_tn_work((int)m, n, k)));
+         dense::gemm_tn((int)m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, work.get(), nullptr);
+         FFTSVD_CUDA(cudaStreamSynchronize(nullptr));
+      } else {
+         FFTSVD_REQUIRE(k <= INT32_MAX, "inner dimension");
+         dense::gemm_nn(m, n, (int)k, alpha, a, lda, b, ldb, beta, c, ldc, nullptr);
+         FFTSVD_CUDA(cudaStreamSynchronize(nullptr));
+      }
+   });
+}
+
+int fftsvd_b200_dense_trsm_device(int32_t rows, int32_t n, int32_t bs, const double* r, int64_t ldr, double* y,
+                                  double* out) {
+   if (rows < 0 || n < 0 || bs <= 0 || !r || !y || !out || ldr < rows) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      DevBuf<double> dinv((size_t)std::max(1, rows) * bs);
+      dense::trsm_upper_left(rows, n, bs, r, ldr, y, dinv.get(), out, nullptr);
+      FFTSVD_CUDA(cudaStreamSynchronize(nullptr));
+   });
+}
 
 void* fftsvd_b200_surface_stream(const fftsvd_surface* s) { return s ? (void*)s->s.stream : nullptr; }
 

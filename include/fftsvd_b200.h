@@ -404,6 +404,16 @@ int fftsvd_b200_group_energies_device(fftsvd_surface* s, int32_t ngroups, const 
    tensor-core kernels bound their waits.  Returns FFTSVD_ERR_TIMEOUT when the wait gave
    up (the expected outcome; the context stays usable), FFTSVD_ERR_CUDA when it completed. */
 int fftsvd_b200_bounded_wait_selftest(int32_t polls);
+/* The block solve's dense FP64 kernels on device arrays (column-major), synchronous on the
+   legacy default stream.  transpose_a = 0: C (m x n) = alpha A B + beta C with A (m x k);
+   transpose_a = 1: C = alpha A^T B + beta C with A (k x m); B is k x n.  Leading dimensions,
+   m (transpose_a = 0) and k even, A and B 16-byte aligned; C must not overlap A or B. */
+int fftsvd_b200_dense_gemm_device(int transpose_a, int64_t m, int32_t n, int64_t k, double alpha, const double* a,
+                                  int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc);
+/* out (rows x n, ld rows) = R^-1 y for the upper-triangular R (rows x rows, ld ldr), by
+   blocks of bs rows (rows a multiple of an even bs); y is overwritten. */
+int fftsvd_b200_dense_trsm_device(int32_t rows, int32_t n, int32_t bs, const double* r, int64_t ldr, double* y,
+                                  double* out);
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
 /* Device allocations (cudaMalloc calls) made by this library since it was loaded. */
