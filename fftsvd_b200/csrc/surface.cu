@@ -127,7 +127,7 @@ void Preconditioner::apply(const double* r, double* z, cudaStream_t s, bool tran
 // ------------------------------------------------------------------ surface
 
 Surface::~Surface() {
-   blk.reset();  // its cuBLAS handle is bound to the stream
+   blk.reset();  // its events and buffers go before the stream they were used on
    release_step_graphs();
    if (st_host) cudaFreeHost(st_host);
    if (hist_host) cudaFreeHost(hist_host);
