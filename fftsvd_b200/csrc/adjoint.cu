@@ -133,29 +133,33 @@ int Surface::adjoint(int precision, double tol, int maxit, double* energy, doubl
                      fftsvd_solve_info* info) {
    FFTSVD_REQUIRE(geom, "surface has no panel geometry");
    const int nq = num_charges, np = geom->num_panels;
-   DevBuf<double> b(n), u(n), c(n), lam(n), phi(std::max(nq, 1));
+   double* const b = work_buf(kWorkB, n);
+   double* const u = work_buf(kWorkU, n);
+   double* const c = work_buf(kWorkC, n);
+   double* const lam = work_buf(kWorkLam, n);
+   double* const phi = work_buf(kWorkPhi, nq);
    fftsvd_solve_info inf[2] = {};
    // forward: u = A^-1 B q
-   rhs_device(*this, b.get());
-   int st = solve(precision, b.get(), u.get(), tol, maxit, &inf[0]);
+   rhs_device(*this, b);
+   int st = solve(precision, b, u, tol, maxit, &inf[0]);
    if (st != FFTSVD_OK) {
       if (info) info[0] = inf[0];
       return st;
    }
-   reaction_device(*this, u.get(), phi.get());
-   *energy = energy_device(*this, phi.get());
+   reaction_device(*this, u, phi);
+   *energy = energy_device(*this, phi);
    if (nq == 0) {
       if (info) { info[0] = inf[0]; info[1] = inf[1]; }
       return FFTSVD_OK;
    }
    // adjoint: lambda = A^-T L^T q
-   FFTSVD_CUDA(cudaMemsetAsync(c.get(), 0, sizeof(double) * n, stream));
+   FFTSVD_CUDA(cudaMemsetAsync(c, 0, sizeof(double) * n, stream));
    collection_t_kernel<<<(np + kAdjThreads - 1) / kAdjThreads, kAdjThreads, 0, stream>>>(
-       np, geom->panels.get(), geom->phi_row.get(), geom->dphi_row.get(), nq, charge_pos.get(), charge_q.get(), c.get());
+       np, geom->panels.get(), geom->phi_row.get(), geom->dphi_row.get(), nq, charge_pos.get(), charge_q.get(), c);
    FFTSVD_CHECK_LAUNCH();
    transposed = true;
    try {
-      st = solve(precision, c.get(), lam.get(), tol, maxit, &inf[1]);
+      st = solve(precision, c, lam, tol, maxit, &inf[1]);
    } catch (...) {
       transposed = false;
       throw;
@@ -165,16 +169,17 @@ int Surface::adjoint(int precision, double tol, int maxit, double* energy, doubl
    if (st != FFTSVD_OK) return st;
    // per-charge sums
    const int chunks = std::max(1, std::min(kAdjChunks, (np + kAdjPanelTile - 1) / kAdjPanelTile));
-   DevBuf<double> partial((size_t)chunks * nq * kAdjOut), out((size_t)nq * kAdjOut);
+   double* const partial = work_buf(kWorkPartial, (size_t)chunks * nq * kAdjOut);
+   double* const out = work_buf(kWorkOut, (size_t)nq * kAdjOut);
    dim3 grid((nq + kAdjThreads - 1) / kAdjThreads, chunks);
    adjoint_charge_kernel<<<grid, kAdjThreads, 0, stream>>>(np, geom->panels.get(), geom->phi_row.get(),
-                                                           geom->dphi_row.get(), u.get(), lam.get(), nq,
-                                                           charge_pos.get(), partial.get());
+                                                           geom->dphi_row.get(), u, lam, nq, charge_pos.get(),
+                                                           partial);
    FFTSVD_CHECK_LAUNCH();
-   adjoint_reduce_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(nq, chunks, partial.get(), out.get());
+   adjoint_reduce_kernel<<<(nq + 127) / 128, 128, 0, stream>>>(nq, chunks, partial, out);
    FFTSVD_CHECK_LAUNCH();
    std::vector<double> h((size_t)nq * kAdjOut);
-   FFTSVD_CUDA(cudaMemcpyAsync(h.data(), out.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
+   FFTSVD_CUDA(cudaMemcpyAsync(h.data(), out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
    FFTSVD_CUDA(cudaStreamSynchronize(stream));
    const double k = 332.112 / eps_in;
    for (int j = 0; j < nq; j++) {

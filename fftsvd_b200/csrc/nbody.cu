@@ -193,13 +193,13 @@ void reaction_device(Surface& S, const double* sol, double* phi) {
    const int nq = S.num_charges, np = S.geom->num_panels;
    if (nq == 0) return;
    const int chunks = std::max(1, std::min(kReactChunks, (np + kReactPanelTile - 1) / kReactPanelTile));
-   DevBuf<double> partial((size_t)chunks * nq);
+   double* const partial = S.work_buf(Surface::kWorkReact, (size_t)chunks * nq);
    dim3 grid((nq + kReactThreads - 1) / kReactThreads, chunks);
    reaction_partial_kernel<<<grid, kReactThreads, 0, S.stream>>>(np, S.geom->panels.get(), S.geom->phi_row.get(),
                                                                  S.geom->dphi_row.get(), sol, nq,
-                                                                 S.charge_pos.get(), partial.get(), nullptr, 0);
+                                                                 S.charge_pos.get(), partial, nullptr, 0);
    FFTSVD_CHECK_LAUNCH();
-   reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, partial.get(), phi);
+   reaction_reduce_kernel<<<(nq + 255) / 256, 256, 0, S.stream>>>(nq, chunks, partial, phi);
    FFTSVD_CHECK_LAUNCH();
    FFTSVD_CUDA(cudaStreamSynchronize(S.stream));
 }

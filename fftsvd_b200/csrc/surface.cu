@@ -134,6 +134,13 @@ Surface::~Surface() {
    if (stream) cudaStreamDestroy(stream);
 }
 
+double* Surface::work_buf(WorkSlot slot, size_t elems) {
+   DevBuf<double>& b = work[slot];
+   elems = std::max<size_t>(elems, 1);
+   if (b.size() < elems) b.alloc(elems);
+   return b.get();
+}
+
 void Surface::release_step_graphs() {
    for (auto& byprec : step_graphs)
       for (StepGraph& g : byprec) {

@@ -54,6 +54,13 @@ struct Surface {
    // setup statistics (zero for surfaces built from a flat operator)
    fftsvd_surface_stats stats{};
 
+   // Work arrays of the adjoint and of the reaction-potential collection, kept between calls
+   // (grown when a call needs more, never shrunk): allocating and freeing them per call put
+   // cudaMalloc/cudaFree, which synchronise the device, inside every adjoint.
+   enum WorkSlot { kWorkB, kWorkU, kWorkC, kWorkLam, kWorkPhi, kWorkPartial, kWorkOut, kWorkReact, kWorkSlots };
+   DevBuf<double> work[kWorkSlots];
+   double* work_buf(WorkSlot slot, size_t elems);
+
    // GMRES workspace
    int capacity = 0;  // basis vectors
    DevBuf<double> V, H, cs, sn, g, h1, h2, partial, normpart, y;
