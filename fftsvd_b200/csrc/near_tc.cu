@@ -10,12 +10,17 @@
 // K-major as stored).  One CTA of four warps computes one leaf for 128 right-hand
 // sides: the chunks of 32 K values of X and D are split into TF32 heads and tails
 // (split_tf32) and staged in shared memory in the K-major layout of tcgen05.cuh; one
-// thread issues kind::tf32 MMAs into a TMEM accumulator of 128 lanes x nrows columns,
-// three per K-step (head x head, head x tail, tail x head: FP32-level products with
-// FP32 accumulation, Ootomo and Yokota 2022); the chunk's commit arrives on an
-// mbarrier that every thread waits on (bounded) before the buffers are refilled.  The
-// epilogue reads the accumulator with tcgen05.ld (thread t = right-hand side t), adds
-// the jump term and writes y.
+// thread issues kind::tf32 MMAs, three per K-step (head x head, head x tail, tail x head:
+// FP32-level products, Ootomo and Yokota 2022); the chunk's commit arrives on an mbarrier
+// that every thread waits on (bounded) before the buffers are refilled.
+//
+// Accumulation: a tensor-core accumulator summed over a long K loses accuracy (measured on
+// the B200 at K = 300: 2.2e-6 relative against 3e-7 for a sequential FP32 sum), while one
+// K-chunk of 32 accumulates at FP32 level.  The chunks are therefore dealt round-robin to
+// up to kTcAccCols / nrows accumulators of 128 lanes x nrows columns in TMEM (a new chunk
+// starts a fresh accumulator while there are unused ones), and the epilogue reads them
+// with tcgen05.ld (thread t = right-hand side t), sums them on the CUDA cores, adds the
+// jump term and writes y.
 //
 // The densities come from xsd_t, the joined panel values transposed to [panel][rhs]
 // (transpose_xsd_kernel), so the staging loads of X are coalesced over right-hand sides.
@@ -32,6 +37,7 @@ namespace {
 
 constexpr int kTcRhs = 128;   // right-hand sides per CTA: the MMA's M
 constexpr int kTcK = 32;      // K values per staged chunk (four K-steps of 8)
+constexpr int kTcAccCols = 128;  // TMEM columns of the chunk accumulators of one CTA (four CTAs per SM)
 constexpr uint32_t kTcPolls = 1u << 24;  // bound of every mbarrier wait
 
 // xsd_t[p * ld + r] = xsd[r * panels + p] for panel p < np, right-hand side r < nrhs;
@@ -76,8 +82,11 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
    const LeafDesc L = leaves[blockIdx.x];
    const int rhs = blockIdx.y * kTcRhs + t;
    const int nr = L.nrows, np = max(8, (nr + 7) & ~7), kdim = 2 * L.ncols;
+   const int nchunks = (kdim + kTcK - 1) / kTcK;
+   const int acc_stride = (np + 15) & ~15;                          // TMEM columns between accumulators
+   const int nacc = max(1, min(nchunks, kTcAccCols / acc_stride));  // chunk accumulators
    uint32_t ncols_tmem = 32;
-   while ((int)ncols_tmem < np) ncols_tmem <<= 1;
+   while ((int)ncols_tmem < nacc * acc_stride) ncols_tmem <<= 1;
    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tslot), ncols_tmem);
    if (t == 0) {
       tc::mbar_init(tc::smem_addr(&mbar[0]), 1);
@@ -96,7 +105,6 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
    const uint32_t tmem = tslot;
    const uint32_t idesc = tc::idesc_tf32(kTcRhs, np);
    const float2* drow = d + L.d_off;
-   const int nchunks = (kdim + kTcK - 1) / kTcK;
    bool ok = true;
    int committed = -1;  // last chunk whose MMAs were committed
    // Chunk k is staged into stage k & 1 while the MMAs of chunk k - 1 run on the other stage;
@@ -164,14 +172,15 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
          tc::fence_after_sync();
          const uint32_t a_h = tc::smem_addr(Ah), a_l = tc::smem_addr(Al);
          const uint32_t b_h = tc::smem_addr(Bh), b_l = tc::smem_addr(Bl);
+         const uint32_t acc_col = tmem + (uint32_t)((chunk % nacc) * acc_stride);
 #pragma unroll
          for (int s = 0; s < kTcK / 8; s++) {
             const uint32_t ao = (uint32_t)s * (2 * kTcRhs * 16), bo = (uint32_t)s * (2 * np * 16);
             const uint64_t ah = tc::smem_desc(a_h + ao, kTcRhs * 16, 128), al = tc::smem_desc(a_l + ao, kTcRhs * 16, 128);
             const uint64_t bh = tc::smem_desc(b_h + bo, np * 16, 128), bl = tc::smem_desc(b_l + bo, np * 16, 128);
-            tc::mma_tf32(tmem, ah, bh, idesc, (chunk > 0 || s > 0) ? 1u : 0u);
-            tc::mma_tf32(tmem, ah, bl, idesc, 1u);
-            tc::mma_tf32(tmem, al, bh, idesc, 1u);
+            tc::mma_tf32(acc_col, ah, bh, idesc, (chunk >= nacc || s > 0) ? 1u : 0u);
+            tc::mma_tf32(acc_col, ah, bl, idesc, 1u);
+            tc::mma_tf32(acc_col, al, bh, idesc, 1u);
          }
          tc::commit(tc::smem_addr(&mbar[st]));  // arrives when every MMA issued so far completed
       }
@@ -193,9 +202,15 @@ __global__ void __launch_bounds__(kTcRhs) near_tc_kernel(
       // every lane takes part in the warp-wide TMEM loads; lanes past nrhs only skip the stores
       const double* xr = x + (int64_t)rhs * ldn;
       double* yr = y + (int64_t)rhs * ldn;
+      const int used = min(nacc, nchunks);  // accumulators that hold a chunk
       for (int c0 = 0; c0 < np; c0 += 8) {
          float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-         if (kdim > 0) tc::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
+         for (int a = 0; a < used; a++) {
+            float part[8];
+            tc::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(a * acc_stride + c0), part);
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[j] += part[j];
+         }
          if (rhs < nrhs) {
 #pragma unroll
             for (int j = 0; j < 8; j++) {

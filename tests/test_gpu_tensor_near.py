@@ -1,11 +1,11 @@
 """The multi-vector FP32 matvec with its near field on the tensor cores
 (fftsvd_b200_matvec_batch_tensor_device: kind::tf32 MMAs with three-product
-splitting, 128 right-hand sides per CTA) against the CUDA-core multi-vector
-matvec and the FP64 matvec.  Three TF32 products with FP32 accumulation give
-FP32-level products, so each column matches the CUDA-core FP32 column to FP32
-rounding (bar 1e-5, relative 2-norm; one TF32 product alone would be near 3e-4) and
-the FP64 matvec to the FP32 operator's
-own error (bar 2e-5, the bar of the FP32 operator against the reference)."""
+splitting and one TMEM accumulator per K-chunk of 32, 128 right-hand sides per CTA)
+against the CUDA-core multi-vector matvec and the FP64 matvec.  Three TF32 products
+accumulated over short chunks give FP32-level results: measured on a 20 480-panel
+blob, 3.5e-7 against the CUDA-core FP32 matvec and 3.3e-7 against FP64 (the FP32
+operator's own error is 1.3e-7), where one accumulator over the whole K gave 1.7e-6.
+Bars: 2e-6 per column (relative 2-norm) against both."""
 import ctypes as C
 
 import numpy as np
@@ -44,7 +44,7 @@ def test_tensor_near_field_matches_cuda_core_matvec(surface, nrhs):
     yt, yc, x = Yt.cpu().numpy(), Yc.cpu().numpy(), X.cpu().numpy()
     for c in range(nrhs):
         e = np.linalg.norm(yt[c] - yc[c]) / np.linalg.norm(yc[c])
-        assert e < 1e-5, (c, e)
+        assert e < 2e-6, (c, e)
     for c in (0, nrhs // 2, nrhs - 1):
         y64 = s.matvec(x[c], "fp64")
-        assert np.linalg.norm(yt[c] - y64) / np.linalg.norm(y64) < 2e-5
+        assert np.linalg.norm(yt[c] - y64) / np.linalg.norm(y64) < 2e-6
