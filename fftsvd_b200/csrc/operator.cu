@@ -777,6 +777,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       g.count++;
       g.smem_elems = std::max(g.smem_elems, src_need(L.src[i]));
       g.max_rank = std::max(g.max_rank, L.src[i].r);
+      g.units += L.src[i].m;
       const int n = L.src[i].n, Np = 2 * n - 1;
       g.batch_shared = std::max(g.batch_shared, 2 * std::min(L.src[i].m, 1024) + 2 * Np);
       g.batch_per_rhs = std::max(g.batch_per_rhs, 2 * L.src[i].r + n * n * n + 2 * n * n * n + 2 * n * Np * n);
@@ -787,6 +788,7 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
       g.count++;
       g.smem_elems = std::max(g.smem_elems, dst_need(L.dst[i]));
       g.max_rank = std::max(g.max_rank, L.dst[i].r);
+      g.units += L.dst[i].p;
       const int n = L.dst[i].n, Np = 2 * n - 1;
       g.batch_shared = std::max(g.batch_shared, 2 * Np);
       g.batch_per_rhs = std::max(g.batch_per_rhs, 2 * Np * Np * n + 2 * n * Np * n + 2 * n * n * n + n * n * n +
@@ -2630,7 +2632,7 @@ void DeviceOperator<T>::stage_ms(float* ms) const {
 template <typename T>
 bool DeviceOperator<T>::warp_path(const LaunchGroup& g) const {
    return g.n >= kWarpMinN && g.n <= kWarpMaxN && g.max_rank >= 1 && g.max_rank <= kWarpMaxRank &&
-          g.count >= warp_min_cubes_;
+          g.count >= warp_min_cubes_ && g.units <= (int64_t)kWarpMaxMeanUnits * g.count;
 }
 
 template <typename T>

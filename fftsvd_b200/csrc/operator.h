@@ -147,6 +147,7 @@ struct LaunchGroup {
    int count = 0;
    int smem_elems = 0;  // in units of the operator element type
    int max_rank = 0;    // largest row (sources) or column (destinations) rank
+   int64_t units = 0;   // panels (sources) or points (destinations) of all the group's cubes
    // shared memory of a block that serves several right-hand sides: batch_shared +
    // right-hand sides x batch_per_rhs elements
    int batch_shared = 0, batch_per_rhs = 0;
@@ -175,7 +176,12 @@ constexpr int kMaxBatch = 65535; // grid y limit
 constexpr int kWarpMinN = 3;
 constexpr int kWarpMaxN = 5;
 constexpr int kWarpMaxRank = 32;
-constexpr int kWarpMinCubes = 4096;  // fewer cubes leave too few warps per SM to hide latency
+constexpr int kWarpMinCubes = 2000;  // fewer cubes leave too few warps per SM to hide latency
+// A warp per cube walks the cube's panels 32 at a time; with many panels per cube a block per
+// cube spreads them over more threads (B200: the 5^3 grid with 75 panels per cube ran the
+// single solve 1.2 % and the 256-column block solve 4 % faster on warps; with 284 panels
+// per cube the single solve ran 1.3 % slower).
+constexpr int kWarpMaxMeanUnits = 160;
 
 // Algorithmic bytes of each matvec kernel [join, far_forward, translate, far_backward, near]:
 // elems * (operator element size) + fixed (FP64 vectors and int32 indices).
