@@ -864,6 +864,19 @@ static int far_threads(int n) {
    const int pg = (2 * n - 1) * (2 * n - 1) * n;
    return pg <= 256 ? 128 : pg <= 512 ? 256 : 512;
 }
+// Block size of a group's block-per-cube launch: a power of two from 64 to 512 covering a
+// quarter of the spectrum and half of the cube's mean panel (or point) count.  Measured on the
+// B200: on the 81 920-panel blob the 6^3 grid (156 panels per cube) ran the mixed solve 2 %
+// faster on 256 threads than on 512; on the 327 680-panel blob, whose coarse cubes hold
+// 284 to 5 851 panels, halving the blocks made the solve 1.6 % slower.
+static int far_threads(const LaunchGroup& g) {
+   const int pg = (2 * g.n - 1) * (2 * g.n - 1) * g.n;
+   const int64_t mean = g.count > 0 ? g.units / g.count : 0;
+   const int64_t want = std::max<int64_t>(pg / 4, mean / 2);
+   int t = 64;
+   while (t < want && t < kFarThreads) t *= 2;
+   return t;
+}
 constexpr int kChunk = 1024;
 
 // right-hand sides per block of the batched far-field kernels
@@ -1333,7 +1346,7 @@ __global__ void __launch_bounds__(kFarThreads) far_backward_kernel(
    }
 }
 
-constexpr int kWarpCubes = 4;  // cubes (warps) per block
+constexpr int kWarpCubes = 2;  // cubes (warps) per block (B200: 0.5 % faster solves than 4)
 constexpr int kWarpThreads = 32 * kWarpCubes;
 
 // ---- transposed operator (y = A^T x), for the adjoint solve
@@ -1584,7 +1597,7 @@ struct SmallGrid {
 };
 
 template <typename T, int N>
-__global__ void __launch_bounds__(kWarpThreads, 12) far_forward_warp_kernel(
+__global__ void __launch_bounds__(kWarpThreads, 24) far_forward_warp_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs) {
@@ -1815,7 +1828,7 @@ struct Prefetch {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forward_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 16 : 8) far_forward_n4_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ xsd, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ spectra, BatchStrides bs,
@@ -1952,7 +1965,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forw
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_backward_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 16 : 8) far_backward_n4_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points,
     const typename Vec2<T>::type* __restrict__ translated, const T* __restrict__ uti, const T* __restrict__ ucm,
     T* __restrict__ staging, int64_t total_points, BatchStrides bs, Prefetch pre) {
@@ -2067,7 +2080,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_back
 // a time), g = UTI^T a at q = lane and lane + 32, F = r2c DFT of g into the cube's
 // translated-spectrum slot
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_backward_t_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 16 : 8) far_backward_t_n4_kernel(
     const DstDesc* __restrict__ cubes, int count, const int32_t* __restrict__ dst_points, const T* __restrict__ zt,
     const T* __restrict__ uti, const T* __restrict__ ucm, typename Vec2<T>::type* __restrict__ out_spectra) {
    using T2 = typename Vec2<T>::type;
@@ -2166,7 +2179,7 @@ __global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_back
 // a_j = {PV_s[j] . g, PV_d[j] . g}, and per panel {VT^T a_s, VT^T a_d} into the level's
 // staging row
 template <typename T>
-__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 8 : 4) far_forward_t_n4_kernel(
+__global__ void __launch_bounds__(kWarpThreads, sizeof(T) == 4 ? 16 : 8) far_forward_t_n4_kernel(
     const SrcDesc* __restrict__ cubes, int count, const int32_t* __restrict__ src_panels,
     const typename Vec2<T>::type* __restrict__ in_spectra, const T* __restrict__ vt,
     const typename Vec2<T>::type* __restrict__ pv, typename Vec2<T>::type* __restrict__ staging,
@@ -2655,11 +2668,11 @@ void DeviceOperator<T>::launch_forward(const LaunchGroup& g, const Bufs& b, cuda
       constexpr int RB = far_rb<T>();
       const int smem_b = far_batch_smem(g, RB, sizeof(T));
       if (b.nrhs % RB == 0 && smem_b <= smem_optin_) {  // RB right-hand sides per block
-         far_forward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g.n), smem_b, stream>>>(
+         far_forward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g), smem_b, stream>>>(
              src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
       } else {
          const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-         far_forward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
+         far_forward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g), smem, stream>>>(
              src_.get() + g.begin, src_panels_.get(), b.xsd, vt_.get(), pv_.get(), b.spectra, b.bs);
       }
    }
@@ -2809,12 +2822,12 @@ void DeviceOperator<T>::launch_backward(const LaunchGroup& g, const Bufs& b, cud
       constexpr int RB = far_rb<T>();
       const int smem_b = far_batch_smem(g, RB, sizeof(T));
       if (b.nrhs % RB == 0 && smem_b <= smem_optin_) {  // RB right-hand sides per block
-         far_backward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g.n), smem_b, stream>>>(
+         far_backward_kernel<T, RB><<<g.count * (b.nrhs / RB), far_threads(g), smem_b, stream>>>(
              dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_,
              b.bs);
       } else {
          const int smem = (int)(g.smem_elems * sizeof(T) + 128);
-         far_backward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g.n), smem, stream>>>(
+         far_backward_kernel<T, 1><<<g.count * b.nrhs, far_threads(g), smem, stream>>>(
              dst_.get() + g.begin, dst_points_.get(), b.translated, uti_.get(), u_.get(), b.staging, total_points_,
              b.bs);
       }
