@@ -12,12 +12,13 @@
 // Device: the multi-vector matvec and preconditioner of the batch, the block
 // Gram-Schmidt and the products with the basis as FP64 tensor-core GEMMs (dense.cu), the
 // block QR as CholQR2 (Gram matrix, Cholesky factor in a one-block kernel, product with
-// the factor's inverse; twice), the final block triangular solve (dense.cu).  Gram-Schmidt is one classical pass while no
-// column of a new block loses more than five digits in it (the new block is then
-// orthogonal to the basis to about 1e-11, far below what a solve to 1e-6 needs), two
-// passes from the first step where one does.  Host: the block
-// Hessenberg least-squares problem (block_ls.cpp), updated for step j while the device
-// runs step j + 1, so its cost hides behind the matvec.
+// the factor's inverse; twice), the final block triangular solve (dense.cu).  Gram-Schmidt
+// is one classical pass while no column of a new block loses more than five digits in it
+// (the new block is then orthogonal to the basis to about 1e-11, far below what a solve to
+// 1e-6 needs), two passes from the first step where one does.  The block Hessenberg
+// least-squares problem is updated on the device too (block_ls.cu), on a second stream:
+// step j's update runs while the main stream runs step j + 1, and the host reads back
+// only the residual estimates, the block's norms and the rank flag (3K + 1 numbers).
 //
 // Refinement: each pass gathers the columns still above the tolerance, scales their
 // residuals to unit norm, pads them to a multiple of 8 with seeded random directions
@@ -180,11 +181,13 @@ int pad8(int k) { return (k + kBatchGroup - 1) / kBatchGroup * kBatchGroup; }
 }  // namespace
 
 BlockWorkspace::~BlockWorkspace() {
+   if (ls_stream) cudaStreamSynchronize(ls_stream);
    for (auto& e : done)
       if (e) cudaEventDestroy(e);
-   for (auto& p : hbuf)
-      if (p) cudaFreeHost(p);
-   for (auto& p : rbuf)
+   for (auto& e : ls_done)
+      if (e) cudaEventDestroy(e);
+   if (ls_stream) cudaStreamDestroy(ls_stream);
+   for (auto& p : stat_h)
       if (p) cudaFreeHost(p);
    if (flag_h) cudaFreeHost(flag_h);
 }
@@ -193,6 +196,12 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
    (void)stream;
    if (!flag_h) {
       for (auto& e : done) FFTSVD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      for (auto& e : ls_done) FFTSVD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      // the least-squares kernels take few SMs for a short time; the greatest priority lets
+      // them start while the next step's matvec fills the device
+      int least = 0, greatest = 0;
+      FFTSVD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      FFTSVD_CUDA(cudaStreamCreateWithPriority(&ls_stream, cudaStreamNonBlocking, greatest));
       FFTSVD_CUDA(cudaMallocHost(&flag_h, 2 * sizeof(int)));
       FFTSVD_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)chol_smem(kBlockMax)));
@@ -216,21 +225,21 @@ void BlockWorkspace::ensure(int64_t n_, int K_, int mmax_, cudaStream_t stream) 
    for (int j = 1; j <= mmax; j++) wmax = std::max(wmax, dense::gemm_tn_work(j * K, K, n));
    gwork.alloc((size_t)std::max<int64_t>(wmax, 1));
    Rd.alloc((size_t)mmax * K * (size_t)mmax * K);
+   Lv.alloc((size_t)mmax * 2 * kk);
+   Ltau.alloc((size_t)mmax * K);
+   Lg.alloc((size_t)(mmax + 1) * kk);
+   for (int s = 0; s < 2; s++) {
+      Lcol[s].alloc((size_t)(mmax + 1) * kk);
+      Lstat[s].alloc((size_t)3 * K + 1);
+      if (stat_h[s]) cudaFreeHost(stat_h[s]);
+      stat_h[s] = nullptr;
+      FFTSVD_CUDA(cudaMallocHost(&stat_h[s], sizeof(double) * ((size_t)3 * K + 1)));
+   }
    scal.alloc(K);
    part.alloc((size_t)K * vec_blocks(n));
    fac.alloc(K);
    idx.alloc(K);
    flag.alloc(1);
-   for (auto& p : hbuf) {
-      if (p) cudaFreeHost(p);
-      p = nullptr;
-      FFTSVD_CUDA(cudaMallocHost(&p, sizeof(double) * (size_t)(mmax + 1) * kk));
-   }
-   for (auto& p : rbuf) {
-      if (p) cudaFreeHost(p);
-      p = nullptr;
-      FFTSVD_CUDA(cudaMallocHost(&p, sizeof(double) * kk));
-   }
 }
 
 // Q R = X (n x K, both column-major with ld n; X may be Q) by CholQR2: twice the Gram
@@ -273,14 +282,18 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
    FFTSVD_CUDA(cudaMemcpyAsync(B.flag_h, B.flag.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
    FFTSVD_CUDA(cudaStreamSynchronize(stream));
    if (B.flag_h[0]) return 0;
-   BlockLeastSquares ls;
-   ls.init(K, mmax, S0.data());
+   // least squares on the device (block_ls.h): the transformed right-hand side starts as S0
+   const int64_t ldl = (int64_t)(B.mmax + 1) * B.K;  // rows of Lg and Lcol
+   const int64_t ldr = (int64_t)B.mmax * B.K;        // rows of Rd
+   lsq::init(K, B.R.get(), B.Lg.get(), ldl, stream);
    // step j: W = P^-1 A V_j, block Gram-Schmidt against V_0 .. V_j (a second pass once
-   // `reorth` is set), V_{j+1} R = W; the coefficients, R and the rank flag then go to the
-   // pinned host slot j & 1
+   // `reorth` is set), V_{j+1} R = W; the coefficients, R and the rank flag are gathered
+   // into slot j & 1, and the least-squares update of step j then runs on the side stream
+   // while the main stream goes on with step j + 1
    bool reorth = false;
    auto issue = [&](int j) {
       const int rows = (j + 1) * K;
+      const int slot = j & 1;
       apply_batch(precision, V + j * vblk, B.W.get(), K);
       precond_batch(B.W.get(), B.W.get(), K);
       dense::gemm_tn(rows, K, n, 1.0, V, n, B.W.get(), n, 0.0, B.H.get(), rows, B.gwork.get(), stream);
@@ -292,12 +305,15 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
       }
       FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
       block_qr(B.W.get(), V + (j + 1) * vblk, K);
-      FFTSVD_CUDA(cudaMemcpyAsync(B.hbuf[j & 1], B.H.get(), sizeof(double) * (size_t)rows * K,
-                                  cudaMemcpyDeviceToHost, stream));
-      FFTSVD_CUDA(cudaMemcpyAsync(B.rbuf[j & 1], B.R.get(), sizeof(double) * (size_t)K * K, cudaMemcpyDeviceToHost,
-                                  stream));
-      FFTSVD_CUDA(cudaMemcpyAsync(B.flag_h + (j & 1), B.flag.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-      FFTSVD_CUDA(cudaEventRecord(B.done[j & 1], stream));
+      lsq::gather(j, K, B.H.get(), rows, B.R.get(), K, B.flag.get(), B.Lcol[slot].get(), ldl, B.Lstat[slot].get(),
+                  stream);
+      FFTSVD_CUDA(cudaEventRecord(B.done[slot], stream));
+      FFTSVD_CUDA(cudaStreamWaitEvent(B.ls_stream, B.done[slot], 0));
+      lsq::step(j, K, B.Lcol[slot].get(), ldl, B.Lv.get(), B.Ltau.get(), B.Lg.get(), ldl, B.Rd.get(), ldr,
+                B.Lstat[slot].get(), B.ls_stream);
+      FFTSVD_CUDA(cudaMemcpyAsync(B.stat_h[slot], B.Lstat[slot].get(), sizeof(double) * (3 * (size_t)K + 1),
+                                  cudaMemcpyDeviceToHost, B.ls_stream));
+      FFTSVD_CUDA(cudaEventRecord(B.ls_done[slot], B.ls_stream));
    };
    // residual estimates after the last two steps (before any step: the columns' norms)
    std::vector<double> prev(K), prev2(K);
@@ -321,17 +337,14 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
    issued = 1;
    for (int j = 0; j < mmax; j++) {
       if (issued == j + 1 && j + 1 < mmax && speculate(j)) issue(issued++);
-      FFTSVD_CUDA(cudaEventSynchronize(B.done[j & 1]));
-      if (B.flag_h[j & 1]) break;  // V_{j+1} is not a basis: keep the first j blocks
-      ls.add_column(B.hbuf[j & 1], B.rbuf[j & 1], res.data());
+      FFTSVD_CUDA(cudaEventSynchronize(B.ls_done[j & 1]));
+      const double* st = B.stat_h[j & 1];
+      if (st[3 * K] != 0.0) break;  // V_{j+1} is not a basis: keep the first j blocks
+      std::copy(st, st + K, res.begin());
       m = j + 1;
       // the new block's norms after the projection against those before it
       for (int c = 0; c < K && !reorth; c++) {
-         const double* hc = B.hbuf[j & 1] + (size_t)c * (j + 1) * K;
-         const double* rc = B.rbuf[j & 1] + (size_t)c * K;
-         double sh = 0.0, sr = 0.0;
-         for (int r = 0; r < (j + 1) * K; r++) sh += hc[r] * hc[r];
-         for (int r = 0; r <= c; r++) sr += rc[r] * rc[r];
+         const double sh = st[K + c], sr = st[2 * K + c];
          if (sr < kReorthRatio * kReorthRatio * (sh + sr)) reorth = true;
       }
       bool all = true;
@@ -341,21 +354,17 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
       prev = res;
       if (issued == j + 1 && j + 1 < mmax) issue(issued++);
    }
-   FFTSVD_CUDA(cudaStreamSynchronize(stream));  // a speculative step may still run
+   // a speculative step and its least-squares update may still run; neither writes the
+   // rows and block columns of the first m steps
+   FFTSVD_CUDA(cudaStreamSynchronize(stream));
+   FFTSVD_CUDA(cudaStreamSynchronize(B.ls_stream));
    if (m == 0) return 0;
-   // Y = R^-1 g_top on the device: the triangular factor's block columns into the dense
-   // upper triangle Rd (ld mmax K), g_top into Y (ld mK)
+   // Y = R^-1 g_top: g's first mK rows into Y (ld mK), block triangular solve on Rd
    const int rows = m * K;
-   const int64_t ldr = (int64_t)B.mmax * B.K;
-   for (int j = 0; j < m; j++)
-      FFTSVD_CUDA(cudaMemcpy2DAsync(B.Rd.get() + (int64_t)j * K * ldr, sizeof(double) * ldr, ls.rcol(j),
-                                    sizeof(double) * (j + 1) * K, sizeof(double) * (j + 1) * K, K,
-                                    cudaMemcpyHostToDevice, stream));
-   FFTSVD_CUDA(cudaMemcpy2DAsync(B.Y.get(), sizeof(double) * rows, ls.g(), sizeof(double) * ls.ldg(),
-                                 sizeof(double) * rows, K, cudaMemcpyHostToDevice, stream));
+   FFTSVD_CUDA(cudaMemcpy2DAsync(B.Y.get(), sizeof(double) * rows, B.Lg.get(), sizeof(double) * ldl,
+                                 sizeof(double) * rows, K, cudaMemcpyDeviceToDevice, stream));
    dense::trsm_upper_left(rows, K, K, B.Rd.get(), ldr, B.Y.get(), B.Dinv.get(), B.Yo.get(), stream);
    dense::gemm_nn(n, K, rows, 1.0, V, n, B.Yo.get(), rows, 1.0, T, n, stream);
-   FFTSVD_CUDA(cudaStreamSynchronize(stream));  // ls is released with this frame
    return m;
 }
 
@@ -383,11 +392,12 @@ int Surface::solve_block(int precision, int k, const double* rhs, double* x, dou
       const int nc = std::min(kBlockMax, k - c0), ncp = pad8(nc);
       // basis: up to maxit blocks (at most 64), as many as a third of the device memory
       // that is free or already held by the basis allows, counting the mmax + 11 blocks of
-      // K x n (basis and work vectors) and the dense (mmax K)^2 least-squares factor
+      // K x n (basis and work vectors), the dense (mmax K)^2 least-squares factor and the
+      // least-squares update's 5 K^2 per block (reflectors, right-hand side, column slots)
       size_t free_b = 0, total_b = 0;
       FFTSVD_CUDA(cudaMemGetInfo(&free_b, &total_b));
       if (blk->n == n) free_b += blk->V.bytes() + blk->Rd.bytes();
-      const size_t per_blk = sizeof(double) * (size_t)ncp * n;
+      const size_t per_blk = sizeof(double) * ((size_t)ncp * n + 5 * (size_t)ncp * ncp);
       int mmax = std::max(1, std::min(maxit, 64));
       while (mmax > 1 && (mmax + 11) * per_blk + sizeof(double) * (size_t)mmax * ncp * (size_t)mmax * ncp > free_b / 3)
          mmax--;

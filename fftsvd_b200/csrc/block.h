@@ -23,12 +23,16 @@ struct BlockWorkspace {
    DevBuf<double> Dinv;                 // mmax blocks K x K: inverted diagonal blocks of Rd
    DevBuf<double> gwork;                // split-K partial products (dense::gemm_tn)
    DevBuf<double> Rd;                   // (mmax K)^2: dense triangular factor of the least squares
+   // least squares (block_ls.h): reflectors, their scalars, the transformed right-hand side
+   // ((mmax + 1) K x K), two slots of the block column being transformed and of its statistics
+   DevBuf<double> Lv, Ltau, Lg, Lcol[2], Lstat[2];
    DevBuf<double> scal, part, fac;      // column norms and partial sums, column factors
    DevBuf<int32_t> idx, flag;
-   cudaEvent_t done[2] = {nullptr, nullptr};
-   double* hbuf[2] = {nullptr, nullptr};  // pinned: coefficients of the last two steps
-   double* rbuf[2] = {nullptr, nullptr};  // pinned: their R blocks
-   int* flag_h = nullptr;                 // pinned: their rank flags
+   cudaStream_t ls_stream = nullptr;        // the least-squares updates, overlapped with the next step
+   cudaEvent_t done[2] = {nullptr, nullptr};     // step j's column gathered (slot j & 1)
+   cudaEvent_t ls_done[2] = {nullptr, nullptr};  // step j's least-squares update and statistics copied
+   double* stat_h[2] = {nullptr, nullptr};  // pinned: statistics of the last two steps (3K + 1)
+   int* flag_h = nullptr;                   // pinned: rank flag of the first block
    BlockWorkspace() = default;
    BlockWorkspace(const BlockWorkspace&) = delete;
    BlockWorkspace& operator=(const BlockWorkspace&) = delete;

@@ -10,6 +10,8 @@
 
 #include "batch.h"
 #include "nbody.h"
+#include "block.h"
+#include "block_ls.h"
 #include "dense.h"
 #include "surface.h"
 
@@ -573,6 +575,27 @@ int fftsvd_b200_dense_trsm_device(int32_t rows, int32_t n, int32_t bs, const dou
    return guarded([&] {
       DevBuf<double> dinv((size_t)std::max(1, rows) * bs);
       dense::trsm_upper_left(rows, n, bs, r, ldr, y, dinv.get(), out, nullptr);
+      FFTSVD_CUDA(cudaStreamSynchronize(nullptr));
+   });
+}
+
+int fftsvd_b200_block_ls_device(int32_t k, int32_t m, const double* s0, const double* hbar, double* res, double* r,
+                                double* gtop) {
+   if (k <= 0 || k > kBlockMax || m <= 0 || !s0 || !hbar || !res || !r || !gtop) return FFTSVD_ERR_ARGUMENT;
+   return guarded([&] {
+      const int64_t K = k, ldh = (int64_t)(m + 1) * K, cols = (int64_t)m * K;
+      DevBuf<double> V((size_t)m * 2 * K * K), tau((size_t)m * K), g((size_t)ldh * K), col((size_t)ldh * K),
+          stat((size_t)3 * K + 1);
+      lsq::init(k, s0, g.get(), ldh, nullptr);
+      for (int j = 0; j < m; j++) {
+         const double* h = hbar + (int64_t)j * K * ldh;
+         lsq::gather(j, k, h, ldh, h + (int64_t)(j + 1) * K, ldh, nullptr, col.get(), ldh, stat.get(), nullptr);
+         lsq::step(j, k, col.get(), ldh, V.get(), tau.get(), g.get(), ldh, r, cols, stat.get(), nullptr);
+         FFTSVD_CUDA(cudaMemcpyAsync(res + (int64_t)j * K, stat.get(), sizeof(double) * K, cudaMemcpyDeviceToDevice,
+                                     nullptr));
+      }
+      FFTSVD_CUDA(cudaMemcpy2DAsync(gtop, sizeof(double) * cols, g.get(), sizeof(double) * ldh, sizeof(double) * cols,
+                                    K, cudaMemcpyDeviceToDevice, nullptr));
       FFTSVD_CUDA(cudaStreamSynchronize(nullptr));
    });
 }

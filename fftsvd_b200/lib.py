@@ -31,7 +31,7 @@ EXPORTED = [
     "fftsvd_b200_host_operator_timings", "fftsvd_b200_host_operator_precond", "fftsvd_b200_host_operator_free",
     "fftsvd_b200_matvec_kernel_bytes", "fftsvd_b200_translate_smem_bytes", "fftsvd_b200_profile_matvec", "fftsvd_b200_surface_stream",
     "fftsvd_b200_launch_count", "fftsvd_b200_device_alloc_count", "fftsvd_b200_bounded_wait_selftest", "fftsvd_b200_dense_gemm_device",
-    "fftsvd_b200_dense_trsm_device", "fftsvd_b200_reaction_potentials_noalloc",
+    "fftsvd_b200_dense_trsm_device", "fftsvd_b200_block_ls_device", "fftsvd_b200_reaction_potentials_noalloc",
     "solveSurfaceOperator", "generateRHS",
     "collectPotentials",
     "fftsvd_b200_matvec_batch_device", "fftsvd_b200_matvec_batch_tensor_device", "fftsvd_b200_solve_batch_device",
@@ -103,6 +103,8 @@ def load():
                                                   C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64]
     lib.fftsvd_b200_dense_trsm_device.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                                   C.c_void_p]
+    lib.fftsvd_b200_block_ls_device.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p]
     lib.fftsvd_b200_reaction_potentials_noalloc.argtypes = [sp, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_matvec_batch_device.argtypes = [sp, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
     lib.fftsvd_b200_matvec_batch_tensor_device.argtypes = [sp, C.c_int32, C.c_void_p, C.c_void_p]

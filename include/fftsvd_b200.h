@@ -414,6 +414,16 @@ int fftsvd_b200_dense_gemm_device(int transpose_a, int64_t m, int32_t n, int64_t
    blocks of bs rows (rows a multiple of an even bs); y is overwritten. */
 int fftsvd_b200_dense_trsm_device(int32_t rows, int32_t n, int32_t bs, const double* r, int64_t ldr, double* y,
                                   double* out);
+/* The block solve's least-squares update on device arrays (column-major), synchronous on
+   the legacy default stream: s0 (k x k, upper triangle read) is the first block's factor,
+   hbar ((m+1)k x mk) the block upper Hessenberg matrix, whose block columns are fed one at
+   a time (rows 0 .. (j+2)k of block column j are read; the k x k block below the diagonal
+   block is upper triangular).  After block column j, res[j k + c] is the residual norm of
+   min || E1 s0 - Hbar_j Y || in column c; r (mk x mk) receives the triangular factor's
+   upper triangle and gtop (mk x k) the transformed right-hand side, so Y = r^-1 gtop.
+   k <= 256. */
+int fftsvd_b200_block_ls_device(int32_t k, int32_t m, const double* s0, const double* hbar, double* res, double* r,
+                                double* gtop);
 /* Kernel launches issued by this library since it was loaded. */
 long long fftsvd_b200_launch_count(void);
 /* Device allocations (cudaMalloc calls) made by this library since it was loaded. */
