@@ -2,8 +2,11 @@
 //
 // One warp owns one column of a 2K-row window (K <= 256): lane l keeps rows q 32 + l,
 // q < 16, in registers.  A reflector H = I - tau v v^T costs the warp one masked dot
-// product, a shuffle reduction and one update, with v read through the read-only cache
-// (the warps of a block read the same v, so it stays in L1).  The transformation of a
+// product, a shuffle reduction and one update.  The warps of a block apply the same
+// reflectors to their columns, so the block copies the vectors and their scalars into
+// shared memory eight at a time, the next eight while the current ones are applied (a
+// warp that read each vector from global memory waited on two dependent loads per
+// reflector).  The transformation of a
 // block column by the earlier blocks is independent per column: one launch applies every
 // earlier block to all K columns, block after block (block i's window is rows
 // iK .. iK + 2K).  The 2K x K panel of the new block is factored left-looking in panels
@@ -15,6 +18,7 @@
 #include "block_ls.h"
 
 #include <algorithm>
+#include <atomic>
 
 #include "common.h"
 
@@ -25,9 +29,14 @@ namespace {
 
 constexpr int kWin = 16;         // window rows per lane: 2K <= 512
 constexpr int kRowsMax = 32 * kWin;
-constexpr int kApplyWarps = 8;   // columns per block of apply_kernel
+constexpr int kApplyWarps = 4;   // columns per block of apply_kernel
 constexpr int kPanel = 16;       // columns per panel_kernel launch
+constexpr int kChunk = 8;        // reflectors per shared-memory stage
 constexpr unsigned kFull = 0xffffffffu;
+
+// dynamic shared memory of the staged reflector application: two stages of kChunk
+// vectors of L = 2K doubles rounded up to 32
+size_t stage_bytes(int K) { return sizeof(double) * 2 * kChunk * (size_t)((2 * K + 31) & ~31); }
 
 __device__ __forceinline__ double warp_sum(double s) {
 #pragma unroll
@@ -35,27 +44,24 @@ __device__ __forceinline__ double warp_sum(double s) {
    return s;
 }
 
-// x <- (I - tau v v^T) x on the window x (L rows) for the reflector v with pivot row r:
-// v is zero above r, so only rows r .. L-1 take part (chunks of 32 rows wholly above r
-// are skipped by the whole warp).
-__device__ __forceinline__ void reflect(double (&x)[kWin], const double* __restrict__ v, double tau, int r, int L,
+// x <- (I - tau v v^T) x on the window x for the reflector v with pivot row r: v holds
+// every row of the window (zeros above r, and zeros from L up to 32 nq, where nq = the
+// window's 32-row chunks), so no row needs a test; chunks of 32 rows wholly above r are
+// skipped by the whole warp.
+__device__ __forceinline__ void reflect(double (&x)[kWin], const double* __restrict__ v, double tau, int r, int nq,
                                         int lane) {
+   const int qlo = r >> 5;
    double vv[kWin];
-   double s = 0.0;
 #pragma unroll
-   for (int q = 0; q < kWin; q++) {
-      const int t = q * 32 + lane;
-      vv[q] = 0.0;
-      if (q * 32 + 32 > r && t >= r && t < L) vv[q] = v[t];
-   }
+   for (int q = 0; q < kWin; q++) vv[q] = q >= qlo && q < nq ? v[q * 32 + lane] : 0.0;
+   // four independent partial sums (rows q = 0, 4, 8, 12 | 1, 5, ... ) shorten the chain
+   double p4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-   for (int q = 0; q < kWin; q++) s = fma(vv[q], x[q], s);
-   s = warp_sum(s) * tau;
+   for (int q = 0; q < kWin; q++) p4[q & 3] = fma(vv[q], x[q], p4[q & 3]);
+   const double s = warp_sum((p4[0] + p4[1]) + (p4[2] + p4[3])) * tau;
 #pragma unroll
-   for (int q = 0; q < kWin; q++) {
-      const int t = q * 32 + lane;
-      if (q * 32 + 32 > r && t >= r && t < L) x[q] = fma(-s, vv[q], x[q]);
-   }
+   for (int q = 0; q < kWin; q++)
+      if (q >= qlo && q < nq) x[q] = fma(-s, vv[q], x[q]);
 }
 
 __device__ __forceinline__ void load_window(double (&x)[kWin], const double* w, int L, int lane) {
@@ -71,6 +77,59 @@ __device__ __forceinline__ void store_window(const double (&x)[kWin], double* w,
    for (int q = 0; q < kWin; q++) {
       const int t = q * 32 + lane;
       if (t < L) w[t] = x[q];
+   }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+   const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Reflectors rb .. re-1 of one block (vectors V + r L, scalars tau) applied in order to the
+// window x of every warp with `active` set.  All threads of the block copy the vectors into
+// shared memory, kChunk at a time through two stages (the next stage is copied while the
+// current one is applied), together with their scalars.  A staged vector has L32 = 32 nq
+// rows: the L rows of V (zeros above the pivot included) and zeros after them.  Every
+// thread of the block must call this with the same arguments but `active` and x.
+// sv: 2 kChunk L32 doubles, st: 2 kChunk doubles.
+__device__ __forceinline__ void apply_staged(double (&x)[kWin], bool active, const double* __restrict__ V,
+                                             const double* __restrict__ tau, int rb, int re, int L, int lane,
+                                             double* sv, double* st) {
+   const int L32 = (L + 31) & ~31, nq = L32 >> 5;
+   const int nchunks = (re - rb + kChunk - 1) / kChunk;
+   // the rows from L to L32 of every slot: zero (the copies below never write them)
+   for (int i = threadIdx.x; i < 2 * kChunk * (L32 - L); i += blockDim.x)
+      sv[(i / (L32 - L)) * L32 + L + i % (L32 - L)] = 0.0;
+   auto stage = [&](int ch, int buf) {
+      const int r0 = rb + ch * kChunk, nr = min(kChunk, re - r0);
+      double* dst = sv + buf * kChunk * L32;
+      for (int k = 0; k < nr; k++)  // 16-byte pieces (L even)
+         for (int t = 2 * (int)threadIdx.x; t < L; t += 2 * (int)blockDim.x)
+            cp_async16(dst + k * L32 + t, V + (int64_t)(r0 + k) * L + t);
+      if (threadIdx.x < nr) st[buf * kChunk + threadIdx.x] = tau[r0 + threadIdx.x];
+      cp_async_commit();
+   };
+   if (nchunks > 0) stage(0, 0);
+   for (int ch = 0; ch < nchunks; ch++) {
+      const int buf = ch & 1, r0 = rb + ch * kChunk, nr = min(kChunk, re - r0);
+      if (ch + 1 < nchunks) {
+         stage(ch + 1, buf ^ 1);
+         cp_async_wait<1>();
+      } else {
+         cp_async_wait<0>();
+      }
+      __syncthreads();
+      if (active)
+         for (int k = 0; k < nr; k++) {
+            const double tr = st[buf * kChunk + k];
+            if (tr != 0.0) reflect(x, sv + (buf * kChunk + k) * L32, tr, r0 + k, nq, lane);
+         }
+      __syncthreads();  // stage buf is refilled by the copies of chunk ch + 2
    }
 }
 
@@ -123,25 +182,22 @@ __global__ void __launch_bounds__(128) gather_kernel(int K, int hrows, const dou
 __global__ void __launch_bounds__(kApplyWarps * 32)
     apply_kernel(int K, int i0, int i1, const double* __restrict__ V, const double* __restrict__ tau,
                  double* __restrict__ X, int64_t ldx, int ncols, double* __restrict__ res) {
+   extern __shared__ __align__(16) double lsm[];
+   __shared__ double st[2 * kChunk];
    const int lane = threadIdx.x & 31;
    const int c = blockIdx.x * kApplyWarps + (threadIdx.x >> 5);
-   if (c >= ncols) return;
+   const bool active = c < ncols;  // the other warps still help to stage the vectors
    const int L = 2 * K;
-   double* column = X + (int64_t)c * ldx;
+   double* column = X + (int64_t)min(c, ncols - 1) * ldx;
    double x[kWin];
    for (int i = i0; i < i1; i++) {
       double* w = column + (int64_t)i * K;
-      load_window(x, w, L, lane);
-      const double* Vi = V + (int64_t)i * L * K;
-      const double* ti = tau + (int64_t)i * K;
-      for (int r = 0; r < K; r++) {
-         const double tr = ti[r];
-         if (tr != 0.0) reflect(x, Vi + (int64_t)r * L, tr, r, L, lane);
-      }
-      store_window(x, w, L, lane);
+      if (active) load_window(x, w, L, lane);
+      apply_staged(x, active, V + (int64_t)i * L * K, tau + (int64_t)i * K, 0, K, L, lane, lsm, st);
+      if (active) store_window(x, w, L, lane);
       __syncwarp();  // the next window starts K rows down, in rows other lanes wrote
    }
-   if (res) {
+   if (res && active) {
       double s = 0.0;
 #pragma unroll
       for (int q = 0; q < kWin; q++) {
@@ -160,17 +216,16 @@ __global__ void __launch_bounds__(kApplyWarps * 32)
 __global__ void __launch_bounds__(kPanel * 32)
     panel_kernel(int K, int b0, double* __restrict__ W, int64_t ldc, double* __restrict__ V,
                  double* __restrict__ tau) {
+   extern __shared__ __align__(16) double lsm[];
    __shared__ double vs[2][kRowsMax];
    __shared__ double ts[2];
+   __shared__ double st[2 * kChunk];
    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nb = blockDim.x >> 5;
-   const int L = 2 * K, c = b0 + w;
+   const int L = 2 * K, c = b0 + w, nq = (L + 31) >> 5;
    double* column = W + (int64_t)c * ldc;
    double x[kWin];
    load_window(x, column, L, lane);
-   for (int r = 0; r < b0; r++) {
-      const double tr = tau[r];
-      if (tr != 0.0) reflect(x, V + (int64_t)r * L, tr, r, L, lane);
-   }
+   apply_staged(x, true, V, tau, 0, b0, L, lane, lsm, st);
    for (int k = 0; k < nb; k++) {
       const int r = b0 + k;
       if (w == k) {
@@ -188,11 +243,14 @@ __global__ void __launch_bounds__(kPanel * 32)
          double* vk = vs[k & 1];
          double* vg = V + (int64_t)r * L;
          double tr = 0.0;
+         // the shared slot gets all 32 nq rows (zeros after L), V the L rows
          if (sigma == 0.0) {
 #pragma unroll
             for (int q = 0; q < kWin; q++) {
                const int t = q * 32 + lane;
-               if (t < L) vk[t] = vg[t] = t == r ? 1.0 : 0.0;
+               const double v = t == r ? 1.0 : 0.0;
+               if (q < nq) vk[t] = v;
+               if (t < L) vg[t] = v;
             }
          } else {
             const double normx = sqrt(alpha * alpha + sigma);
@@ -202,9 +260,10 @@ __global__ void __launch_bounds__(kPanel * 32)
 #pragma unroll
             for (int q = 0; q < kWin; q++) {
                const int t = q * 32 + lane;
+               const double v = t > r && t < L ? x[q] * scale : (t == r ? 1.0 : 0.0);
+               if (q < nq) vk[t] = v;
                if (t < L) {
-                  const double v = t > r ? x[q] * scale : (t == r ? 1.0 : 0.0);
-                  vk[t] = vg[t] = v;
+                  vg[t] = v;
                   if (t > r) x[q] = 0.0;
                   if (t == r) x[q] = beta;
                }
@@ -220,10 +279,23 @@ __global__ void __launch_bounds__(kPanel * 32)
       __syncthreads();
       if (w > k) {
          const double tr = ts[k & 1];
-         if (tr != 0.0) reflect(x, vs[k & 1], tr, r, L, lane);
+         if (tr != 0.0) reflect(x, vs[k & 1], tr, r, nq, lane);
       }
    }
    store_window(x, column, L, lane);
+}
+
+// raises the staged kernels' dynamic shared-memory limits (K = 256), once per device
+void prepare() {
+   static std::atomic<uint64_t> done{0};
+   int dev = 0;
+   FFTSVD_CUDA(cudaGetDevice(&dev));
+   const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
+   if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+   const int bytes = (int)stage_bytes(kRowsMax / 2);
+   FFTSVD_CUDA(cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+   FFTSVD_CUDA(cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+   done.fetch_or(bit, std::memory_order_acq_rel);
 }
 
 }  // namespace
@@ -250,23 +322,25 @@ void step(int j, int K, double* col, int64_t ldc, double* V, double* tau, double
    FFTSVD_REQUIRE(K > 0 && K <= kRowsMax / 2 && j >= 0 && ldc >= (int64_t)(j + 2) * K && ldg >= (int64_t)(j + 2) * K,
                   "block least squares: sizes");
    FFTSVD_REQUIRE(!Rd || ldr >= (int64_t)(j + 1) * K, "block least squares: factor rows");
+   prepare();
    const int L = 2 * K;
+   const size_t smem = stage_bytes(K);
    const int apply_blocks = (K + kApplyWarps - 1) / kApplyWarps;
    if (j > 0) {
-      apply_kernel<<<apply_blocks, kApplyWarps * 32, 0, s>>>(K, 0, j, V, tau, col, ldc, K, nullptr);
+      apply_kernel<<<apply_blocks, kApplyWarps * 32, smem, s>>>(K, 0, j, V, tau, col, ldc, K, nullptr);
       FFTSVD_CHECK_LAUNCH();
    }
    double* Vj = V + (int64_t)j * L * K;
    double* tj = tau + (int64_t)j * K;
    for (int b0 = 0; b0 < K; b0 += kPanel) {
       const int nb = std::min(kPanel, K - b0);
-      panel_kernel<<<1, nb * 32, 0, s>>>(K, b0, col + (int64_t)j * K, ldc, Vj, tj);
+      panel_kernel<<<1, nb * 32, smem, s>>>(K, b0, col + (int64_t)j * K, ldc, Vj, tj);
       FFTSVD_CHECK_LAUNCH();
    }
    if (Rd)
       FFTSVD_CUDA(cudaMemcpy2DAsync(Rd + (int64_t)j * K * ldr, sizeof(double) * ldr, col, sizeof(double) * ldc,
                                     sizeof(double) * (j + 1) * K, K, cudaMemcpyDeviceToDevice, s));
-   apply_kernel<<<apply_blocks, kApplyWarps * 32, 0, s>>>(K, j, j + 1, V, tau, g, ldg, K, stat);
+   apply_kernel<<<apply_blocks, kApplyWarps * 32, smem, s>>>(K, j, j + 1, V, tau, g, ldg, K, stat);
    FFTSVD_CHECK_LAUNCH();
 }
 
