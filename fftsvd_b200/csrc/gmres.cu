@@ -3,7 +3,9 @@
 // each Arnoldi step uses classical Gram-Schmidt applied twice (two passes of
 // one multi-dot and one multi-axpy over the whole basis), which is as stable as
 // MGS and turns 2(i+1) dependent vector sweeps into four.  The multi-dot runs one
-// block per (4096-row chunk, basis vector); updates one row per thread.  All
+// block per (4096-row chunk, basis vector); updates four rows per thread.  Each thread
+// issues all its loads of a chunk (or of four basis vectors) before it multiplies, so
+// the sweeps are not bound by the latency of one load at a time.  All
 // reductions are two-stage with a fixed order, so results are bitwise
 // reproducible run to run.
 #include <cmath>
@@ -58,15 +60,29 @@ __global__ void __launch_bounds__(kVecThreads) dots_partial_kernel(int64_t n, in
    V += blockIdx.z * col + (int64_t)j * ldv;
    w += blockIdx.z * col;
    partial += blockIdx.z * pcol;
-   const int64_t k0 = (int64_t)blockIdx.x * kDotChunk, k1 = min(n, k0 + kDotChunk);
-   double s0 = 0.0, s1 = 0.0;
-   int64_t k = k0 + threadIdx.x;
-   for (; k + blockDim.x < k1; k += 2 * blockDim.x) {
-      s0 += V[k] * w[k];
-      s1 += V[k + blockDim.x] * w[k + blockDim.x];
+   // a thread's kDotChunk / kVecThreads rows (k0 + t + kVecThreads i) are all loaded before
+   // any is multiplied, so each thread has 2 R loads in flight instead of two
+   constexpr int R = kDotChunk / kVecThreads;
+   const int64_t k0 = (int64_t)blockIdx.x * kDotChunk + threadIdx.x;
+   double a[R], b[R];
+   if ((int64_t)(blockIdx.x + 1) * kDotChunk <= n) {  // a whole chunk: no row test
+#pragma unroll
+      for (int i = 0; i < R; i++) {
+         a[i] = __ldg(V + k0 + (int64_t)i * kVecThreads);
+         b[i] = __ldg(w + k0 + (int64_t)i * kVecThreads);
+      }
+   } else {
+#pragma unroll
+      for (int i = 0; i < R; i++) {
+         const int64_t k = k0 + (int64_t)i * kVecThreads;
+         a[i] = k < n ? V[k] : 0.0;
+         b[i] = k < n ? w[k] : 0.0;
+      }
    }
-   if (k < k1) s0 += V[k] * w[k];
-   const double s = block_sum(s0 + s1, red);
+   double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+   for (int i = 0; i < R; i++) s4[i & 3] = fma(a[i], b[i], s4[i & 3]);
+   const double s = block_sum((s4[0] + s4[1]) + (s4[2] + s4[3]), red);
    if (threadIdx.x == 0) partial[(int64_t)j * gridDim.x + blockIdx.x] = s;
 }
 
@@ -113,25 +129,56 @@ __global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec
       }
    }
    __syncthreads();
-   const int64_t k = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
-   double x = 0.0;
-   if (k < n) {
-      x = w[k];
-      const double* v = V + k;
-      int j = 0;
-      for (; j + 3 < nvec; j += 4) {
-         const double a0 = v[(int64_t)j * ldv], a1 = v[(int64_t)(j + 1) * ldv];
-         const double a2 = v[(int64_t)(j + 2) * ldv], a3 = v[(int64_t)(j + 3) * ldv];
-         x -= a0 * hs[j];
-         x -= a1 * hs[j + 1];
-         x -= a2 * hs[j + 2];
-         x -= a3 * hs[j + 3];
+   // kRowsPerThread rows per thread, kVecThreads apart (coalesced); four basis vectors at a
+   // time, so each thread has 4 kRowsPerThread loads in flight
+   constexpr int RT = kRowsPerThread;
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+   double x[RT];
+#pragma unroll
+   for (int r = 0; r < RT; r++) {
+      const int64_t k = k0 + (int64_t)r * kVecThreads;
+      x[r] = k < n ? w[k] : 0.0;
+   }
+   const bool whole = (int64_t)(blockIdx.x + 1) * kRowsPerBlock <= n;  // no row test needed
+   int j = 0;
+   for (; j + 3 < nvec; j += 4) {
+      double a[4][RT];
+      if (whole) {
+#pragma unroll
+         for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int r = 0; r < RT; r++) a[q][r] = __ldg(V + (int64_t)(j + q) * ldv + k0 + (int64_t)r * kVecThreads);
+      } else {
+#pragma unroll
+         for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int r = 0; r < RT; r++) {
+               const int64_t k = k0 + (int64_t)r * kVecThreads;
+               a[q][r] = k < n ? V[(int64_t)(j + q) * ldv + k] : 0.0;
+            }
       }
-      for (; j < nvec; j++) x -= v[(int64_t)j * ldv] * hs[j];
-      out[k] = x;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+         for (int r = 0; r < RT; r++) x[r] -= a[q][r] * hs[j + q];
+   }
+   for (; j < nvec; j++)
+#pragma unroll
+      for (int r = 0; r < RT; r++) {
+         const int64_t k = k0 + (int64_t)r * kVecThreads;
+         if (k < n) x[r] -= V[(int64_t)j * ldv + k] * hs[j];
+      }
+   double ss = 0.0;
+#pragma unroll
+   for (int r = 0; r < RT; r++) {
+      const int64_t k = k0 + (int64_t)r * kVecThreads;
+      if (k < n) {
+         out[k] = x[r];
+         ss = fma(x[r], x[r], ss);
+      }
    }
    if (norm_partial) {
-      const double s = block_sum(x * x, red);
+      const double s = block_sum(ss, red);
       if (threadIdx.x == 0) norm_partial[blockIdx.z * pcol + blockIdx.x] = s;
    }
 }
@@ -142,9 +189,15 @@ __global__ void __launch_bounds__(kVecThreads) norm_partial_kernel(int64_t n, co
    __shared__ double red[kVecThreads / 32];
    w += blockIdx.z * col;
    partial += blockIdx.z * pcol;
-   const int64_t k = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
-   const double x = k < n ? w[k] : 0.0;
-   const double s = block_sum(x * x, red);
+   const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+   double ss = 0.0;
+#pragma unroll
+   for (int r = 0; r < kRowsPerThread; r++) {
+      const int64_t k = k0 + (int64_t)r * kVecThreads;
+      const double x = k < n ? w[k] : 0.0;
+      ss = fma(x, x, ss);
+   }
+   const double s = block_sum(ss, red);
    if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 

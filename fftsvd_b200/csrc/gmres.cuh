@@ -15,7 +15,8 @@
 namespace fftsvd {
 
 constexpr int kVecThreads = 256;
-constexpr int kRowsPerBlock = kVecThreads;  // one row per thread in row-wise kernels
+constexpr int kRowsPerThread = 4;  // rows per thread in row-wise kernels, kVecThreads apart
+constexpr int kRowsPerBlock = kVecThreads * kRowsPerThread;
 constexpr int kDotChunk = 4096;             // rows per block of the multi-dot
 
 // z[idx] = inv * r[idx] for every preconditioner block (blocks of size <= 8).
