@@ -129,9 +129,9 @@ __global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec
       }
    }
    __syncthreads();
-   // kRowsPerThread rows per thread, kVecThreads apart (coalesced); four basis vectors at a
-   // time, so each thread has 4 kRowsPerThread loads in flight
-   constexpr int RT = kRowsPerThread;
+   // kRowsPerThread rows per thread, kVecThreads apart (coalesced); kUpdateGroup basis vectors
+   // at a time, so each thread has kUpdateGroup kRowsPerThread loads in flight
+   constexpr int RT = kRowsPerThread, G = kUpdateGroup;
    const int64_t k0 = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
    double x[RT];
 #pragma unroll
@@ -141,16 +141,16 @@ __global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec
    }
    const bool whole = (int64_t)(blockIdx.x + 1) * kRowsPerBlock <= n;  // no row test needed
    int j = 0;
-   for (; j + 3 < nvec; j += 4) {
-      double a[4][RT];
+   for (; j + G - 1 < nvec; j += G) {
+      double a[G][RT];
       if (whole) {
 #pragma unroll
-         for (int q = 0; q < 4; q++)
+         for (int q = 0; q < G; q++)
 #pragma unroll
             for (int r = 0; r < RT; r++) a[q][r] = __ldg(V + (int64_t)(j + q) * ldv + k0 + (int64_t)r * kVecThreads);
       } else {
 #pragma unroll
-         for (int q = 0; q < 4; q++)
+         for (int q = 0; q < G; q++)
 #pragma unroll
             for (int r = 0; r < RT; r++) {
                const int64_t k = k0 + (int64_t)r * kVecThreads;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kVecThreads) update_kernel(int64_t n, int nvec
             }
       }
 #pragma unroll
-      for (int q = 0; q < 4; q++)
+      for (int q = 0; q < G; q++)
 #pragma unroll
          for (int r = 0; r < RT; r++) x[r] -= a[q][r] * hs[j + q];
    }

@@ -17,6 +17,7 @@ namespace fftsvd {
 constexpr int kVecThreads = 256;
 constexpr int kRowsPerThread = 4;  // rows per thread in row-wise kernels, kVecThreads apart
 constexpr int kRowsPerBlock = kVecThreads * kRowsPerThread;
+constexpr int kUpdateGroup = 4;    // basis vectors per load group of the update
 constexpr int kDotChunk = 4096;             // rows per block of the multi-dot
 
 // z[idx] = inv * r[idx] for every preconditioner block (blocks of size <= 8).

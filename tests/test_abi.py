@@ -49,6 +49,10 @@ def test_null_arguments_are_rejected_without_crashing():
     lib = F.load()
     assert lib.fftsvd_b200_matvec(None, 0, None, None) == _abi.FFTSVD_ERR_ARGUMENT
     assert lib.fftsvd_b200_solve(None, 0, None, None, 1e-6, 10, None) == _abi.FFTSVD_ERR_ARGUMENT
+    # the block least-squares hook checks its sizes and pointers before any device call
+    for k, m, ptr in ((0, 1, 8), (257, 1, 8), (8, 0, 8), (8, 1, None)):
+        p = C.c_void_p(ptr)
+        assert lib.fftsvd_b200_block_ls_device(k, m, p, p, p, p, p) == _abi.FFTSVD_ERR_ARGUMENT
 
 
 def test_create_without_device_reports_status():
