@@ -139,22 +139,40 @@ static void build_tiles(const TileProblem& P, const TileLimits& lim, TileSet& S)
    for (auto& kv : by_key) {
       std::vector<int>& ids = kv.second;
       std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return P.morton[a] < P.morton[b]; });
-      std::vector<MemberGroup> groups;
+      // runs of at most kGroupMax siblings, each made into one group (or single outputs)
+      // in parallel and concatenated in run order
+      std::vector<std::pair<size_t, size_t>> runs;
       for (size_t i = 0; i < ids.size();) {
          size_t last = i + 1;
          while (last < ids.size() && (int)(last - i) < kGroupMax && (P.morton[ids[last]] >> 3) == (P.morton[ids[i]] >> 3))
             last++;
-         MemberGroup G;
-         if (make_group(P, ids, i, last, G)) {
-            groups.push_back(std::move(G));
-         } else {
-            for (size_t k = i; k < last; k++) {
-               FFTSVD_REQUIRE(make_group(P, ids, k, k + 1, G), "interaction outside the 7x7x7 offset range");
-               groups.push_back(std::move(G));
-            }
-         }
+         runs.push_back({i, last});
          i = last;
       }
+      std::vector<std::vector<MemberGroup>> made(runs.size());
+      std::exception_ptr err;
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t r = 0; r < (int64_t)runs.size(); r++) {
+         try {
+            const size_t first = runs[r].first, last = runs[r].second;
+            MemberGroup G;
+            if (make_group(P, ids, first, last, G)) {
+               made[r].push_back(std::move(G));
+            } else {
+               for (size_t k = first; k < last; k++) {
+                  FFTSVD_REQUIRE(make_group(P, ids, k, k + 1, G), "interaction outside the 7x7x7 offset range");
+                  made[r].push_back(std::move(G));
+               }
+            }
+         } catch (...) {
+#pragma omp critical(fftsvd_tile_groups)
+            if (!err) err = std::current_exception();
+         }
+      }
+      if (err) std::rethrow_exception(err);
+      std::vector<MemberGroup> groups;
+      for (auto& v : made)
+         for (auto& g : v) groups.push_back(std::move(g));
       size_t pos = 0;
       while (pos < groups.size()) {
          TileDesc tile;
@@ -235,48 +253,58 @@ static void build_tiles(const TileProblem& P, const TileLimits& lim, TileSet& S)
 // Every index the translation kernel forms stays inside its buffers: table rows, the
 // in_elems input spectra and the out_elems output spectra, and the shared-memory rows.
 static void check_tiles(const TileSet& S, int64_t nt, int64_t in_elems, int64_t out_elems) {
-   for (const TileDesc& t : S.tiles) {
-      FFTSVD_REQUIRE(t.ngroups > 0 && t.ngroups <= kTileMaxGroups && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
-                         t.nentries > 0 && t.nentries <= kTileMaxEntries && t.nentries % 4 == 0 &&
-                         t.nmembers > 0 && t.nmembers <= kTileMaxGroups * kGroupMax && t.pg > 0 && t.pg % 16 == 0,
-                     "tile descriptor");
-      FFTSVD_REQUIRE(t.grp_off + t.ngroups <= (int64_t)S.tile_grp.size(), "tile groups out of range");
-      FFTSVD_REQUIRE(t.mem_off + t.nmembers <= (int64_t)S.tile_dst.size() &&
-                         t.mem_off + t.nmembers <= (int64_t)S.tile_delta.size(),
-                     "tile members out of range");
-      FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)S.tile_src.size(), "tile sources out of range");
-      FFTSVD_REQUIRE(t.ent_off + t.nentries <= (int64_t)S.tile_entries.size(), "tile entries out of range");
-      FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
-      for (int i = 0; i < t.nmembers; i++) {
-         const int64_t so = S.tile_dst[t.mem_off + i];
-         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= out_elems, "tile destination spectrum out of range");
-      }
-      for (int i = 0; i < t.nsrc; i++) {
-         const int64_t so = S.tile_src[t.src_off + i];
-         FFTSVD_REQUIRE(so >= 0 && so + t.pg <= in_elems, "tile source spectrum out of range");
-      }
-      for (int g = 0; g < t.ngroups; g++) {
-         const int4 gi = S.tile_grp[t.grp_off + g];
-         FFTSVD_REQUIRE(gi.x >= 0 && gi.x % 4 == 0 && gi.y > 0 && gi.y % 4 == 0 && gi.x + gi.y <= t.nentries &&
-                            gi.z >= 0 && gi.w >= 1 && gi.w <= kGroupMax && gi.z + gi.w <= t.nmembers,
-                        "tile group out of range");
-         for (int e = gi.x; e < gi.x + gi.y; e++) {
-            const uint32_t w = S.tile_entries[t.ent_off + e];
-            const int halo = (int)(w >> 17), base = (int)(w & 0x1ffu) - kEntryBaseBias;
-            const uint32_t mask = (w >> 9) & 0xffu;
-            // the kernel reads slot base + delta_j for every member j of the warp's largest
-            // group (delta 0 beyond this group's members): all of them must be table rows
-            FFTSVD_REQUIRE(halo < t.nsrc && (mask >> gi.w) == 0 && base >= 0 && base < 343, "tile entry out of range");
-            for (int j = 0; j < gi.w; j++) {
-               const int slot = base + S.tile_delta[t.mem_off + gi.z + j] + kEntryBaseBias;
-               FFTSVD_REQUIRE(slot >= 0 && slot < 343, "tile entry slot out of range");
-               const int dx = slot / 49 - 3, dy = (slot / 7) % 7 - 3, dz = slot % 7 - 3;
-               const bool local = std::abs(dx) <= 1 && std::abs(dy) <= 1 && std::abs(dz) <= 1;
-               FFTSVD_REQUIRE(local != (((mask >> j) & 1u) != 0), "tile entry reaches a non-interacting member");
+   // tiles are checked independently on all host threads; the first failure is rethrown
+   std::exception_ptr err;
+#pragma omp parallel for schedule(dynamic, 16)
+   for (int64_t ti = 0; ti < (int64_t)S.tiles.size(); ti++) {
+      try {
+         const TileDesc& t = S.tiles[ti];
+         FFTSVD_REQUIRE(t.ngroups > 0 && t.ngroups <= kTileMaxGroups && t.nsrc > 0 && t.nsrc <= kTileMaxSrc &&
+                            t.nentries > 0 && t.nentries <= kTileMaxEntries && t.nentries % 4 == 0 &&
+                            t.nmembers > 0 && t.nmembers <= kTileMaxGroups * kGroupMax && t.pg > 0 && t.pg % 16 == 0,
+                        "tile descriptor");
+         FFTSVD_REQUIRE(t.grp_off + t.ngroups <= (int64_t)S.tile_grp.size(), "tile groups out of range");
+         FFTSVD_REQUIRE(t.mem_off + t.nmembers <= (int64_t)S.tile_dst.size() &&
+                            t.mem_off + t.nmembers <= (int64_t)S.tile_delta.size(),
+                        "tile members out of range");
+         FFTSVD_REQUIRE(t.src_off + t.nsrc <= (int64_t)S.tile_src.size(), "tile sources out of range");
+         FFTSVD_REQUIRE(t.ent_off + t.nentries <= (int64_t)S.tile_entries.size(), "tile entries out of range");
+         FFTSVD_REQUIRE(t.t_off >= 0 && t.t_off + 343LL * t.pg <= nt, "tile translation table out of range");
+         for (int i = 0; i < t.nmembers; i++) {
+            const int64_t so = S.tile_dst[t.mem_off + i];
+            FFTSVD_REQUIRE(so >= 0 && so + t.pg <= out_elems, "tile destination spectrum out of range");
+         }
+         for (int i = 0; i < t.nsrc; i++) {
+            const int64_t so = S.tile_src[t.src_off + i];
+            FFTSVD_REQUIRE(so >= 0 && so + t.pg <= in_elems, "tile source spectrum out of range");
+         }
+         for (int g = 0; g < t.ngroups; g++) {
+            const int4 gi = S.tile_grp[t.grp_off + g];
+            FFTSVD_REQUIRE(gi.x >= 0 && gi.x % 4 == 0 && gi.y > 0 && gi.y % 4 == 0 && gi.x + gi.y <= t.nentries &&
+                               gi.z >= 0 && gi.w >= 1 && gi.w <= kGroupMax && gi.z + gi.w <= t.nmembers,
+                           "tile group out of range");
+            for (int e = gi.x; e < gi.x + gi.y; e++) {
+               const uint32_t w = S.tile_entries[t.ent_off + e];
+               const int halo = (int)(w >> 17), base = (int)(w & 0x1ffu) - kEntryBaseBias;
+               const uint32_t mask = (w >> 9) & 0xffu;
+               // the kernel reads slot base + delta_j for every member j of the warp's largest
+               // group (delta 0 beyond this group's members): all of them must be table rows
+               FFTSVD_REQUIRE(halo < t.nsrc && (mask >> gi.w) == 0 && base >= 0 && base < 343, "tile entry out of range");
+               for (int j = 0; j < gi.w; j++) {
+                  const int slot = base + S.tile_delta[t.mem_off + gi.z + j] + kEntryBaseBias;
+                  FFTSVD_REQUIRE(slot >= 0 && slot < 343, "tile entry slot out of range");
+                  const int dx = slot / 49 - 3, dy = (slot / 7) % 7 - 3, dz = slot % 7 - 3;
+                  const bool local = std::abs(dx) <= 1 && std::abs(dy) <= 1 && std::abs(dz) <= 1;
+                  FFTSVD_REQUIRE(local != (((mask >> j) & 1u) != 0), "tile entry reaches a non-interacting member");
+               }
             }
          }
+      } catch (...) {
+#pragma omp critical(fftsvd_tile_check)
+         if (!err) err = std::current_exception();
       }
    }
+   if (err) std::rethrow_exception(err);
 }
 
 void make_tiles(const TileProblems& P, const TileLimits& lim, TileSet& fwd, TileSet& adj) {
@@ -285,10 +313,9 @@ void make_tiles(const TileProblems& P, const TileLimits& lim, TileSet& fwd, Tile
                   "tile limits out of range");
    fwd = TileSet();
    adj = TileSet();
-   // the two directions are independent: built side by side (an exception in either is
-   // carried out of the parallel region and rethrown here)
+   // the two directions one after the other, each building its member groups on all
+   // host threads (an exception in either is carried out and rethrown here)
    std::exception_ptr err[2];
-#pragma omp parallel for num_threads(2) schedule(static, 1)
    for (int d = 0; d < 2; d++) {
       try {
          if (d == 0) {
@@ -326,6 +353,50 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
    }
    L.tree_panel_off[num_trees] = np;
    L.tree_point_off[num_trees] = nq;
+   // room for every tree's arrays at once (bounds from the trees' own totals), so that no
+   // tree's growth reallocates and copies the arrays of the trees before it
+   {
+      size_t rows = 0, cols = 0, dp = 0, sp = 0, vt = 0, pv = 0, pts = 0, uti = 0, u = 0, ip = 0, tp = 0, cubes = 0;
+      size_t leaves = 0;
+      for (int t = 0; t < num_trees; t++) {
+         const fftsvd_tree_flat& T = trees[t];
+         const int nl = std::max(T.num_leaves, 0), nc = std::max(T.num_cubes, 0);
+         leaves += nl;
+         cubes += nc;
+         if (nl > 0) {
+            rows += (size_t)std::max(T.leaf_row_ptr[nl], 0);
+            cols += (size_t)std::max(T.leaf_col_ptr[nl], 0) + nl;  // columns padded to even counts
+            dp += 2 * ((size_t)std::max<int64_t>(T.leaf_d_ptr[nl], 0) + (size_t)std::max(T.leaf_row_ptr[nl], 0));
+         }
+         if (nc > 0) {
+            sp += (size_t)std::max(T.cube_panel_ptr[nc], 0);
+            vt += (size_t)std::max<int64_t>(T.cube_vt_ptr[nc], 0);
+            pv += 2 * (size_t)std::max<int64_t>(T.cube_pv_ptr[nc], 0);
+            pts += (size_t)std::max(T.cube_point_ptr[nc], 0);
+            uti += (size_t)std::max<int64_t>(T.cube_uti_ptr[nc], 0);
+            u += (size_t)std::max<int64_t>(T.cube_u_ptr[nc], 0);
+            ip += 2 * (size_t)std::max(T.inter_ptr[nc], 0);
+         }
+         for (int l = 0; l < (int)std::min<int64_t>(T.depth, FFTSVD_MAX_DEPTH); l++) {
+            const int n = T.grid[l], Npl = 2 * n - 1;
+            if (n >= 2 && n <= 12) tp += 2 * 343 * (size_t)pad16(Npl * Npl * n);
+         }
+      }
+      L.leaves.reserve(leaves);
+      L.leaf_rows.reserve(rows);
+      L.leaf_cols.reserve(cols);
+      L.d_pairs.reserve(dp);
+      L.src.reserve(cubes);
+      L.src_panels.reserve(sp);
+      L.vt.reserve(vt);
+      L.pv_pairs.reserve(pv);
+      L.dst.reserve(cubes);
+      L.dst_points.reserve(pts);
+      L.uti.reserve(uti);
+      L.u_cm.reserve(u);
+      L.inter_pairs.reserve(ip);
+      L.t_pairs.reserve(tp);
+   }
    L.total_panels = np + 1;  // last slot stays zero: target of padding columns
    L.total_points = nq;
    const int32_t zero_slot = (int32_t)np;
@@ -650,10 +721,33 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
    {
       TileProblem& fwd = L.problems->fwd;
       TileProblem& adj = L.problems->adj;
-      std::unordered_map<int64_t, int> src_of_spec;
-      src_of_spec.reserve(2 * L.src.size());
-      for (int i = 0; i < (int)L.src.size(); i++) src_of_spec[L.src[i].spec_off] = i;
-      std::vector<std::vector<std::pair<int64_t, int>>> adj_lists(L.src.size());
+      // source index of each spectrum (spectra start at distinct multiples of 16)
+      std::vector<int32_t> src_of_spec((size_t)(L.spectra_elems / 16) + 1, -1);
+      for (int i = 0; i < (int)L.src.size(); i++) {
+         FFTSVD_REQUIRE(L.src[i].spec_off % 16 == 0, "spectrum offset");
+         src_of_spec[(size_t)(L.src[i].spec_off / 16)] = i;
+      }
+      auto source_of = [&](int64_t so) {
+         const int i = so >= 0 && so < L.spectra_elems && so % 16 == 0 ? src_of_spec[(size_t)(so / 16)] : -1;
+         FFTSVD_REQUIRE(i >= 0, "interaction with an unknown source spectrum");
+         return i;
+      };
+      const int64_t npairs = (int64_t)L.inter_pairs.size() / 2;
+      fwd.in_off.reserve(npairs);
+      fwd.slot.reserve(npairs);
+      adj.in_off.reserve(npairs);
+      adj.slot.reserve(npairs);
+      // the transposed lists in compressed form: per source, its destinations in the order
+      // of the destinations and their interactions
+      std::vector<int64_t> adj_ptr(L.src.size() + 1, 0);
+      for (int i = 0; i < (int)L.dst.size(); i++) {
+         const DstDesc& d = L.dst[i];
+         for (int q = 0; q < d.inter_cnt; q++) adj_ptr[source_of(L.inter_pairs[2 * (d.inter_off + q)]) + 1]++;
+      }
+      for (size_t i = 0; i < L.src.size(); i++) adj_ptr[i + 1] += adj_ptr[i];
+      std::vector<int64_t> adj_out((size_t)adj_ptr.back());
+      std::vector<int> adj_slot((size_t)adj_ptr.back());
+      std::vector<int64_t> fill(adj_ptr.begin(), adj_ptr.end() - 1);
       for (int i = 0; i < (int)L.dst.size(); i++) {
          const DstDesc& d = L.dst[i];
          const DstExtra& e = dst_extra[i];
@@ -664,15 +758,15 @@ OperatorLayout build_layout(int num_unknowns, int num_trees, const fftsvd_tree_f
             const int64_t slot = (to - e.t_base) / e.pg;
             FFTSVD_REQUIRE(slot >= 0 && slot < 343 && (to - e.t_base) % e.pg == 0, "translation slot");
             fwd.add_pair(so, (int)slot);
-            auto it = src_of_spec.find(so);
-            FFTSVD_REQUIRE(it != src_of_spec.end(), "interaction with an unknown source spectrum");
-            adj_lists[it->second].push_back({d.s_off, 342 - (int)slot});
+            const int64_t at = fill[source_of(so)]++;
+            adj_out[at] = d.s_off;
+            adj_slot[at] = 342 - (int)slot;
          }
       }
       for (int i = 0; i < (int)L.src.size(); i++) {
          const DstExtra& e = src_extra[i];
          adj.add_output(e.key, e.morton, e.t_base, e.pg, L.src[i].spec_off);
-         for (const auto& pr : adj_lists[i]) adj.add_pair(pr.first, pr.second);
+         for (int64_t k = adj_ptr[i]; k < adj_ptr[i + 1]; k++) adj.add_pair(adj_out[k], adj_slot[k]);
       }
    }
 
@@ -2407,8 +2501,13 @@ __global__ void far_add_kernel(int64_t nrows, const int32_t* __restrict__ rows, 
 
 // ------------------------------------------------------------------ host side
 
-template <typename T>
-static void upload_cast(DevBuf<T>& dst, const std::vector<double>& src) {
+// FP64 uploads go straight from the layout's arrays; FP32 ones through a converted copy
+template <typename T, typename Vec>
+static void upload_cast(DevBuf<T>& dst, const Vec& src) {
+   if constexpr (std::is_same<T, double>::value) {
+      dst.upload(src.data(), src.size());
+      return;
+   }
    std::vector<T, FillLater<T>> tmp(src.size());
    const int64_t n = (int64_t)tmp.size();
 #pragma omp parallel for schedule(static)
@@ -2419,6 +2518,10 @@ static void upload_cast(DevBuf<T>& dst, const std::vector<double>& src) {
 template <typename T, typename Vec>
 static void upload_pairs(DevBuf<typename Vec2<T>::type>& dst, const Vec& src) {
    using T2 = typename Vec2<T>::type;
+   if constexpr (std::is_same<T, double>::value) {  // {re, im} pairs are double2 in memory
+      dst.upload(reinterpret_cast<const T2*>(src.data()), src.size() / 2);
+      return;
+   }
    std::vector<T2, FillLater<T2>> tmp(src.size() / 2);
    const int64_t np = (int64_t)tmp.size();
 #pragma omp parallel for schedule(static)

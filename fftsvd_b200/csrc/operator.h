@@ -215,13 +215,13 @@ struct OperatorLayout {
    // far field
    std::vector<SrcDesc> src;
    std::vector<int32_t> src_panels;
-   std::vector<double> vt;
+   LayoutDoubles vt;
    LayoutDoubles pv_pairs;             // interleaved {PVs, PVd}, r x n^3
    std::vector<DstDesc> dst;
    std::vector<int32_t> dst_points;
-   std::vector<double> uti, u_cm;
+   LayoutDoubles uti, u_cm;
    std::vector<int64_t> inter_pairs;   // {spectrum offset, T offset} packed as 2 x int64
-   std::vector<double> t_pairs;        // translation operators {re, im}
+   LayoutDoubles t_pairs;              // translation operators {re, im}
    int64_t spectra_elems = 0;
    int64_t translated_elems = 0;       // S buffer, complex elements
    int max_src_smem_elems = 0, max_dst_smem_elems = 0;

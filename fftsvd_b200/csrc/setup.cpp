@@ -819,6 +819,9 @@ void Tree::flatten(FlatTree& F) const {
    }
    F.num_cubes = nc;
    int64_t off = 0;
+   size_t t_total = 0;
+   for (int d = 0; d < depth; d++) t_total += tops[d].size();
+   F.t_ops.reserve(t_total);
    for (int d = 0; d < depth; d++) {
       F.t_level_ptr.push_back(off);
       off += (int64_t)tops[d].size() / 2;

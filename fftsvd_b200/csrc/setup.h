@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/fftsvd_b200.h"
+#include "fill_later.h"
 #include "integrals.h"
 
 namespace fftsvd {
@@ -64,11 +65,12 @@ struct FlatTree {
    std::vector<int> grid;
    std::vector<int32_t> leaf_row_ptr, leaf_rows, leaf_col_ptr, leaf_cols;
    std::vector<int64_t> leaf_d_ptr;
-   std::vector<double> d_single, d_double;
+   // the large arrays are sized first and filled in parallel: no zero-fill pass
+   std::vector<double, FillLater<double>> d_single, d_double;
    std::vector<int32_t> cube_level, cube_index, cube_panel_ptr, cube_panels, cube_point_ptr, cube_points;
    std::vector<int32_t> cube_row_rank, cube_col_rank, inter_ptr, inter_cubes;
    std::vector<int64_t> cube_vt_ptr, cube_pv_ptr, cube_uti_ptr, cube_u_ptr, t_level_ptr;
-   std::vector<double> vt, pv_single, pv_double, uti, u, t_ops;
+   std::vector<double, FillLater<double>> vt, pv_single, pv_double, uti, u, t_ops;
    void view(fftsvd_tree_flat& t) const;
 };
 
