@@ -270,8 +270,62 @@ static void r2c3(int N, const std::vector<double>& in, std::vector<std::complex<
 
 // ------------------------------------------------------------------ tree
 
+// Children of cube ci in cx, cy, cz order: one pass over its panels and points sends each
+// to the octant its coordinates select (coordinate >= the centre: upper half), keeping the
+// parent's order within every child; empty octants get no cube.
+void Tree::split_cube(size_t ci) {
+   const Cube& par = cubes[ci];
+   const double cc[3] = {par.center[0], par.center[1], par.center[2]};
+   const double pb0[3] = {par.b0[0], par.b0[1], par.b0[2]};
+   const int pidx[3] = {par.idx[0], par.idx[1], par.idx[2]}, plevel = par.level;
+   auto octant = [&](const double* p) { return (p[0] >= cc[0]) * 4 + (p[1] >= cc[1]) * 2 + (p[2] >= cc[2]); };
+   std::vector<int> bp[8], bq[8];
+   for (int i : par.panels) bp[octant((*panels)[i].centroid)].push_back(i);
+   for (int i : par.points) bq[octant(&(*points)[3 * (size_t)i])].push_back(i);
+   for (int slot = 0; slot < 8; slot++) {
+      if (bp[slot].empty() && bq[slot].empty()) continue;
+      const int cbit[3] = {slot >> 2, (slot >> 1) & 1, slot & 1};
+      Cube ch;
+      ch.panels = std::move(bp[slot]);
+      ch.points = std::move(bq[slot]);
+      for (int k = 0; k < 3; k++) {
+         ch.b0[k] = pb0[k];
+         ch.b1[k] = cc[k];
+         if (cbit[k] == 1) {
+            const double diff = cc[k] - ch.b0[k];
+            ch.b0[k] += diff;
+            ch.b1[k] += diff;
+         }
+         ch.idx[k] = 2 * pidx[k] + cbit[k];
+      }
+      ch.level = plevel + 1;
+      ch.parent = (int)ci;
+      cubes.push_back(std::move(ch));  // may move the parent: nothing of it is used below
+      cubes[ci].child[slot] = (int)cubes.size() - 1;
+   }
+}
+
+// Cubes are kept in breadth-first creation order (children of one cube in cx, cy, cz
+// order), so the tree of depth d + 1 is the tree of depth d with the children of its
+// leaves appended in order.
+void Tree::add_level() {
+   const size_t n0 = cubes.size();
+   for (size_t ci = 0; ci < n0; ci++)
+      if (cubes[ci].level == depth - 1) {
+         cubes[ci].leaf = false;
+         split_cube(ci);
+      }
+   depth++;
+   for (size_t ci = n0; ci < cubes.size(); ci++) {
+      Cube& c = cubes[ci];
+      for (int k = 0; k < 3; k++) c.center[k] = (c.b0[k] + c.b1[k]) * 0.5;
+      for (int k = 0; k < 8; k++) c.child[k] = -1;
+      c.leaf = true;
+   }
+}
+
 void Tree::build_cubes(int depth_) {
-   depth = depth_;
+   depth = 1;
    cubes.clear();
    Cube root;
    root.level = 0;
@@ -281,49 +335,11 @@ void Tree::build_cubes(int depth_) {
    root.panels.resize(panels->size());
    for (size_t i = 0; i < panels->size(); i++) root.panels[i] = (int)i;
    root.points = root.panels;
+   for (int k = 0; k < 3; k++) root.center[k] = (root.b0[k] + root.b1[k]) * 0.5;
+   for (int k = 0; k < 8; k++) root.child[k] = -1;
+   root.leaf = true;
    cubes.push_back(std::move(root));
-   // breadth-first in creation order; children of one cube in cx, cy, cz order
-   for (size_t ci = 0; ci < cubes.size(); ci++) {
-      Cube& c = cubes[ci];
-      for (int k = 0; k < 3; k++) c.center[k] = (c.b0[k] + c.b1[k]) * 0.5;
-      for (int k = 0; k < 8; k++) c.child[k] = -1;
-      if (c.level == depth - 1) {
-         c.leaf = true;
-         continue;
-      }
-      c.leaf = false;
-      const double cc[3] = {c.center[0], c.center[1], c.center[2]};
-      for (int cx = 0; cx <= 1; cx++)
-         for (int cy = 0; cy <= 1; cy++)
-            for (int cz = 0; cz <= 1; cz++) {
-               auto inside = [&](const double* p) {
-                  return ((cx == 0 && p[0] < cc[0]) || (cx == 1 && p[0] >= cc[0])) &&
-                         ((cy == 0 && p[1] < cc[1]) || (cy == 1 && p[1] >= cc[1])) &&
-                         ((cz == 0 && p[2] < cc[2]) || (cz == 1 && p[2] >= cc[2]));
-               };
-               Cube ch;
-               for (int i : cubes[ci].panels)
-                  if (inside((*panels)[i].centroid)) ch.panels.push_back(i);
-               for (int i : cubes[ci].points)
-                  if (inside(&(*points)[3 * (size_t)i])) ch.points.push_back(i);
-               if (ch.panels.empty() && ch.points.empty()) continue;
-               const Cube& par = cubes[ci];
-               for (int k = 0; k < 3; k++) { ch.b0[k] = par.b0[k]; ch.b1[k] = par.center[k]; }
-               const int cbit[3] = {cx, cy, cz};
-               for (int k = 0; k < 3; k++)
-                  if (cbit[k] == 1) {
-                     const double diff = par.center[k] - ch.b0[k];
-                     ch.b0[k] += diff;
-                     ch.b1[k] += diff;
-                  }
-               for (int k = 0; k < 3; k++) ch.idx[k] = 2 * par.idx[k] + cbit[k];
-               ch.level = par.level + 1;
-               ch.parent = (int)ci;
-               const int slot = cx * 4 + cy * 2 + cz;
-               cubes.push_back(std::move(ch));
-               cubes[ci].child[slot] = (int)cubes.size() - 1;
-            }
-   }
+   while (depth < depth_) add_level();
 }
 
 void Tree::choose_depth(int max_panels) {
@@ -346,7 +362,10 @@ void Tree::choose_depth(int max_panels) {
    }
    for (int k = 0; k < 3; k++) { bounds0[k] = ctr[k] - ext * 0.5; bounds1[k] = ctr[k] + ext * 0.5; }
    for (int d = 2;; d++) {
-      build_cubes(d);
+      if (d == 2)
+         build_cubes(d);
+      else
+         add_level();
       if (panels->empty() || np == 0) break;
       int leaves = 0, within = 0;
       for (const Cube& c : cubes)

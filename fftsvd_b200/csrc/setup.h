@@ -91,6 +91,8 @@ struct Tree {
    double eval_ms = 0.0;                     // wall time inside eval
 
    void build_cubes(int depth);
+   void split_cube(size_t ci);  // children of cube ci, appended
+   void add_level();            // one more level below the current leaves
    void choose_depth(int max_panels);
    void make_lists();
    void fill_near();
