@@ -20,6 +20,7 @@
 
 #include "common.h"
 #include "integrals.h"
+#include "fill_later.h"
 #include "setup.h"
 
 namespace fftsvd {
@@ -82,6 +83,14 @@ struct Buf {  // device allocation owned by the evaluator (freed on scope exit)
       alloc(count);
       if (count) cuda_check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s), "copy to device");
    }
+   // at least count elements, reallocated only to grow (the contents are not kept)
+   void reserve(size_t count) {
+      if (count > n) alloc(count);
+   }
+   void upload_grow(const T* h, size_t count, cudaStream_t s) {
+      reserve(count);
+      if (count) cuda_check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s), "copy to device");
+   }
    void release() {
       if (p) cudaFree(p);
       p = nullptr;
@@ -95,25 +104,33 @@ struct DeviceSampler {
    Buf<FlatPanel> panels;
    const FlatPanel* host_panels = nullptr;  // the panel list the device copy was made from
    size_t host_count = 0;
-   // Pinned host copy of the last batch's output, grown to the largest batch: the results
-   // come back at full link speed and the setup's several batches reuse one allocation.
-   double* pinned = nullptr;
-   size_t pinned_elems = 0;
+   // Host copy of the last batch's output, grown to the largest batch and reused by the
+   // setup's later batches.  Pageable, not pinned: page-locking a buffer of several GB
+   // (3.6 GB of samples at 327 680 panels) took seconds, far longer than the copy itself.
+   std::vector<double, FillLater<double>> host_out;
+   // device buffers of the batches, grown to the largest and reused (a setup's batches
+   // would otherwise allocate and free several GB each)
+   Buf<DevBlock> d_blocks;
+   Buf<PairTile> d_tiles;
+   Buf<double> d_pts, d_out;
+   Buf<int32_t> d_pan;
+   Buf<unsigned int> d_status;
    ~DeviceSampler() {
       if (stream) cudaStreamDestroy(stream);
-      if (pinned) cudaFreeHost(pinned);
    }
 
    double* host_output(size_t elems) {
-      if (elems > pinned_elems) {
-         if (pinned) cudaFreeHost(pinned);
-         pinned = nullptr;
-         pinned_elems = 0;
-         cuda_check(cudaHostAlloc((void**)&pinned, elems * sizeof(double), cudaHostAllocDefault),
-                    "cudaHostAlloc (setup integrals)");
-         pinned_elems = elems;
+      if (elems > host_out.size()) {
+         host_out = std::vector<double, FillLater<double>>();  // the old contents are not needed
+         host_out.resize(elems);                               // every entry is copied in below
+         // one write per 4 KB page on all host threads: the copy then lands in mapped pages,
+         // instead of taking a fresh buffer's page faults one at a time (1.2 s for 3.6 GB)
+         double* p = host_out.data();
+         const int64_t n = (int64_t)elems;
+#pragma omp parallel for schedule(static)
+         for (int64_t i = 0; i < n; i += 512) p[i] = 0.0;
       }
-      return pinned;
+      return host_out.data();
    }
 
    const double* operator()(const Kernel& kern, const std::vector<FlatPanel>& pl, const IntegralBatch& B) {
@@ -156,19 +173,14 @@ struct DeviceSampler {
          std::fill(out, out + B.out_elems, 0.0);
          return out;
       }
-      Buf<DevBlock> d_blocks;
-      Buf<PairTile> d_tiles;
-      Buf<double> d_pts, d_out;
-      Buf<int32_t> d_pan;
-      Buf<unsigned int> d_status;
-      d_blocks.upload(blocks.data(), blocks.size(), stream);
-      d_tiles.upload(tiles.data(), tiles.size(), stream);
-      d_pts.upload(B.points.data(), B.points.size(), stream);
-      d_pan.upload(B.panels.data(), B.panels.size(), stream);
-      d_out.alloc((size_t)B.out_elems);
+      d_blocks.upload_grow(blocks.data(), blocks.size(), stream);
+      d_tiles.upload_grow(tiles.data(), tiles.size(), stream);
+      d_pts.upload_grow(B.points.data(), B.points.size(), stream);
+      d_pan.upload_grow(B.panels.data(), B.panels.size(), stream);
+      d_out.reserve((size_t)B.out_elems);
       // output entries no block covers (none in the batches built by setup.cpp) read as zero
       cuda_check(cudaMemsetAsync(d_out.p, 0, sizeof(double) * (size_t)B.out_elems, stream), "memset");
-      d_status.alloc(1);
+      d_status.reserve(1);
       cuda_check(cudaMemsetAsync(d_status.p, 0, sizeof(unsigned int), stream), "memset");
       // grid x is limited to 2^31 - 1 blocks; split longer tile lists into launches
       const size_t max_grid = 1u << 30;

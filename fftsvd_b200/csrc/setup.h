@@ -41,7 +41,7 @@ struct IntegralBatch {
 // Evaluates every block of a batch with one kernel over the tree's panels and returns the
 // output array (out_elems doubles), valid until the evaluator's next call.  Trees without an
 // evaluator integrate on the host, panel by panel; the device evaluator (sampling.cu) runs
-// the same integrals on the GPU and returns them in pinned host memory.
+// the same integrals on the GPU and returns them in a host buffer it owns.
 using BatchEvaluator =
     std::function<const double*(const Kernel& k, const std::vector<FlatPanel>& panels, const IntegralBatch& b)>;
 
