@@ -145,3 +145,19 @@ def test_iteration_cap_reports_not_converged(blob3):
         assert info[c].iterations <= 2
         # the residual reported is the true one of the returned iterate
         assert abs(_presid(s, R[c], sol[c]) - info[c].residual) < 1e-6 * info[c].residual
+
+
+def test_krylov_space_exhausted_by_a_wide_block(blob3):
+    """256 random columns on a surface of 2 560 unknowns fill the whole space in ten block
+    steps, before a 1e-8 solve would converge from its rate: the tenth block is what remains
+    after projecting against every direction, rounding noise, and its factor in the block
+    Hessenberg matrix is at rounding level.  The least-squares update on the device then
+    reports residuals at rounding level (a lucky breakdown) and the recomputed FP64
+    residuals meet the tolerance, with no more block steps than the space has blocks."""
+    s = blob3[0]
+    R = np.random.default_rng(21).standard_normal((256, s.n))
+    sol, info = s.solve_block(R, precision="fp64", tol=1e-8)
+    for c in range(0, 256, 17):
+        assert info[c].status == 0, c
+        assert _presid(s, R[c], sol[c]) < 1e-8 * 1.001, c
+    assert max(i.iterations for i in info) <= s.n // 256
