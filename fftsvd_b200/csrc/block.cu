@@ -274,6 +274,9 @@ int Surface::gmres_block(int precision, int K, const double* R0, double* T, int 
    const int64_t vblk = (int64_t)K * n;
    double* V = B.V.get();
    res.assign(K, 0.0);
+   // nothing of an earlier cycle may still run on the least-squares stream (a cycle left by
+   // an error does not wait for it): its buffers are rewritten below
+   FFTSVD_CUDA(cudaStreamSynchronize(B.ls_stream));
    // V_0 S0 = R0
    FFTSVD_CUDA(cudaMemsetAsync(B.flag.get(), 0, sizeof(int32_t), stream));
    block_qr(R0, V, K);
