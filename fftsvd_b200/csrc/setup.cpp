@@ -414,32 +414,52 @@ void Tree::fill_near() {
    std::vector<int> leaves;
    for (size_t i = 0; i < cubes.size(); i++)
       if (cubes[i].leaf) leaves.push_back((int)i);
-   for (int li : leaves) {
-      Cube& c = cubes[li];
+   const int64_t nl = (int64_t)leaves.size();
+#pragma omp parallel for schedule(dynamic, 64)
+   for (int64_t li = 0; li < nl; li++) {
+      Cube& c = cubes[leaves[li]];
       c.dcols = c.panels;
       for (int o : c.local) c.dcols.insert(c.dcols.end(), cubes[o].panels.begin(), cubes[o].panels.end());
    }
    if (eval) {
-      // every leaf block in one batch: Ds then Dd of each leaf, row-major
+      // every leaf block in one batch: Ds then Dd of each leaf, row-major.  Sizes first,
+      // running offsets from them, then every leaf's part written in parallel: the batch is
+      // laid out exactly as if the leaves' blocks were appended one after another.
       IntegralBatch B;
       std::vector<int64_t> off(leaves.size(), -1);
-      for (size_t li = 0; li < leaves.size(); li++) {
+      std::vector<int64_t> pt_at(nl + 1, 0), pan_at(nl + 1, 0), out_at(nl + 1, 0), blk_at(nl + 1, 0);
+      for (int64_t li = 0; li < nl; li++) {
+         const Cube& c = cubes[leaves[li]];
+         const int64_t nr = (int64_t)c.points.size(), nc = (int64_t)c.dcols.size();
+         const bool some = nr > 0 && nc > 0;
+         pt_at[li + 1] = pt_at[li] + (some ? nr : 0);
+         pan_at[li + 1] = pan_at[li] + (some ? nc : 0);
+         out_at[li + 1] = out_at[li] + (some ? 2 * nr * nc : 0);
+         blk_at[li + 1] = blk_at[li] + (some ? 1 : 0);
+      }
+      B.points.resize(3 * (size_t)pt_at[nl]);
+      B.panels.resize((size_t)pan_at[nl]);
+      B.blocks.resize((size_t)blk_at[nl]);
+      B.out_elems = out_at[nl];
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t li = 0; li < nl; li++) {
          const Cube& c = cubes[leaves[li]];
          const int nr = (int)c.points.size(), nc = (int)c.dcols.size();
          if (nr == 0 || nc == 0) continue;
          IntegralBlock b;
          b.npts = nr;
          b.npan = nc;
-         b.pt_off = (int64_t)B.points.size() / 3;
-         for (int pt : c.points) B.points.insert(B.points.end(), &(*points)[3 * (size_t)pt], &(*points)[3 * (size_t)pt + 3]);
-         b.pan_off = (int64_t)B.panels.size();
-         B.panels.insert(B.panels.end(), c.dcols.begin(), c.dcols.end());
-         off[li] = B.out_elems;
-         b.out_s = B.out_elems;
-         b.out_d = B.out_elems + (int64_t)nr * nc;
+         b.pt_off = pt_at[li];
+         double* pdst = B.points.data() + 3 * (size_t)pt_at[li];
+         for (int pt : c.points)
+            for (int k = 0; k < 3; k++) *pdst++ = (*points)[3 * (size_t)pt + k];
+         b.pan_off = pan_at[li];
+         std::copy(c.dcols.begin(), c.dcols.end(), B.panels.begin() + pan_at[li]);
+         off[li] = out_at[li];
+         b.out_s = out_at[li];
+         b.out_d = out_at[li] + (int64_t)nr * nc;
          b.ld_s = b.ld_d = nc;
-         B.out_elems += 2 * (int64_t)nr * nc;
-         B.blocks.push_back(b);
+         B.blocks[blk_at[li]] = b;
       }
       const auto e0 = std::chrono::steady_clock::now();
       const double* out = (*eval)(kernel, *panels, B);
@@ -583,49 +603,95 @@ void Tree::fill_bases() {
    std::vector<int64_t> roff(work.size(), -1), coff(work.size(), -1), soff(work.size(), -1);
    if (eval) {
       IntegralBatch B;
-      auto add_point = [&](const double* p) { B.points.insert(B.points.end(), p, p + 3); };
-      for (size_t wi = 0; wi < work.size(); wi++) {
+      // per cube: a row block and its sphere-fit block (when it has panels and interacting
+      // cubes with points), then a column block (when it has points and interacting cubes
+      // with panels).  Sizes first, running offsets from them, then every cube's part
+      // written in parallel at its offsets: the batch is laid out exactly as if the blocks
+      // were appended one cube after another.
+      const size_t nw = work.size();
+      std::vector<int64_t> pan_at(nw + 1, 0), pt_at(nw + 1, 0), out_at(nw + 1, 0), blk_at(nw + 1, 0);
+#pragma omp parallel for schedule(static)
+      for (int64_t wi = 0; wi < (int64_t)nw; wi++) {
+         const Cube& c = cubes[work[wi]];
+         const int64_t m = (int64_t)c.panels.size(), np = (int64_t)c.points.size();
+         const int64_t nwp = (int64_t)wpts[wi].size(), nwq = (int64_t)wpan[wi].size();
+         int64_t pan = 0, pt = 0, out = 0, blk = 0;
+         if (m > 0 && nwp > 0) {
+            pan += m;
+            pt += nwp + kNumSphere;
+            out += 2 * nwp * m + 2 * (int64_t)kNumSphere * m;
+            blk += 2;
+         }
+         if (np > 0 && nwq > 0) {
+            pan += nwq;
+            pt += np;
+            out += np * 2 * nwq;
+            blk += 1;
+         }
+         pan_at[wi + 1] = pan;
+         pt_at[wi + 1] = pt;
+         out_at[wi + 1] = out;
+         blk_at[wi + 1] = blk;
+      }
+      for (size_t wi = 0; wi < nw; wi++) {
+         pan_at[wi + 1] += pan_at[wi];
+         pt_at[wi + 1] += pt_at[wi];
+         out_at[wi + 1] += out_at[wi];
+         blk_at[wi + 1] += blk_at[wi];
+      }
+      B.panels.resize((size_t)pan_at[nw]);
+      B.points.resize(3 * (size_t)pt_at[nw]);
+      B.blocks.resize((size_t)blk_at[nw]);
+      B.out_elems = out_at[nw];
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t wi = 0; wi < (int64_t)nw; wi++) {
          const Cube& c = cubes[work[wi]];
          const int m = (int)c.panels.size(), np = (int)c.points.size();
          const int nwp = (int)wpts[wi].size(), nwq = (int)wpan[wi].size();
+         int64_t pan = pan_at[wi], pt = pt_at[wi], out = out_at[wi], blk = blk_at[wi];
+         auto put_point = [&](const double* p) {
+            std::copy(p, p + 3, B.points.begin() + 3 * pt);
+            pt++;
+         };
          if (m > 0 && nwp > 0) {
             IntegralBlock b;
-            b.pan_off = (int64_t)B.panels.size();
-            B.panels.insert(B.panels.end(), c.panels.begin(), c.panels.end());
+            b.pan_off = pan;
+            std::copy(c.panels.begin(), c.panels.end(), B.panels.begin() + pan);
+            pan += m;
             b.npan = m;
             b.npts = nwp;
-            b.pt_off = (int64_t)B.points.size() / 3;
-            for (int o : wpts[wi]) add_point(&(*points)[3 * (size_t)cubes[o].points[0]]);
-            roff[wi] = b.out_s = B.out_elems;
-            b.out_d = B.out_elems + (int64_t)nwp * m;
+            b.pt_off = pt;
+            for (int o : wpts[wi]) put_point(&(*points)[3 * (size_t)cubes[o].points[0]]);
+            roff[wi] = b.out_s = out;
+            b.out_d = out + (int64_t)nwp * m;
             b.ld_s = b.ld_d = m;
-            B.out_elems += 2 * (int64_t)nwp * m;
-            B.blocks.push_back(b);
+            out += 2 * (int64_t)nwp * m;
+            B.blocks[blk++] = b;
             // sphere fits of the same panels
             IntegralBlock sb = b;
             double sphere[kNumSphere][3];
             sphere_points(c, sphere);
             sb.npts = kNumSphere;
-            sb.pt_off = (int64_t)B.points.size() / 3;
-            for (int q = 0; q < kNumSphere; q++) add_point(sphere[q]);
-            soff[wi] = sb.out_s = B.out_elems;
-            sb.out_d = B.out_elems + (int64_t)kNumSphere * m;
-            B.out_elems += 2 * (int64_t)kNumSphere * m;
-            B.blocks.push_back(sb);
+            sb.pt_off = pt;
+            for (int q = 0; q < kNumSphere; q++) put_point(sphere[q]);
+            soff[wi] = sb.out_s = out;
+            sb.out_d = out + (int64_t)kNumSphere * m;
+            out += 2 * (int64_t)kNumSphere * m;
+            B.blocks[blk++] = sb;
          }
          if (np > 0 && nwq > 0) {
             IntegralBlock b;
-            b.pan_off = (int64_t)B.panels.size();
-            for (int o : wpan[wi]) B.panels.push_back(cubes[o].panels[0]);
+            b.pan_off = pan;
+            for (int o : wpan[wi]) B.panels[pan++] = cubes[o].panels[0];
             b.npan = nwq;
             b.npts = np;
-            b.pt_off = (int64_t)B.points.size() / 3;
-            for (int pt : c.points) add_point(&(*points)[3 * (size_t)pt]);
-            coff[wi] = b.out_s = B.out_elems;
-            b.out_d = B.out_elems + nwq;
+            b.pt_off = pt;
+            for (int p : c.points) put_point(&(*points)[3 * (size_t)p]);
+            coff[wi] = b.out_s = out;
+            b.out_d = out + nwq;
             b.ld_s = b.ld_d = 2 * nwq;
-            B.out_elems += (int64_t)np * 2 * nwq;
-            B.blocks.push_back(b);
+            out += (int64_t)np * 2 * nwq;
+            B.blocks[blk++] = b;
          }
       }
       const auto e0 = std::chrono::steady_clock::now();

@@ -32,8 +32,8 @@ struct IntegralBlock {
    int32_t ld_s = 0, ld_d = 0;
 };
 struct IntegralBatch {
-   std::vector<double> points;   // 3 per point
-   std::vector<int32_t> panels;  // indices into the tree's panels
+   std::vector<double, FillLater<double>> points;  // 3 per point (sized, then written in parallel)
+   std::vector<int32_t> panels;                    // indices into the tree's panels
    std::vector<IntegralBlock> blocks;
    int64_t out_elems = 0;        // size of the output array
 };
