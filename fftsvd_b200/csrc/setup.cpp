@@ -383,31 +383,44 @@ void Tree::choose_depth(int max_panels) {
 
 void Tree::make_lists() {
    for (Cube& c : cubes) { c.local.clear(); c.inter.clear(); }
-   for (size_t ci = 0; ci < cubes.size(); ci++) {
-      Cube& c = cubes[ci];
-      if (c.parent < 0) continue;
-      const Cube& par = cubes[c.parent];
-      for (int k = 0; k < 8; k++)
-         if (par.child[k] >= 0 && par.child[k] != (int)ci) c.local.push_back(par.child[k]);
-      for (int pl : par.local)
-         for (int k = 0; k < 8; k++) {
-            const int o = cubes[pl].child[k];
-            if (o < 0) continue;
-            const Cube& oc = cubes[o];
-            const bool near = std::abs(oc.idx[0] - c.idx[0]) <= 1 && std::abs(oc.idx[1] - c.idx[1]) <= 1 &&
-                              std::abs(oc.idx[2] - c.idx[2]) <= 1;
-            if (near) c.local.push_back(o);
-         }
-      for (int pl : par.local)
-         for (int k = 0; k < 8; k++) {
-            const int o = cubes[pl].child[k];
-            if (o < 0) continue;
-            const Cube& oc = cubes[o];
-            const bool far = std::abs(oc.idx[0] - c.idx[0]) > 1 || std::abs(oc.idx[1] - c.idx[1]) > 1 ||
-                             std::abs(oc.idx[2] - c.idx[2]) > 1;
-            if (far) c.inter.push_back(o);
-         }
+   // cubes are in breadth-first order, so each level is one contiguous range and a cube needs
+   // only its parent's list, complete once the level above is: one level at a time, its
+   // cubes in parallel
+   for (size_t lo = 0; lo < cubes.size();) {
+      size_t hi = lo;
+      while (hi < cubes.size() && cubes[hi].level == cubes[lo].level) hi++;
+#pragma omp parallel for schedule(dynamic, 256)
+      for (int64_t ci = (int64_t)lo; ci < (int64_t)hi; ci++) make_lists_of((size_t)ci);
+      lo = hi;
    }
+}
+
+// The local (neighbouring) and interaction lists of cube ci: the other children of its
+// parent and the children of the parent's neighbours, split by whether they touch cube ci.
+void Tree::make_lists_of(size_t ci) {
+   Cube& c = cubes[ci];
+   if (c.parent < 0) return;
+   const Cube& par = cubes[c.parent];
+   for (int k = 0; k < 8; k++)
+      if (par.child[k] >= 0 && par.child[k] != (int)ci) c.local.push_back(par.child[k]);
+   for (int pl : par.local)
+      for (int k = 0; k < 8; k++) {
+         const int o = cubes[pl].child[k];
+         if (o < 0) continue;
+         const Cube& oc = cubes[o];
+         const bool near = std::abs(oc.idx[0] - c.idx[0]) <= 1 && std::abs(oc.idx[1] - c.idx[1]) <= 1 &&
+                           std::abs(oc.idx[2] - c.idx[2]) <= 1;
+         if (near) c.local.push_back(o);
+      }
+   for (int pl : par.local)
+      for (int k = 0; k < 8; k++) {
+         const int o = cubes[pl].child[k];
+         if (o < 0) continue;
+         const Cube& oc = cubes[o];
+         const bool far = std::abs(oc.idx[0] - c.idx[0]) > 1 || std::abs(oc.idx[1] - c.idx[1]) > 1 ||
+                          std::abs(oc.idx[2] - c.idx[2]) > 1;
+         if (far) c.inter.push_back(o);
+      }
 }
 
 void Tree::fill_near() {

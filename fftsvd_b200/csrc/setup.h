@@ -95,6 +95,7 @@ struct Tree {
    void add_level();            // one more level below the current leaves
    void choose_depth(int max_panels);
    void make_lists();
+   void make_lists_of(size_t ci);
    void fill_near();
    void fill_pinv();
    void fill_T();
