@@ -17,6 +17,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -270,18 +271,22 @@ static void r2c3(int N, const std::vector<double>& in, std::vector<std::complex<
 
 // ------------------------------------------------------------------ tree
 
-// Children of cube ci in cx, cy, cz order: one pass over its panels and points sends each
-// to the octant its coordinates select (coordinate >= the centre: upper half), keeping the
-// parent's order within every child; empty octants get no cube.
-void Tree::split_cube(size_t ci) {
+// The octant of every panel and point of cube ci (coordinate >= the centre: upper half), in
+// the cube's own order within each octant.
+void Tree::octants(size_t ci, Octants& bp, Octants& bq) const {
+   const Cube& par = cubes[ci];
+   const double cc[3] = {par.center[0], par.center[1], par.center[2]};
+   auto octant = [&](const double* p) { return (p[0] >= cc[0]) * 4 + (p[1] >= cc[1]) * 2 + (p[2] >= cc[2]); };
+   for (int i : par.panels) bp[octant((*panels)[i].centroid)].push_back(i);
+   for (int i : par.points) bq[octant(&(*points)[3 * (size_t)i])].push_back(i);
+}
+
+// Children of cube ci in cx, cy, cz order from its octant lists; empty octants get no cube.
+void Tree::append_children(size_t ci, Octants& bp, Octants& bq) {
    const Cube& par = cubes[ci];
    const double cc[3] = {par.center[0], par.center[1], par.center[2]};
    const double pb0[3] = {par.b0[0], par.b0[1], par.b0[2]};
    const int pidx[3] = {par.idx[0], par.idx[1], par.idx[2]}, plevel = par.level;
-   auto octant = [&](const double* p) { return (p[0] >= cc[0]) * 4 + (p[1] >= cc[1]) * 2 + (p[2] >= cc[2]); };
-   std::vector<int> bp[8], bq[8];
-   for (int i : par.panels) bp[octant((*panels)[i].centroid)].push_back(i);
-   for (int i : par.points) bq[octant(&(*points)[3 * (size_t)i])].push_back(i);
    for (int slot = 0; slot < 8; slot++) {
       if (bp[slot].empty() && bq[slot].empty()) continue;
       const int cbit[3] = {slot >> 2, (slot >> 1) & 1, slot & 1};
@@ -307,14 +312,20 @@ void Tree::split_cube(size_t ci) {
 
 // Cubes are kept in breadth-first creation order (children of one cube in cx, cy, cz
 // order), so the tree of depth d + 1 is the tree of depth d with the children of its
-// leaves appended in order.
+// leaves appended in order.  The leaves' panels and points are sorted into octants in
+// parallel; the children are then appended leaf after leaf.
 void Tree::add_level() {
    const size_t n0 = cubes.size();
+   std::vector<size_t> split;
    for (size_t ci = 0; ci < n0; ci++)
-      if (cubes[ci].level == depth - 1) {
-         cubes[ci].leaf = false;
-         split_cube(ci);
-      }
+      if (cubes[ci].level == depth - 1) split.push_back(ci);
+   std::vector<Octants> bp(split.size()), bq(split.size());
+#pragma omp parallel for schedule(dynamic, 16)
+   for (int64_t i = 0; i < (int64_t)split.size(); i++) octants(split[i], bp[i], bq[i]);
+   for (size_t i = 0; i < split.size(); i++) {
+      cubes[split[i]].leaf = false;
+      append_children(split[i], bp[i], bq[i]);
+   }
    depth++;
    for (size_t ci = n0; ci < cubes.size(); ci++) {
       Cube& c = cubes[ci];

@@ -1,6 +1,7 @@
 // Host setup of the compressed FFTSVD operator (see setup.cpp).
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <functional>
 #include <stdexcept>
@@ -91,8 +92,10 @@ struct Tree {
    double eval_ms = 0.0;                     // wall time inside eval
 
    void build_cubes(int depth);
-   void split_cube(size_t ci);  // children of cube ci, appended
-   void add_level();            // one more level below the current leaves
+   using Octants = std::array<std::vector<int>, 8>;
+   void octants(size_t ci, Octants& panels_in, Octants& points_in) const;  // cube ci's items by octant
+   void append_children(size_t ci, Octants& panels_in, Octants& points_in);  // its children, appended
+   void add_level();  // one more level below the current leaves
    void choose_depth(int max_panels);
    void make_lists();
    void make_lists_of(size_t ci);
